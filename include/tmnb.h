@@ -1,0 +1,217 @@
+/*
+ * tmnb: C ABI of the B200 (sm_100a) nonbonded potential.
+ *
+ * Drop-in boundary for timemachine's Nonbonded hot path. Each entry point
+ * below names the reference interface it replaces (paths relative to the
+ * timemachine source tree). Conventions shared by all entry points:
+ *
+ *  - Device pointers are plain CUDA device addresses; `stream` is a
+ *    cudaStream_t passed as void* (0 = legacy default stream).
+ *  - A NULL output pointer means "do not compute" that output; it selects the
+ *    kernel variant (timemachine/cpp/src/nonbonded_all_pairs.cu:375-379).
+ *  - Outputs ACCUMULATE (+=) in the reference's int64 fixed-point encoding
+ *    (du_dx, u, du_dl and du_dcharge at 2^36; du_dsigma at 2^37; du_depsilon
+ *    at 2^38; timemachine/cpp/src/fixed_point.hpp:3-8). The caller zeroes
+ *    them (timemachine/cpp/src/potential.cu:141-157).
+ *  - du_dl and u are per-atom buffers of length N whose SUM is the result
+ *    (timemachine/cpp/src/wrap_kernels.cpp:596-601); the per-atom split itself is
+ *    not part of the contract.
+ *  - Parameters are [N,3] (or [2N,3] for interpolated potentials, lambda=0
+ *    block first) doubles: charge * sqrt(138.935456), sigma/2, sqrt(epsilon).
+ *  - Every call returns a tmnb_status; tmnb_last_error() gives the message of
+ *    the last failing call on the calling thread. No call aborts the process
+ *    (the reference calls exit() on CUDA errors, timemachine/cpp/src/gpu_utils.cuh:12-20).
+ *  - A handle is not thread-safe (timemachine/cpp/src/potential.hpp:7): use
+ *    one handle per stream/thread.
+ */
+#ifndef TMNB_H
+#define TMNB_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct tmnb_potential tmnb_potential;
+
+typedef enum tmnb_status {
+    TMNB_OK = 0,
+    TMNB_ERR_INVALID_ARGUMENT = 1,
+    TMNB_ERR_CUDA = 2,
+    TMNB_ERR_NONORTHO_BOX = 3,  /* "Provided non-ortholinear box, unable to compute nonbonded energy" */
+    TMNB_ERR_BOX_TOO_SMALL = 4, /* "Cutoff with padding is more than half of the box width, ..." */
+    TMNB_ERR_UNSUPPORTED = 5,
+    TMNB_ERR_INTERNAL = 6
+} tmnb_status;
+
+/* Message of the last failing call on this thread ("" if none). */
+const char *tmnb_last_error(void);
+
+/* Library version string. */
+const char *tmnb_version(void);
+
+/*
+ * NonbondedAllPairs: every pair of the atom set (all N atoms, or the subset
+ * atom_idxs[0..K) when atom_idxs != NULL) within cutoff, through a tile
+ * neighbour list. Replaces the constructor
+ * timemachine/cpp/src/nonbonded_all_pairs.cu:16-141 as bound at
+ * timemachine/cpp/src/wrap_kernels.cpp:835-893 (NonbondedAllPairs_f32 and
+ * NonbondedAllPairsInterpolated_f32). precision: 32 (FP32 pair arithmetic).
+ * The lambda transforms are the identity ("lambda"), the reference default.
+ */
+tmnb_status tmnb_all_pairs_create(
+    int N,
+    const int32_t *lambda_plane_idxs,  /* [N] host */
+    const int32_t *lambda_offset_idxs, /* [N] host */
+    double beta,
+    double cutoff,
+    const int32_t *atom_idxs, /* [K] host, unique, or NULL */
+    int K,
+    int interpolated,
+    int precision,
+    tmnb_potential **out);
+
+/*
+ * NonbondedPairList / NonbondedPairListNegated: the listed pairs only, each
+ * scaled by (charge_scale, lj_scale), subtracted when negated != 0. Replaces
+ * timemachine/cpp/src/nonbonded_pair_list.cu:10-75 as bound at
+ * timemachine/cpp/src/wrap_kernels.cpp:962-1013.
+ */
+tmnb_status tmnb_pair_list_create(
+    int N,
+    const int32_t *pair_idxs, /* [M,2] host */
+    const double *scales,     /* [M,2] host: (charge_scale, lj_scale) */
+    int M,
+    const int32_t *lambda_plane_idxs,  /* [N] host */
+    const int32_t *lambda_offset_idxs, /* [N] host */
+    double beta,
+    double cutoff,
+    int negated,
+    int interpolated,
+    int precision,
+    tmnb_potential **out);
+
+/*
+ * Nonbonded: all pairs minus the scaled exclusions, in ONE device pipeline
+ * (one neighbour list, the exclusion pairs fused into the pair kernel's
+ * launch). Replaces timemachine/lib/potentials.py:269-301, i.e.
+ * FanoutSummedPotential([NonbondedAllPairs, NonbondedPairListNegated]),
+ * and its interpolated form (timemachine/lib/potentials.py:333-344).
+ */
+tmnb_status tmnb_nonbonded_create(
+    int N,
+    const int32_t *exclusion_idxs, /* [M,2] host */
+    const double *scales,          /* [M,2] host */
+    int M,
+    const int32_t *lambda_plane_idxs,  /* [N] host */
+    const int32_t *lambda_offset_idxs, /* [N] host */
+    double beta,
+    double cutoff,
+    int interpolated,
+    int precision,
+    tmnb_potential **out);
+
+/* Releases all device memory of the handle (NULL is a no-op). */
+tmnb_status tmnb_potential_destroy(tmnb_potential *pot);
+
+/*
+ * Device entry: replaces the virtual Potential::execute_device
+ * (timemachine/cpp/src/potential.hpp:51-62). No host synchronisation and no
+ * allocation happen inside; the neighbour-list rebuild decision is taken on
+ * the device, so the call can be captured in a CUDA graph. Box errors are
+ * recorded on the device; read them with tmnb_potential_check_device_error.
+ */
+tmnb_status tmnb_potential_execute_device(
+    tmnb_potential *pot,
+    int N,
+    int P,
+    const double *d_x,   /* [N,3] */
+    const double *d_p,   /* [P] */
+    const double *d_box, /* [3,3] */
+    double lambda,
+    unsigned long long *d_du_dx, /* [N,3] or NULL */
+    unsigned long long *d_du_dp, /* [P] or NULL */
+    unsigned long long *d_du_dl, /* [N] or NULL */
+    unsigned long long *d_u,     /* [N] or NULL */
+    void *stream);
+
+/*
+ * Host entry: replaces Potential::execute_host
+ * (timemachine/cpp/src/potential.cu:110-185): copies the host inputs in,
+ * zeroes and computes the selected outputs, copies them out and
+ * synchronises. Outputs are OVERWRITTEN (not accumulated), as in the
+ * reference. Device staging buffers are owned by the handle and reused.
+ */
+tmnb_status tmnb_potential_execute_host(
+    tmnb_potential *pot,
+    int N,
+    int P,
+    const double *h_x,
+    const double *h_p,
+    const double *h_box,
+    double lambda,
+    unsigned long long *h_du_dx,
+    unsigned long long *h_du_dp,
+    unsigned long long *h_du_dl,
+    unsigned long long *h_u);
+
+/*
+ * Batched host entry: replaces Potential::execute_batch_host behind
+ * execute_selective_batch (timemachine/cpp/src/wrap_kernels.cpp:381-551).
+ * Executes every (coords, params, lambda) combination; outputs have the
+ * leading shape [coord_batches, param_batches, lambda_batches].
+ */
+tmnb_status tmnb_potential_execute_batch_host(
+    tmnb_potential *pot,
+    int coord_batches,
+    int N,
+    int param_batches,
+    int P,
+    int lambda_batches,
+    const double *h_x,       /* [coord_batches,N,3] */
+    const double *h_p,       /* [param_batches,P] */
+    const double *h_boxes,   /* [coord_batches,3,3] */
+    const double *h_lambdas, /* [lambda_batches] */
+    unsigned long long *h_du_dx,
+    unsigned long long *h_du_dp,
+    unsigned long long *h_du_dl,
+    unsigned long long *h_u);
+
+/* Fixed-point du_dp to float with per-column exponents
+ * (timemachine/cpp/src/nonbonded_all_pairs.cu:435-450). */
+tmnb_status tmnb_potential_du_dp_fixed_to_float(
+    tmnb_potential *pot, int N, int P, const unsigned long long *du_dp, double *du_dp_float);
+
+/* timemachine/cpp/src/nonbonded_all_pairs.cu:180-187 */
+tmnb_status tmnb_potential_set_nblist_padding(tmnb_potential *pot, double padding);
+tmnb_status tmnb_potential_disable_hilbert_sort(tmnb_potential *pot);
+
+/* Synchronises `stream`, returns (and clears) a box error recorded by the
+ * device since the last check. */
+tmnb_status tmnb_potential_check_device_error(tmnb_potential *pot, void *stream);
+
+/* Diagnostics of the last neighbour-list build (synchronises `stream`):
+ * tiles, work items and the number of rebuilds so far. */
+tmnb_status tmnb_potential_nblist_stats(
+    tmnb_potential *pot, void *stream, int *n_tiles, int *n_items, int *n_rebuilds);
+
+/* Instrumentation (no reference counterpart): CUDA events around every
+ * pair-kernel launch on the launching stream, and the duration of the last
+ * one (synchronises on its end event). */
+tmnb_status tmnb_potential_enable_timing(tmnb_potential *pot, int on);
+tmnb_status tmnb_potential_last_pair_kernel_ms(tmnb_potential *pot, float *ms);
+
+/* Measured FP32 FMA throughput of the current device in TFLOP/s (the
+ * denominator of the pair kernel's FP32 roofline; no reference counterpart). */
+tmnb_status tmnb_probe_fp32_peak(double *tflops);
+
+/* Expected parameter count P (N*3, or 2*N*3 when interpolated). */
+int tmnb_potential_num_params(const tmnb_potential *pot);
+int tmnb_potential_num_atoms(const tmnb_potential *pot);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* TMNB_H */

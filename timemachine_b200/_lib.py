@@ -1,0 +1,117 @@
+"""Loader and build recipe of the native library (libtmnb.so, C ABI in include/tmnb.h).
+
+The library is built in-tree for sm_100a. There is no fallback: importing a
+potential whose library is missing raises immediately.
+"""
+
+import ctypes
+import os
+import subprocess
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+REPO = os.path.dirname(HERE)
+LIB_PATH = os.path.join(HERE, "libtmnb.so")
+CSRC = os.path.join(HERE, "csrc")
+INCLUDE = os.path.join(REPO, "include")
+
+NVCC_FLAGS = [
+    "-O3",
+    "-lineinfo",
+    "-std=c++17",
+    "-gencode",
+    "arch=compute_100a,code=sm_100a",
+    "-Xcompiler",
+    "-fPIC",
+    "-shared",
+]
+
+SOURCES = ["nonbonded.cu"]
+
+
+def build(verbose: bool = False) -> str:
+    """Compile libtmnb.so for sm_100a (nvcc cross-compiles without a GPU)."""
+    nvcc = os.environ.get("NVCC", "nvcc")
+    cmd = [nvcc, *NVCC_FLAGS, "-I" + INCLUDE, "-o", LIB_PATH] + [os.path.join(CSRC, s) for s in SOURCES]
+    if verbose:
+        print(" ".join(cmd))
+    subprocess.run(cmd, check=True)
+    return LIB_PATH
+
+
+c_ull_p = ctypes.POINTER(ctypes.c_ulonglong)
+c_double_p = ctypes.POINTER(ctypes.c_double)
+c_int_p = ctypes.POINTER(ctypes.c_int32)
+
+_lib = None
+
+
+class TmnbError(RuntimeError):
+    """Error reported by the native library (subclass of RuntimeError, as the reference raises)."""
+
+    def __init__(self, status, message):
+        super().__init__(message)
+        self.status = status
+
+
+def _declare(lib):
+    vp = ctypes.c_void_p
+    i = ctypes.c_int
+    d = ctypes.c_double
+    lib.tmnb_last_error.restype = ctypes.c_char_p
+    lib.tmnb_version.restype = ctypes.c_char_p
+    lib.tmnb_all_pairs_create.argtypes = [i, vp, vp, d, d, vp, i, i, i, ctypes.POINTER(vp)]
+    lib.tmnb_pair_list_create.argtypes = [i, vp, vp, i, vp, vp, d, d, i, i, i, ctypes.POINTER(vp)]
+    lib.tmnb_nonbonded_create.argtypes = [i, vp, vp, i, vp, vp, d, d, i, i, ctypes.POINTER(vp)]
+    lib.tmnb_potential_destroy.argtypes = [vp]
+    lib.tmnb_potential_execute_device.argtypes = [vp, i, i, vp, vp, vp, d, vp, vp, vp, vp, vp]
+    lib.tmnb_potential_execute_host.argtypes = [vp, i, i, vp, vp, vp, d, vp, vp, vp, vp]
+    lib.tmnb_potential_execute_batch_host.argtypes = [vp, i, i, i, i, i, vp, vp, vp, vp, vp, vp, vp, vp]
+    lib.tmnb_potential_du_dp_fixed_to_float.argtypes = [vp, i, i, vp, vp]
+    lib.tmnb_potential_set_nblist_padding.argtypes = [vp, d]
+    lib.tmnb_potential_disable_hilbert_sort.argtypes = [vp]
+    lib.tmnb_potential_check_device_error.argtypes = [vp, vp]
+    lib.tmnb_potential_nblist_stats.argtypes = [vp, vp, c_int_p, c_int_p, c_int_p]
+    lib.tmnb_potential_enable_timing.argtypes = [vp, i]
+    lib.tmnb_potential_last_pair_kernel_ms.argtypes = [vp, ctypes.POINTER(ctypes.c_float)]
+    lib.tmnb_probe_fp32_peak.argtypes = [ctypes.POINTER(ctypes.c_double)]
+    lib.tmnb_potential_num_params.argtypes = [vp]
+    lib.tmnb_potential_num_atoms.argtypes = [vp]
+    for name in [
+        "tmnb_all_pairs_create",
+        "tmnb_pair_list_create",
+        "tmnb_nonbonded_create",
+        "tmnb_potential_destroy",
+        "tmnb_potential_execute_device",
+        "tmnb_potential_execute_host",
+        "tmnb_potential_execute_batch_host",
+        "tmnb_potential_du_dp_fixed_to_float",
+        "tmnb_potential_set_nblist_padding",
+        "tmnb_potential_disable_hilbert_sort",
+        "tmnb_potential_check_device_error",
+        "tmnb_potential_nblist_stats",
+        "tmnb_potential_enable_timing",
+        "tmnb_potential_last_pair_kernel_ms",
+        "tmnb_probe_fp32_peak",
+    ]:
+        getattr(lib, name).restype = ctypes.c_int
+    lib.tmnb_potential_num_params.restype = ctypes.c_int
+    lib.tmnb_potential_num_atoms.restype = ctypes.c_int
+    return lib
+
+
+def lib():
+    """The loaded native library; raises if it has not been built."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(
+                f"{LIB_PATH} is missing: build it with timemachine_b200._lib.build() "
+                "(there is no CPU fallback for the nonbonded potential)"
+            )
+        _lib = _declare(ctypes.CDLL(LIB_PATH))
+    return _lib
+
+
+def check(status):
+    if status != 0:
+        raise TmnbError(status, lib().tmnb_last_error().decode())

@@ -1,0 +1,1052 @@
+// Device pipeline of one nonbonded evaluation on sm_100a.
+//
+// Per evaluation (stream-ordered, no host synchronisation):
+//   k_check_prepare   rebuild decision (any atom moved > padding/2, or box
+//                     changed), box validation, and the per-slot FP32 staging
+//                     of coordinates, w, parameters (and dp/dlambda) using the
+//                     current slot order.
+//   k_bin_keys / k_bin_scan / k_bin_scatter / k_block_bounds / k_build_tiles
+//                     neighbour-list rebuild; every one returns at once unless
+//                     the rebuild flag is set, so the sequence is graph-capturable.
+//   k_pair            persistent kernel over the tile work items and the
+//                     exclusion / scaled-pair chunks (dynamic scheduling).
+//   k_finalize        scatter of the slot-ordered int64 accumulators into the
+//                     caller's original-order outputs, then zeroing.
+//
+// The work of each stage follows the reference pipeline
+// (timemachine/cpp/src/nonbonded_all_pairs.cu:222-433,
+//  timemachine/cpp/src/neighborlist.cu:126-185,
+//  timemachine/cpp/src/nonbonded_pair_list.cu:95-166); the data layout,
+// spatial sort, scheduling and fusion are this file's own.
+#pragma once
+
+#include "nb_pair_math.cuh"
+
+namespace tmb {
+
+constexpr unsigned FULL_MASK = 0xffffffffu;
+constexpr int TILE = 32;
+
+// Sticky device-side state of one potential instance.
+struct DevState {
+    int rebuild;          // 1: the neighbour list must be rebuilt in this evaluation
+    int error;            // sticky error code (TMNB_ERR_* values), 0 = ok
+    int n_items;          // tile work items produced by the last rebuild
+    int next_item;        // dynamic work counter of k_pair (reset by k_check_prepare)
+    unsigned done_ctas;   // completion counter of k_build_tiles
+    unsigned total_tiles; // tiles produced by the last rebuild
+    int rebuilds;         // number of rebuilds performed (diagnostics)
+    int pad;
+};
+
+// Error codes written into DevState::error (mirrored in include/tmnb.h).
+constexpr int DEV_ERR_NONORTHO_BOX = 3;
+constexpr int DEV_ERR_BOX_TOO_SMALL = 4;
+
+struct SlotArrays {
+    float4 *posw;  // [S] x, y, z, w
+    float4 *prm;   // [S] q, sig, eps, dw/dlambda
+    float4 *dprm;  // [S] dq/dl, dsig/dl, deps/dl, 0 (interpolated only)
+};
+
+struct PrepareArgs {
+    int N;                      // atoms in the system
+    int S;                      // slots (atoms in the evaluated set)
+    const double *x;            // [N,3]
+    const double *p;            // [N,3] or [2N,3] (interpolated)
+    const double *box;          // [3,3]
+    double lambda;
+    double cutoff;
+    double padding;
+    const int *plane;           // [N]
+    const int *offset;          // [N]
+    int interpolated;
+    SlotArrays slots;
+};
+
+// Stage one atom into its slot. w = cutoff*(plane + offset*lambda),
+// dw/dlambda = offset*cutoff (timemachine/cpp/src/kernels/k_lambda_transformer_jit.cuh:25-55
+// with the identity lambda transform); interpolated parameters
+// p = (1-lambda) p0 + lambda p1, dp/dlambda = p1 - p0 (same file :57-98).
+__device__ __forceinline__ void prepare_slot(const PrepareArgs &a, int s, int atom) {
+    const double lambda = a.lambda;
+    const int plane = a.plane[atom];
+    const int offset = a.offset[atom];
+    const double f_lambda = lambda;
+    const double f_lambda_grad = 1.0;
+    const double w = (plane + offset * f_lambda) * a.cutoff;
+    const double dw_dl = offset * f_lambda_grad * a.cutoff;
+    const double *xa = a.x + 3 * (size_t)atom;
+    a.slots.posw[s] = make_float4((float)xa[0], (float)xa[1], (float)xa[2], (float)w);
+    if (a.interpolated) {
+        const double *p0 = a.p + 3 * (size_t)atom;
+        const double *p1 = a.p + 3 * ((size_t)a.N + atom);
+        double pq = (1 - f_lambda) * p0[0] + f_lambda * p1[0];
+        double ps = (1 - f_lambda) * p0[1] + f_lambda * p1[1];
+        double pe = (1 - f_lambda) * p0[2] + f_lambda * p1[2];
+        double dq = f_lambda_grad * (p1[0] - p0[0]);
+        double ds = f_lambda_grad * (p1[1] - p0[1]);
+        double de = f_lambda_grad * (p1[2] - p0[2]);
+        a.slots.prm[s] = make_float4((float)pq, (float)ps, (float)pe, (float)dw_dl);
+        a.slots.dprm[s] = make_float4((float)dq, (float)ds, (float)de, 0.0f);
+    } else {
+        const double *pa = a.p + 3 * (size_t)atom;
+        a.slots.prm[s] = make_float4((float)pa[0], (float)pa[1], (float)pa[2], (float)dw_dl);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Rebuild decision + staging.
+// ---------------------------------------------------------------------------
+__global__ void k_check_prepare(
+    PrepareArgs a,
+    const unsigned *__restrict__ perm, // [S] slot -> atom
+    const double *__restrict__ nb_x,   // [N,3] coordinates at the last rebuild (nullptr: no neighbour list)
+    const double *__restrict__ nb_box, // [9]
+    DevState *state) {
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (tid == 0) {
+        state->next_item = 0;
+        if (nb_x != nullptr) {
+            // Orthorhombic box whose every edge is at least twice cutoff+padding
+            // (timemachine/cpp/src/nonbonded_all_pairs.cu:315-329); checked in
+            // the reference's order, so an off-diagonal entry wins.
+            const double db_cutoff = (a.cutoff + a.padding) * 2;
+            int err = 0;
+            for (int k = 0; k < 9 && err == 0; k++) {
+                if (k == 0 || k == 4 || k == 8) {
+                    if (a.box[k] < db_cutoff) {
+                        err = DEV_ERR_BOX_TOO_SMALL;
+                    }
+                } else if (a.box[k] != 0.0) {
+                    err = DEV_ERR_NONORTHO_BOX;
+                }
+            }
+            if (err != 0) {
+                state->error = err;
+            }
+            for (int k = 0; k < 9; k++) {
+                if (a.box[k] != nb_box[k]) {
+                    state->rebuild = 1;
+                }
+            }
+        }
+    }
+    const double half_pad2 = 0.25 * a.padding * a.padding;
+    for (int s = tid; s < a.S; s += gridDim.x * blockDim.x) {
+        const int atom = perm[s];
+        if (nb_x != nullptr) {
+            const double *xn = a.x + 3 * (size_t)atom;
+            const double *xo = nb_x + 3 * (size_t)atom;
+            const double dx = xn[0] - xo[0];
+            const double dy = xn[1] - xo[1];
+            const double dz = xn[2] - xo[2];
+            if (dx * dx + dy * dy + dz * dz > half_pad2) {
+                state->rebuild = 1; // benign race: every writer stores 1
+            }
+        }
+        prepare_slot(a, s, atom);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Spatial sort: atoms are binned into a 2^b x 2^b x 2^b grid whose cells are
+// ordered along a 3D Hilbert curve; a counting sort over the cells gives the
+// slot order. The Hilbert index uses Skilling's transposed-axes algorithm
+// (J. Skilling, "Programming the Hilbert curve", AIP Conf. Proc. 707, 2004).
+// Order inside a cell is arbitrary: results do not depend on it because all
+// accumulation is exact integer arithmetic.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ unsigned hilbert_index_3d(unsigned x, unsigned y, unsigned z, int bits) {
+    unsigned X[3] = {x, y, z};
+    const unsigned M = 1u << (bits - 1);
+    for (unsigned Q = M; Q > 1; Q >>= 1) {
+        const unsigned P = Q - 1;
+        for (int i = 0; i < 3; i++) {
+            if (X[i] & Q) {
+                X[0] ^= P;
+            } else {
+                const unsigned t = (X[0] ^ X[i]) & P;
+                X[0] ^= t;
+                X[i] ^= t;
+            }
+        }
+    }
+    X[1] ^= X[0];
+    X[2] ^= X[1];
+    unsigned t = 0;
+    for (unsigned Q = M; Q > 1; Q >>= 1) {
+        if (X[2] & Q) {
+            t ^= Q - 1;
+        }
+    }
+    X[0] ^= t;
+    X[1] ^= t;
+    X[2] ^= t;
+    unsigned h = 0;
+    for (int b = bits - 1; b >= 0; b--) {
+        h = (h << 3) | (((X[0] >> b) & 1u) << 2) | (((X[1] >> b) & 1u) << 1) | ((X[2] >> b) & 1u);
+    }
+    return h;
+}
+
+struct SortArgs {
+    int N;
+    int S;
+    const double *x;
+    const double *box;
+    const int *set_atoms; // [S] atoms of the evaluated set, nullptr: identity (S == N)
+    int grid_bits;        // b: 2^b cells per axis
+    int hilbert;          // 0: keep the set order
+    unsigned *keys;       // [S]
+    int *bin_count;       // [8^b]
+    int *bin_cursor;      // [8^b]
+};
+
+__device__ __forceinline__ int set_atom(const SortArgs &a, int k) { return a.set_atoms ? a.set_atoms[k] : k; }
+
+__global__ void k_bin_keys(SortArgs a, const DevState *state) {
+    if (!state->rebuild || state->error || !a.hilbert) {
+        return;
+    }
+    const int G = 1 << a.grid_bits;
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < a.S; k += gridDim.x * blockDim.x) {
+        const int atom = set_atom(a, k);
+        unsigned c[3];
+        for (int d = 0; d < 3; d++) {
+            const double L = a.box[d * 4];
+            double v = a.x[3 * (size_t)atom + d];
+            v -= L * floor(v / L);
+            int ci = (int)(v / L * G);
+            ci = ci < 0 ? 0 : (ci >= G ? G - 1 : ci);
+            c[d] = (unsigned)ci;
+        }
+        const unsigned key = hilbert_index_3d(c[0], c[1], c[2], a.grid_bits);
+        a.keys[k] = key;
+        atomicAdd(&a.bin_count[key], 1);
+    }
+}
+
+// Single-CTA exclusive scan of the cell counts (and reset of the counts and
+// of the tile-build counters).
+__global__ void k_bin_scan(SortArgs a, DevState *state) {
+    if (!state->rebuild || state->error) {
+        return;
+    }
+    if (threadIdx.x == 0) {
+        state->done_ctas = 0;
+        state->total_tiles = 0;
+    }
+    if (!a.hilbert) {
+        return;
+    }
+    const int NB = 1 << (3 * a.grid_bits);
+    __shared__ int warp_sums[32];
+    __shared__ int carry;
+    if (threadIdx.x == 0) {
+        carry = 0;
+    }
+    __syncthreads();
+    const int lane = threadIdx.x & 31;
+    const int wid = threadIdx.x >> 5;
+    const int nwarps = blockDim.x >> 5;
+    for (int base = 0; base < NB; base += blockDim.x) {
+        const int b = base + threadIdx.x;
+        const int v = b < NB ? a.bin_count[b] : 0;
+        int incl = v;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int n = __shfl_up_sync(FULL_MASK, incl, o);
+            if (lane >= o) {
+                incl += n;
+            }
+        }
+        if (lane == 31) {
+            warp_sums[wid] = incl;
+        }
+        __syncthreads();
+        if (wid == 0) {
+            int ws = lane < nwarps ? warp_sums[lane] : 0;
+            for (int o = 1; o < 32; o <<= 1) {
+                const int n = __shfl_up_sync(FULL_MASK, ws, o);
+                if (lane >= o) {
+                    ws += n;
+                }
+            }
+            if (lane < nwarps) {
+                warp_sums[lane] = ws; // inclusive
+            }
+        }
+        __syncthreads();
+        const int warp_prefix = wid > 0 ? warp_sums[wid - 1] : 0;
+        if (b < NB) {
+            a.bin_cursor[b] = carry + warp_prefix + incl - v;
+            a.bin_count[b] = 0;
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            carry += warp_sums[nwarps - 1];
+        }
+        __syncthreads();
+    }
+}
+
+__global__ void k_bin_scatter(
+    SortArgs sa,
+    PrepareArgs pa,
+    unsigned *__restrict__ perm,    // [S] slot -> atom
+    int *__restrict__ slot_of,      // [N] atom -> slot (nullptr: not needed)
+    double *__restrict__ nb_x,      // [N,3]
+    double *__restrict__ nb_box,    // [9]
+    const DevState *state) {
+    if (!state->rebuild || state->error) {
+        return;
+    }
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    if (tid < 9) {
+        nb_box[tid] = sa.box[tid];
+    }
+    for (int k = tid; k < sa.S; k += gridDim.x * blockDim.x) {
+        const int atom = set_atom(sa, k);
+        const int s = sa.hilbert ? atomicAdd(&sa.bin_cursor[sa.keys[k]], 1) : k;
+        perm[s] = (unsigned)atom;
+        if (slot_of) {
+            slot_of[atom] = s;
+        }
+        nb_x[3 * (size_t)atom + 0] = sa.x[3 * (size_t)atom + 0];
+        nb_x[3 * (size_t)atom + 1] = sa.x[3 * (size_t)atom + 1];
+        nb_x[3 * (size_t)atom + 2] = sa.x[3 * (size_t)atom + 2];
+        prepare_slot(pa, s, atom);
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Block bounding boxes: one warp per 32-slot block; every atom is imaged
+// next to the block's first atom, then min/max give centre and half-extent.
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ float wrap_delta(float d, float L, float inv_L) { return d - L * rintf(d * inv_L); }
+
+__global__ void k_block_bounds(
+    int S,
+    const double *__restrict__ box,
+    const float4 *__restrict__ posw,
+    float4 *__restrict__ bb_ctr,
+    float4 *__restrict__ bb_ext,
+    const DevState *state) {
+    if (!state->rebuild || state->error) {
+        return;
+    }
+    const int lane = threadIdx.x & 31;
+    const int RB = (S + TILE - 1) / TILE;
+    const float Lx = (float)box[0], Ly = (float)box[4], Lz = (float)box[8];
+    const float iLx = 1.0f / Lx, iLy = 1.0f / Ly, iLz = 1.0f / Lz;
+    for (int rb = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; rb < RB; rb += (gridDim.x * blockDim.x) >> 5) {
+        const int s = rb * TILE + lane;
+        const bool valid = s < S;
+        float4 p = valid ? posw[s] : make_float4(0.f, 0.f, 0.f, 0.f);
+        const float rx = __shfl_sync(FULL_MASK, p.x, 0);
+        const float ry = __shfl_sync(FULL_MASK, p.y, 0);
+        const float rz = __shfl_sync(FULL_MASK, p.z, 0);
+        float dx = wrap_delta(p.x - rx, Lx, iLx);
+        float dy = wrap_delta(p.y - ry, Ly, iLy);
+        float dz = wrap_delta(p.z - rz, Lz, iLz);
+        float mnx = valid ? dx : 3.0e38f, mny = valid ? dy : 3.0e38f, mnz = valid ? dz : 3.0e38f;
+        float mxx = valid ? dx : -3.0e38f, mxy = valid ? dy : -3.0e38f, mxz = valid ? dz : -3.0e38f;
+        for (int o = 16; o > 0; o >>= 1) {
+            mnx = fminf(mnx, __shfl_xor_sync(FULL_MASK, mnx, o));
+            mny = fminf(mny, __shfl_xor_sync(FULL_MASK, mny, o));
+            mnz = fminf(mnz, __shfl_xor_sync(FULL_MASK, mnz, o));
+            mxx = fmaxf(mxx, __shfl_xor_sync(FULL_MASK, mxx, o));
+            mxy = fmaxf(mxy, __shfl_xor_sync(FULL_MASK, mxy, o));
+            mxz = fmaxf(mxz, __shfl_xor_sync(FULL_MASK, mxz, o));
+        }
+        if (lane == 0) {
+            bb_ctr[rb] = make_float4(rx + 0.5f * (mnx + mxx), ry + 0.5f * (mny + mxy), rz + 0.5f * (mnz + mxz), 0.f);
+            // widen by a relative rounding allowance so the box test stays conservative
+            bb_ext[rb] = make_float4(
+                0.5f * (mxx - mnx) * 1.000001f + 1e-6f,
+                0.5f * (mxy - mny) * 1.000001f + 1e-6f,
+                0.5f * (mxz - mnz) * 1.000001f + 1e-6f,
+                0.f);
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Tile list. One CTA (4 warps) per row block rb. For every column block
+// cb >= rb (upper triangle) whose bounding box is within the list radius of
+// rb's box, each column atom is kept when any row atom lies within the list
+// radius (minimum image, 3D). Kept atoms are packed 32 to a tile; the tiles of
+// row block rb occupy the fixed range tile_offset(rb) .. + (CB - rb), which
+// bounds their number. The last CTA to finish turns the per-row-block tile
+// counts into work items of at most `chunk` tiles.
+// (Same selection rule as timemachine/cpp/src/kernels/k_neighborlist.cuh:168-427.)
+// ---------------------------------------------------------------------------
+struct TileArgs {
+    int S;
+    int RB;           // row blocks = column blocks = ceil(S/32)
+    float radius;     // list radius (cutoff + padding + margin)
+    const double *box;
+    const float4 *posw;
+    const float4 *bb_ctr;
+    const float4 *bb_ext;
+    unsigned *tile_cols;   // [capacity*32] slot of each column atom (S = empty)
+    int *rb_ntiles;        // [RB]
+    int4 *items;           // [item_capacity] (rb, first tile, tile count, 0)
+    int chunk;             // tiles per work item
+};
+
+__host__ __device__ __forceinline__ long long tile_offset(int rb, int RB) {
+    return (long long)rb * RB - ((long long)rb * (rb - 1)) / 2;
+}
+
+constexpr int TB_WARPS = 4;
+
+__global__ void __launch_bounds__(TB_WARPS * 32) k_build_tiles(TileArgs a, DevState *state) {
+    if (!state->rebuild || state->error) {
+        return;
+    }
+    __shared__ float4 row_pos[TILE];
+    __shared__ unsigned buf[TB_WARPS][2 * TILE];
+    __shared__ unsigned rem[TB_WARPS * TILE];
+    __shared__ int tile_count;
+    __shared__ int rem_count;
+    __shared__ int is_last;
+
+    const int rb = blockIdx.x;
+    const int lane = threadIdx.x & 31;
+    const int warp = threadIdx.x >> 5;
+    const int S = a.S;
+    const float Lx = (float)a.box[0], Ly = (float)a.box[4], Lz = (float)a.box[8];
+    const float iLx = 1.0f / Lx, iLy = 1.0f / Ly, iLz = 1.0f / Lz;
+    const float r2 = a.radius * a.radius;
+
+    if (threadIdx.x < TILE) {
+        const int s = rb * TILE + threadIdx.x;
+        row_pos[threadIdx.x] = s < S ? a.posw[s] : make_float4(0.f, 0.f, 0.f, 0.f);
+    }
+    if (threadIdx.x == 0) {
+        tile_count = 0;
+        rem_count = 0;
+    }
+    __syncthreads();
+    const int row_n = min(TILE, S - rb * TILE);
+    const float4 rc = a.bb_ctr[rb];
+    const float4 re = a.bb_ext[rb];
+    const long long base_tile = tile_offset(rb, a.RB);
+    const unsigned lane_lt = (1u << lane) - 1;
+
+    int count = 0; // atoms in this warp's buffer
+    for (int cbase = rb + warp * TILE; cbase < a.RB; cbase += TB_WARPS * TILE) {
+        const int cb = cbase + lane;
+        bool pass = false;
+        if (cb < a.RB) {
+            const float4 cc = a.bb_ctr[cb];
+            const float4 ce = a.bb_ext[cb];
+            float dx = fmaxf(0.f, fabsf(wrap_delta(rc.x - cc.x, Lx, iLx)) - re.x - ce.x);
+            float dy = fmaxf(0.f, fabsf(wrap_delta(rc.y - cc.y, Ly, iLy)) - re.y - ce.y);
+            float dz = fmaxf(0.f, fabsf(wrap_delta(rc.z - cc.z, Lz, iLz)) - re.z - ce.z);
+            pass = dx * dx + dy * dy + dz * dz < r2;
+        }
+        unsigned blocks = __ballot_sync(FULL_MASK, pass);
+        while (blocks) {
+            const int cb_sel = cbase + __ffs(blocks) - 1;
+            blocks &= blocks - 1;
+            const int s = cb_sel * TILE + lane;
+            const bool valid = s < S;
+            const float4 pj = valid ? a.posw[s] : make_float4(0.f, 0.f, 0.f, 0.f);
+            bool hit = false;
+            for (int r = 0; r < row_n; r++) {
+                const float4 pi = row_pos[r];
+                const float dx = wrap_delta(pi.x - pj.x, Lx, iLx);
+                const float dy = wrap_delta(pi.y - pj.y, Ly, iLy);
+                const float dz = wrap_delta(pi.z - pj.z, Lz, iLz);
+                hit |= dx * dx + dy * dy + dz * dz < r2;
+                if ((r & 7) == 7 && __all_sync(FULL_MASK, hit || !valid)) {
+                    break;
+                }
+            }
+            hit = hit && valid;
+            const unsigned hmask = __ballot_sync(FULL_MASK, hit);
+            if (hit) {
+                buf[warp][count + __popc(hmask & lane_lt)] = (unsigned)s;
+            }
+            count += __popc(hmask);
+            __syncwarp();
+            if (count >= TILE) {
+                int t = 0;
+                if (lane == 0) {
+                    t = atomicAdd(&tile_count, 1);
+                }
+                t = __shfl_sync(FULL_MASK, t, 0);
+                a.tile_cols[(base_tile + t) * TILE + lane] = buf[warp][lane];
+                __syncwarp();
+                buf[warp][lane] = buf[warp][TILE + lane];
+                __syncwarp();
+                count -= TILE;
+            }
+        }
+    }
+    // merge the partial buffers of the four warps
+    int off = 0;
+    if (lane == 0) {
+        off = atomicAdd(&rem_count, count);
+    }
+    off = __shfl_sync(FULL_MASK, off, 0);
+    if (lane < count) {
+        rem[off + lane] = buf[warp][lane];
+    }
+    __syncthreads();
+    if (warp == 0) {
+        const int n = rem_count;
+        for (int b = 0; b < n; b += TILE) {
+            const int t = tile_count + b / TILE;
+            a.tile_cols[(base_tile + t) * TILE + lane] = b + lane < n ? rem[b + lane] : (unsigned)S;
+        }
+        __syncwarp();
+        if (lane == 0) {
+            const int total = tile_count + (n + TILE - 1) / TILE;
+            a.rb_ntiles[rb] = total;
+            atomicAdd(&state->total_tiles, (unsigned)total);
+        }
+    }
+    // the last CTA to finish builds the work-item list
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const unsigned prev = atomicAdd(&state->done_ctas, 1u);
+        is_last = (prev == (unsigned)a.RB - 1);
+    }
+    __syncthreads();
+    if (!is_last) {
+        return;
+    }
+    __threadfence();
+    __shared__ int carry;
+    __shared__ int wsum[TB_WARPS];
+    if (threadIdx.x == 0) {
+        carry = 0;
+    }
+    __syncthreads();
+    for (int base = 0; base < a.RB; base += blockDim.x) {
+        const int r = base + threadIdx.x;
+        const int nt = r < a.RB ? *((volatile int *)&a.rb_ntiles[r]) : 0;
+        const int ni = (nt + a.chunk - 1) / a.chunk;
+        int incl = ni;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int n = __shfl_up_sync(FULL_MASK, incl, o);
+            if (lane >= o) {
+                incl += n;
+            }
+        }
+        if (lane == 31) {
+            wsum[warp] = incl;
+        }
+        __syncthreads();
+        int wprefix = 0;
+        for (int w = 0; w < warp; w++) {
+            wprefix += wsum[w];
+        }
+        int pos = carry + wprefix + incl - ni;
+        for (int c = 0; c < ni; c++) {
+            const int first = c * a.chunk;
+            a.items[pos + c] = make_int4(r, (int)(tile_offset(r, a.RB) + first), min(a.chunk, nt - first), 0);
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            int tot = 0;
+            for (int w = 0; w < TB_WARPS; w++) {
+                tot += wsum[w];
+            }
+            carry += tot;
+        }
+        __syncthreads();
+    }
+    if (threadIdx.x == 0) {
+        state->n_items = carry;
+        state->rebuilds += 1;
+        state->done_ctas = 0;
+        state->rebuild = 0;
+    }
+}
+
+// Clears the rebuild flag when no neighbour list exists (pair lists only).
+__global__ void k_clear_rebuild(DevState *state) { state->rebuild = 0; }
+
+// ---------------------------------------------------------------------------
+// Pair kernel.
+// ---------------------------------------------------------------------------
+struct Accum {
+    unsigned long long *x, *y, *z;       // du_dx [S] each
+    unsigned long long *q, *sig, *eps;   // du_dp [S] each
+    unsigned long long *u, *dl;          // per-slot energy and du_dl [S]
+    unsigned long long *pq, *psig, *peps; // du_dp of the scaled-pair part (interpolated), else == q/sig/eps
+};
+
+struct PairArgs {
+    int S;
+    const float4 *posw;
+    const float4 *prm;
+    const float4 *dprm;
+    const double *box;
+    double beta;
+    double cutoff;
+    const unsigned *tile_cols;
+    const int4 *items;
+    // scaled pairs (exclusions / 1-4): original atom indices and scales
+    int M;
+    const int *pair_idxs;  // [M,2]
+    const double *scales;  // [M,2]
+    const int *slot_of;    // [N] atom -> slot, nullptr: identity
+    int negated;
+    Accum acc;
+    DevState *state;
+};
+
+__device__ __forceinline__ void red_add(unsigned long long *p, unsigned long long v) { atomicAdd(p, v); }
+
+// One 32x32 tile: lane owns row slot i; the column atoms rotate through the
+// lanes by one position per round (32 rounds), carrying their accumulators.
+// Per-pair arithmetic and validity follow
+// timemachine/cpp/src/kernels/k_nonbonded.cuh:424-546; the column
+// contribution of du_dx is the exact negation of the row contribution
+// (llrint is odd under round-half-even), so it is converted once.
+template <typename Real, bool U, bool DX, bool DL, bool DP, bool INTERP, bool ALCH>
+__device__ __forceinline__ void sweep_tile(
+    const int lane,
+    const unsigned S,
+    const unsigned i,
+    unsigned j,
+    const Real ci_x,
+    const Real ci_y,
+    const Real ci_z,
+    const Real ci_w,
+    const Real qi,
+    const Real sig_i,
+    const Real eps_i,
+    const Real dw_dl_i,
+    const Real dq_dl_i,
+    const Real dsig_dl_i,
+    const Real deps_dl_i,
+    Real cj_x,
+    Real cj_y,
+    Real cj_z,
+    Real cj_w,
+    Real qj,
+    Real sig_j,
+    Real eps_j,
+    Real dw_dl_j,
+    Real dq_dl_j,
+    Real dsig_dl_j,
+    Real deps_dl_j,
+    const Real box_x,
+    const Real box_y,
+    const Real box_z,
+    const Real inv_box_x,
+    const Real inv_box_y,
+    const Real inv_box_z,
+    const Real cutoff_squared,
+    const Real beta,
+    unsigned long long &gi_x,
+    unsigned long long &gi_y,
+    unsigned long long &gi_z,
+    unsigned long long &g_qi,
+    unsigned long long &g_sigi,
+    unsigned long long &g_epsi,
+    unsigned long long &du_dl,
+    unsigned long long &energy,
+    unsigned long long &gj_x,
+    unsigned long long &gj_y,
+    unsigned long long &gj_z,
+    unsigned long long &g_qj,
+    unsigned long long &g_sigj,
+    unsigned long long &g_epsj) {
+    const int src = (lane + 1) & 31;
+#pragma unroll 2
+    for (int round = 0; round < TILE; round++) {
+        Real delta_x = ci_x - cj_x;
+        Real delta_y = ci_y - cj_y;
+        Real delta_z = ci_z - cj_z;
+        delta_x = min_image(delta_x, box_x, inv_box_x);
+        delta_y = min_image(delta_y, box_y, inv_box_y);
+        delta_z = min_image(delta_z, box_z, inv_box_z);
+        Real d2 = delta_x * delta_x + delta_y * delta_y + delta_z * delta_z;
+        Real delta_w;
+        if (ALCH) {
+            delta_w = ci_w - cj_w;
+            d2 += delta_w * delta_w;
+        }
+        const bool valid = i < S && j < S && i < j;
+        if (valid && d2 < cutoff_squared) {
+            Real u;
+            Real prefactor;
+            Real erfc_bd;
+            Real d;
+            Real inv_d;
+            Real inv_d2;
+            electrostatics<Real, U>(1.0, qi, qj, d2, beta, d, inv_d, inv_d2, erfc_bd, prefactor, u);
+            Real real_du_dl = 0;
+            if (eps_i != 0 && eps_j != 0) {
+                Real sig_grad;
+                Real eps_grad;
+                lennard_jones<Real, U>(1.0, eps_i, eps_j, sig_i, sig_j, inv_d, inv_d2, u, prefactor, sig_grad, eps_grad);
+                if (DP) {
+                    const unsigned long long gs = to_fixed(sig_grad, FX_EXPONENT_SIG);
+                    g_sigi += gs;
+                    g_sigj += gs;
+                    g_epsi += to_fixed(eps_grad * eps_j, FX_EXPONENT_EPS);
+                    g_epsj += to_fixed(eps_grad * eps_i, FX_EXPONENT_EPS);
+                }
+                if (DL && ALCH && INTERP) {
+                    real_du_dl += sig_grad * (dsig_dl_i + dsig_dl_j);
+                    Real term = eps_grad * sum_of_products_rn(eps_j, deps_dl_i, eps_i, deps_dl_j);
+                    real_du_dl += term;
+                }
+            }
+            if (DX) {
+                const unsigned long long fx = to_fixed(prefactor * delta_x, FX_EXPONENT);
+                const unsigned long long fy = to_fixed(prefactor * delta_y, FX_EXPONENT);
+                const unsigned long long fz = to_fixed(prefactor * delta_z, FX_EXPONENT);
+                gi_x += fx;
+                gi_y += fy;
+                gi_z += fz;
+                gj_x -= fx;
+                gj_y -= fy;
+                gj_z -= fz;
+            }
+            if (DP) {
+                g_qi += to_fixed(qj * inv_d * erfc_bd, FX_EXPONENT);
+                g_qj += to_fixed(qi * inv_d * erfc_bd, FX_EXPONENT);
+            }
+            if (DL && ALCH) {
+                real_du_dl += delta_w * prefactor * (dw_dl_i - dw_dl_j);
+                if (INTERP) {
+                    real_du_dl += inv_d * erfc_bd * sum_of_products_rn(qj, dq_dl_i, qi, dq_dl_j);
+                }
+                du_dl += to_fixed(real_du_dl, FX_EXPONENT);
+            }
+            if (U) {
+                energy += to_fixed(u, FX_EXPONENT);
+            }
+        }
+        j = __shfl_sync(FULL_MASK, j, src);
+        qj = __shfl_sync(FULL_MASK, qj, src);
+        eps_j = __shfl_sync(FULL_MASK, eps_j, src);
+        sig_j = __shfl_sync(FULL_MASK, sig_j, src);
+        cj_x = __shfl_sync(FULL_MASK, cj_x, src);
+        cj_y = __shfl_sync(FULL_MASK, cj_y, src);
+        cj_z = __shfl_sync(FULL_MASK, cj_z, src);
+        if (ALCH) {
+            cj_w = __shfl_sync(FULL_MASK, cj_w, src);
+            dw_dl_j = __shfl_sync(FULL_MASK, dw_dl_j, src);
+        }
+        if (DX) {
+            gj_x = __shfl_sync(FULL_MASK, gj_x, src);
+            gj_y = __shfl_sync(FULL_MASK, gj_y, src);
+            gj_z = __shfl_sync(FULL_MASK, gj_z, src);
+        }
+        if (DP) {
+            g_qj = __shfl_sync(FULL_MASK, g_qj, src);
+            g_sigj = __shfl_sync(FULL_MASK, g_sigj, src);
+            g_epsj = __shfl_sync(FULL_MASK, g_epsj, src);
+        }
+        if (DL && ALCH && INTERP) {
+            dsig_dl_j = __shfl_sync(FULL_MASK, dsig_dl_j, src);
+            deps_dl_j = __shfl_sync(FULL_MASK, deps_dl_j, src);
+            dq_dl_j = __shfl_sync(FULL_MASK, dq_dl_j, src);
+        }
+    }
+}
+
+// One scaled pair (exclusion / 1-4 correction), arithmetic of
+// timemachine/cpp/src/kernels/k_nonbonded_pair_list.cuh:103-215.
+template <typename Real, bool U, bool DX, bool DL, bool DP, bool INTERP>
+__device__ __forceinline__ void scaled_pair(const PairArgs &a, int pair, const Real box_x, const Real box_y,
+                                            const Real box_z, const Real inv_box_x, const Real inv_box_y,
+                                            const Real inv_box_z, const Real cutoff_squared) {
+    const int atom_i = a.pair_idxs[2 * pair + 0];
+    const int atom_j = a.pair_idxs[2 * pair + 1];
+    const int si = a.slot_of ? a.slot_of[atom_i] : atom_i;
+    const int sj = a.slot_of ? a.slot_of[atom_j] : atom_j;
+    const float4 pwi = a.posw[si];
+    const float4 pwj = a.posw[sj];
+    const float4 pri = a.prm[si];
+    const float4 prj = a.prm[sj];
+    float4 dpi = make_float4(0.f, 0.f, 0.f, 0.f);
+    float4 dpj = dpi;
+    if (INTERP) {
+        dpi = a.dprm[si];
+        dpj = a.dprm[sj];
+    }
+    const Real ci_x = pwi.x, ci_y = pwi.y, ci_z = pwi.z, ci_w = pwi.w;
+    const Real cj_x = pwj.x, cj_y = pwj.y, cj_z = pwj.z, cj_w = pwj.w;
+    const Real qi = pri.x, sig_i = pri.y, eps_i = pri.z, dw_dl_i = pri.w;
+    const Real qj = prj.x, sig_j = prj.y, eps_j = prj.z, dw_dl_j = prj.w;
+    const Real dq_dl_i = dpi.x, dsig_dl_i = dpi.y, deps_dl_i = dpi.z;
+    const Real dq_dl_j = dpj.x, dsig_dl_j = dpj.y, deps_dl_j = dpj.z;
+    const Real beta = a.beta;
+    const Real charge_scale = a.scales[2 * pair + 0];
+    const Real lj_scale = a.scales[2 * pair + 1];
+
+    Real delta_x = ci_x - cj_x;
+    Real delta_y = ci_y - cj_y;
+    Real delta_z = ci_z - cj_z;
+    delta_x = min_image(delta_x, box_x, inv_box_x);
+    delta_y = min_image(delta_y, box_y, inv_box_y);
+    delta_z = min_image(delta_z, box_z, inv_box_z);
+    const Real delta_w = ci_w - cj_w;
+    const Real d2 = delta_x * delta_x + delta_y * delta_y + delta_z * delta_z + delta_w * delta_w;
+
+    const bool is_vanilla = (ci_w == 0 && dq_dl_i == 0 && dsig_dl_i == 0 && deps_dl_i == 0 && cj_w == 0 &&
+                             dq_dl_j == 0 && dsig_dl_j == 0 && deps_dl_j == 0);
+    if (!(d2 < cutoff_squared)) {
+        return;
+    }
+    Real u;
+    Real erfc_bd;
+    Real prefactor;
+    Real d;
+    Real inv_d;
+    Real inv_d2;
+    electrostatics<Real, true>(charge_scale, qi, qj, d2, beta, d, inv_d, inv_d2, erfc_bd, prefactor, u);
+    Real real_du_dl = 0;
+    unsigned long long g_sig = 0, g_epsi = 0, g_epsj = 0;
+    if (eps_i != 0 && eps_j != 0) {
+        Real sig_grad;
+        Real eps_grad;
+        lennard_jones<Real, true>(lj_scale, eps_i, eps_j, sig_i, sig_j, inv_d, inv_d2, u, prefactor, sig_grad, eps_grad);
+        g_sig = to_fixed(sig_grad, FX_EXPONENT_SIG);
+        g_epsi = to_fixed(eps_grad * eps_j, FX_EXPONENT_EPS);
+        g_epsj = to_fixed(eps_grad * eps_i, FX_EXPONENT_EPS);
+        if (INTERP) {
+            real_du_dl += sig_grad * (dsig_dl_i + dsig_dl_j);
+            Real term = eps_grad * sum_of_products_rn(eps_j, deps_dl_i, eps_i, deps_dl_j);
+            real_du_dl += term;
+        }
+    }
+    const bool neg = a.negated != 0;
+    auto acc = [neg](unsigned long long *p, unsigned long long v) { red_add(p, neg ? (0ULL - v) : v); };
+    if (DX) {
+        const unsigned long long fx = to_fixed(prefactor * delta_x, FX_EXPONENT);
+        const unsigned long long fy = to_fixed(prefactor * delta_y, FX_EXPONENT);
+        const unsigned long long fz = to_fixed(prefactor * delta_z, FX_EXPONENT);
+        acc(a.acc.x + si, fx);
+        acc(a.acc.y + si, fy);
+        acc(a.acc.z + si, fz);
+        acc(a.acc.x + sj, 0ULL - fx);
+        acc(a.acc.y + sj, 0ULL - fy);
+        acc(a.acc.z + sj, 0ULL - fz);
+    }
+    if (DP) {
+        acc(a.acc.pq + si, to_fixed(charge_scale * qj * inv_d * erfc_bd, FX_EXPONENT));
+        acc(a.acc.pq + sj, to_fixed(charge_scale * qi * inv_d * erfc_bd, FX_EXPONENT));
+        acc(a.acc.psig + si, g_sig);
+        acc(a.acc.peps + si, g_epsi);
+        acc(a.acc.psig + sj, g_sig);
+        acc(a.acc.peps + sj, g_epsj);
+    }
+    if (DL && !is_vanilla) {
+        real_du_dl += delta_w * prefactor * (dw_dl_i - dw_dl_j);
+        if (INTERP) {
+            real_du_dl += charge_scale * inv_d * erfc_bd * sum_of_products_rn(qj, dq_dl_i, qi, dq_dl_j);
+        }
+        acc(a.acc.dl + si, to_fixed(real_du_dl, FX_EXPONENT));
+    }
+    if (U) {
+        acc(a.acc.u + si, to_fixed(u, FX_EXPONENT));
+    }
+}
+
+template <typename Real, bool U, bool DX, bool DL, bool DP, bool INTERP>
+__global__ void __launch_bounds__(128) k_pair(PairArgs a) {
+    if (a.state->error) {
+        return;
+    }
+    const int lane = threadIdx.x & 31;
+    const Real box_x = a.box[0 * 3 + 0];
+    const Real box_y = a.box[1 * 3 + 1];
+    const Real box_z = a.box[2 * 3 + 2];
+    const Real inv_box_x = 1 / box_x;
+    const Real inv_box_y = 1 / box_y;
+    const Real inv_box_z = 1 / box_z;
+    const Real real_cutoff = static_cast<Real>(a.cutoff);
+    const Real cutoff_squared = real_cutoff * real_cutoff;
+    const Real beta = static_cast<Real>(a.beta);
+    const unsigned S = (unsigned)a.S;
+    const int n_items = a.state->n_items;
+    const int n_total = n_items + (a.M + TILE - 1) / TILE;
+
+    for (;;) {
+        int item = 0;
+        if (lane == 0) {
+            item = atomicAdd(&a.state->next_item, 1);
+        }
+        item = __shfl_sync(FULL_MASK, item, 0);
+        if (item >= n_total) {
+            break;
+        }
+        if (item >= n_items) {
+            const int pair = (item - n_items) * TILE + lane;
+            if (pair < a.M) {
+                scaled_pair<Real, U, DX, DL, DP, INTERP>(a, pair, box_x, box_y, box_z, inv_box_x, inv_box_y,
+                                                         inv_box_z, cutoff_squared);
+            }
+            continue;
+        }
+        const int4 it = a.items[item];
+        const unsigned i = (unsigned)(it.x * TILE + lane);
+        const bool row_ok = i < S;
+        const float4 pwi = row_ok ? a.posw[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+        const float4 pri = row_ok ? a.prm[i] : make_float4(0.f, 0.f, 0.f, 0.f);
+        float4 dpi = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (INTERP && row_ok) {
+            dpi = a.dprm[i];
+        }
+        const bool row_alch = pwi.w != 0.f || (INTERP && (dpi.x != 0.f || dpi.y != 0.f || dpi.z != 0.f));
+
+        unsigned long long gi_x = 0, gi_y = 0, gi_z = 0, g_qi = 0, g_sigi = 0, g_epsi = 0, du_dl = 0, energy = 0;
+        for (int t = 0; t < it.z; t++) {
+            const long long tile = (long long)it.y + t;
+            const unsigned j = a.tile_cols[tile * TILE + lane];
+            const bool col_ok = j < S;
+            const float4 pwj = col_ok ? a.posw[j] : make_float4(0.f, 0.f, 0.f, 0.f);
+            const float4 prj = col_ok ? a.prm[j] : make_float4(0.f, 0.f, 0.f, 0.f);
+            float4 dpj = make_float4(0.f, 0.f, 0.f, 0.f);
+            if (INTERP && col_ok) {
+                dpj = a.dprm[j];
+            }
+            const bool col_alch = pwj.w != 0.f || (INTERP && (dpj.x != 0.f || dpj.y != 0.f || dpj.z != 0.f));
+            const bool alch = __any_sync(FULL_MASK, row_alch || col_alch);
+            unsigned long long gj_x = 0, gj_y = 0, gj_z = 0, g_qj = 0, g_sigj = 0, g_epsj = 0;
+            if (alch) {
+                sweep_tile<Real, U, DX, DL, DP, INTERP, true>(
+                    lane, S, i, j, pwi.x, pwi.y, pwi.z, pwi.w, pri.x, pri.y, pri.z, pri.w, dpi.x, dpi.y, dpi.z, pwj.x,
+                    pwj.y, pwj.z, pwj.w, prj.x, prj.y, prj.z, prj.w, dpj.x, dpj.y, dpj.z, box_x, box_y, box_z,
+                    inv_box_x, inv_box_y, inv_box_z, cutoff_squared, beta, gi_x, gi_y, gi_z, g_qi, g_sigi, g_epsi,
+                    du_dl, energy, gj_x, gj_y, gj_z, g_qj, g_sigj, g_epsj);
+            } else {
+                sweep_tile<Real, U, DX, DL, DP, INTERP, false>(
+                    lane, S, i, j, pwi.x, pwi.y, pwi.z, pwi.w, pri.x, pri.y, pri.z, pri.w, dpi.x, dpi.y, dpi.z, pwj.x,
+                    pwj.y, pwj.z, pwj.w, prj.x, prj.y, prj.z, prj.w, dpj.x, dpj.y, dpj.z, box_x, box_y, box_z,
+                    inv_box_x, inv_box_y, inv_box_z, cutoff_squared, beta, gi_x, gi_y, gi_z, g_qi, g_sigi, g_epsi,
+                    du_dl, energy, gj_x, gj_y, gj_z, g_qj, g_sigj, g_epsj);
+            }
+            if (col_ok) {
+                if (DX) {
+                    red_add(a.acc.x + j, gj_x);
+                    red_add(a.acc.y + j, gj_y);
+                    red_add(a.acc.z + j, gj_z);
+                }
+                if (DP) {
+                    red_add(a.acc.q + j, g_qj);
+                    red_add(a.acc.sig + j, g_sigj);
+                    red_add(a.acc.eps + j, g_epsj);
+                }
+            }
+        }
+        if (row_ok) {
+            if (DX) {
+                red_add(a.acc.x + i, gi_x);
+                red_add(a.acc.y + i, gi_y);
+                red_add(a.acc.z + i, gi_z);
+            }
+            if (DP) {
+                red_add(a.acc.q + i, g_qi);
+                red_add(a.acc.sig + i, g_sigi);
+                red_add(a.acc.eps + i, g_epsi);
+            }
+            if (DL) {
+                red_add(a.acc.dl + i, du_dl);
+            }
+            if (U) {
+                red_add(a.acc.u + i, energy);
+            }
+        }
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Scatter of the slot-ordered accumulators into the caller's outputs (which
+// accumulate, +=), and reset of the accumulators.
+// du_dp of interpolated potentials is split into the lambda=0 and lambda=1
+// halves per potential part, with the rounding of
+// timemachine/cpp/src/kernels/k_lambda_transformer_jit.cuh:100-137.
+// ---------------------------------------------------------------------------
+struct FinalizeArgs {
+    int N;
+    int S;
+    const unsigned *perm;
+    Accum acc;
+    int split_pair_dp; // 1: acc.pq/psig/peps are separate buffers
+    int interpolated;
+    double lambda;
+    unsigned long long *du_dx;
+    unsigned long long *du_dp;
+    unsigned long long *du_dl;
+    unsigned long long *u;
+    const DevState *state;
+};
+
+__device__ __forceinline__ unsigned long long interp_part(double f, unsigned long long v, unsigned long long e) {
+    const double real = static_cast<double>(static_cast<long long>(v)) / e;
+    return static_cast<unsigned long long>(llrint((f * real) * e));
+}
+
+__global__ void k_finalize(FinalizeArgs a) {
+    const bool ok = a.state->error == 0;
+    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < a.S; s += gridDim.x * blockDim.x) {
+        const int atom = a.perm[s];
+        if (a.du_dx) {
+            if (ok) {
+                a.du_dx[3 * (size_t)atom + 0] += a.acc.x[s];
+                a.du_dx[3 * (size_t)atom + 1] += a.acc.y[s];
+                a.du_dx[3 * (size_t)atom + 2] += a.acc.z[s];
+            }
+            a.acc.x[s] = 0;
+            a.acc.y[s] = 0;
+            a.acc.z[s] = 0;
+        }
+        if (a.du_dp) {
+            unsigned long long v0[3] = {a.acc.q[s], a.acc.sig[s], a.acc.eps[s]};
+            unsigned long long v1[3] = {0, 0, 0};
+            a.acc.q[s] = 0;
+            a.acc.sig[s] = 0;
+            a.acc.eps[s] = 0;
+            if (a.split_pair_dp) {
+                v1[0] = a.acc.pq[s];
+                v1[1] = a.acc.psig[s];
+                v1[2] = a.acc.peps[s];
+                a.acc.pq[s] = 0;
+                a.acc.psig[s] = 0;
+                a.acc.peps[s] = 0;
+            }
+            if (ok) {
+                const unsigned long long ex[3] = {FX_EXPONENT, FX_EXPONENT_SIG, FX_EXPONENT_EPS};
+                for (int c = 0; c < 3; c++) {
+                    if (a.interpolated) {
+                        const double f = a.lambda;
+                        unsigned long long lo = interp_part(1 - f, v0[c], ex[c]) + interp_part(1 - f, v1[c], ex[c]);
+                        unsigned long long hi = interp_part(f, v0[c], ex[c]) + interp_part(f, v1[c], ex[c]);
+                        a.du_dp[3 * (size_t)atom + c] += lo;
+                        a.du_dp[3 * ((size_t)a.N + atom) + c] += hi;
+                    } else {
+                        a.du_dp[3 * (size_t)atom + c] += v0[c] + v1[c];
+                    }
+                }
+            }
+        }
+        if (a.u) {
+            if (ok) {
+                a.u[atom] += a.acc.u[s];
+            }
+            a.acc.u[s] = 0;
+        }
+        if (a.du_dl) {
+            if (ok) {
+                a.du_dl[atom] += a.acc.dl[s];
+            }
+            a.acc.dl[s] = 0;
+        }
+    }
+}
+
+} // namespace tmb

@@ -1,0 +1,1006 @@
+// Host side of the B200 nonbonded potential: instance state, launch
+// sequence and the C ABI declared in include/tmnb.h.
+//
+// One class covers the three reference potentials of the path:
+//   AllPairs  (timemachine/cpp/src/nonbonded_all_pairs.cu)
+//   PairList  (timemachine/cpp/src/nonbonded_pair_list.cu, plain or negated)
+//   Nonbonded (timemachine/lib/potentials.py:269-301: AllPairs + negated
+//              PairList of the exclusions), evaluated as ONE pipeline whose
+//              exclusion pairs run inside the pair kernel's launch.
+#include "nb_kernels.cuh"
+#include "tmnb.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <memory>
+#include <set>
+#include <stdexcept>
+#include <string>
+#include <vector>
+
+namespace tmb {
+
+namespace {
+
+thread_local std::string g_last_error;
+
+struct Error : std::runtime_error {
+    tmnb_status status;
+    Error(tmnb_status s, const std::string &msg) : std::runtime_error(msg), status(s) {}
+};
+
+void cuda_check(cudaError_t e, const char *what) {
+    if (e != cudaSuccess) {
+        throw Error(TMNB_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+    }
+}
+#define CK(call) cuda_check((call), #call)
+
+template <typename T> struct DevBuf {
+    T *p = nullptr;
+    size_t n = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf &) = delete;
+    DevBuf &operator=(const DevBuf &) = delete;
+    ~DevBuf() { release(); }
+    void release() {
+        if (p) {
+            cudaFree(p);
+        }
+        p = nullptr;
+        n = 0;
+    }
+    void alloc(size_t count) {
+        release();
+        if (count == 0) {
+            return;
+        }
+        CK(cudaMalloc(&p, count * sizeof(T)));
+        n = count;
+    }
+    void ensure(size_t count) {
+        if (count > n) {
+            alloc(count);
+        }
+    }
+    void upload(const T *h, size_t count) {
+        alloc(count);
+        if (count) {
+            CK(cudaMemcpy(p, h, count * sizeof(T), cudaMemcpyHostToDevice));
+        }
+    }
+    void zero() {
+        if (n) {
+            CK(cudaMemset(p, 0, n * sizeof(T)));
+        }
+    }
+};
+
+int num_sms() {
+    static int sms = -1;
+    if (sms < 0) {
+        int dev = 0;
+        CK(cudaGetDevice(&dev));
+        CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    }
+    return sms;
+}
+
+} // namespace
+
+enum class Kind { AllPairs, PairList, Nonbonded };
+
+typedef void (*pair_kernel_t)(PairArgs);
+
+template <int I> struct PairKernelTable {
+    static constexpr bool U = (I >> 3) & 1;
+    static constexpr bool DX = (I >> 2) & 1;
+    static constexpr bool DL = (I >> 1) & 1;
+    static constexpr bool DP = (I >> 0) & 1;
+};
+
+// kernel index: bit3 U, bit2 DU_DX, bit1 DU_DL, bit0 DU_DP (+16 when interpolated),
+// the same flag order as timemachine/cpp/src/nonbonded_all_pairs.cu:374-379.
+template <int... Is> struct KernelList {
+    static void fill(pair_kernel_t *out, bool interp) {
+        ((out[Is] = interp ? &k_pair<float, PairKernelTable<Is>::U, PairKernelTable<Is>::DX, PairKernelTable<Is>::DL,
+                                     PairKernelTable<Is>::DP, true>
+                           : &k_pair<float, PairKernelTable<Is>::U, PairKernelTable<Is>::DX, PairKernelTable<Is>::DL,
+                                     PairKernelTable<Is>::DP, false>),
+         ...);
+    }
+};
+using AllKernels = KernelList<0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 14, 15>;
+
+class NonbondedPotential {
+  public:
+    NonbondedPotential(
+        Kind kind,
+        int N,
+        const int *plane,
+        const int *offset,
+        double beta,
+        double cutoff,
+        const int *atom_idxs,
+        int K,
+        const int *pair_idxs,
+        const double *scales,
+        int M,
+        bool negated,
+        bool interpolated)
+        : kind_(kind), N_(N), beta_(beta), cutoff_(cutoff), interp_(interpolated), negated_(negated), M_(M) {
+        if (N <= 0) {
+            throw Error(TMNB_ERR_INVALID_ARGUMENT, "N must be positive");
+        }
+        if (!(cutoff > 0)) {
+            throw Error(TMNB_ERR_INVALID_ARGUMENT, "cutoff must be positive");
+        }
+        has_nblist_ = kind != Kind::PairList;
+        S_ = N;
+        std::vector<int> set_atoms;
+        if (kind == Kind::AllPairs && atom_idxs != nullptr) {
+            std::set<int> uniq(atom_idxs, atom_idxs + K);
+            if ((int)uniq.size() != K) {
+                throw Error(TMNB_ERR_INVALID_ARGUMENT, "atom indices must be unique");
+            }
+            if (K <= 0) {
+                throw Error(TMNB_ERR_INVALID_ARGUMENT, "atom indices can't be empty");
+            }
+            for (int a : uniq) {
+                if (a < 0 || a >= N) {
+                    throw Error(TMNB_ERR_INVALID_ARGUMENT, "atom indices must be in [0, N)");
+                }
+            }
+            set_atoms.assign(uniq.begin(), uniq.end()); // the reference keeps a sorted std::set
+            S_ = K;
+        }
+        if (kind != Kind::AllPairs) {
+            for (int i = 0; i < M; i++) {
+                const int src = pair_idxs[2 * i], dst = pair_idxs[2 * i + 1];
+                if (src == dst) {
+                    throw Error(
+                        TMNB_ERR_INVALID_ARGUMENT,
+                        "illegal pair with src == dst: " + std::to_string(src) + ", " + std::to_string(dst));
+                }
+                if (src < 0 || src >= N || dst < 0 || dst >= N) {
+                    throw Error(TMNB_ERR_INVALID_ARGUMENT, "pair index out of range [0, N)");
+                }
+            }
+        } else {
+            M_ = 0;
+        }
+
+        CK(cudaSetDevice(current_device()));
+        plane_.upload(plane, N);
+        offset_.upload(offset, N);
+        if (!set_atoms.empty()) {
+            set_atoms_.upload(set_atoms.data(), set_atoms.size());
+        }
+        if (M_ > 0) {
+            pair_idxs_.upload(pair_idxs, 2 * (size_t)M_);
+            scales_.upload(scales, 2 * (size_t)M_);
+        }
+
+        // slot order: initially the set order
+        std::vector<unsigned> perm(S_);
+        for (int s = 0; s < S_; s++) {
+            perm[s] = set_atoms.empty() ? (unsigned)s : (unsigned)set_atoms[s];
+        }
+        perm_.upload(perm.data(), S_);
+        if (kind == Kind::Nonbonded) {
+            std::vector<int> slot(N);
+            for (int s = 0; s < S_; s++) {
+                slot[perm[s]] = s;
+            }
+            slot_of_.upload(slot.data(), N);
+        }
+
+        posw_.alloc(S_);
+        prm_.alloc(S_);
+        if (interp_) {
+            dprm_.alloc(S_);
+        }
+        split_pair_dp_ = interp_ && kind == Kind::Nonbonded;
+        acc_.alloc((size_t)S_ * (split_pair_dp_ ? 11 : 8));
+        acc_.zero();
+
+        if (has_nblist_) {
+            RB_ = (S_ + TILE - 1) / TILE;
+            nb_x_.alloc(3 * (size_t)N);
+            nb_x_.zero();
+            nb_box_.alloc(9);
+            nb_box_.zero();
+            // cells ~ S/8 atoms-per-cell target: 2^b per axis, b in [2, 6]
+            int b = (int)std::ceil(std::log2(std::cbrt(std::max(1.0, S_ / 8.0))));
+            grid_bits_ = std::min(6, std::max(2, b));
+            keys_.alloc(S_);
+            bin_count_.alloc((size_t)1 << (3 * grid_bits_));
+            bin_count_.zero();
+            bin_cursor_.alloc((size_t)1 << (3 * grid_bits_));
+            bb_ctr_.alloc(RB_);
+            bb_ext_.alloc(RB_);
+            const long long cap_tiles = tile_offset(RB_, RB_);
+            tile_cols_.alloc((size_t)cap_tiles * TILE);
+            rb_ntiles_.alloc(RB_);
+            set_chunk(4);
+        }
+        state_.alloc(1);
+        DevState st{};
+        st.rebuild = has_nblist_ ? 1 : 0;
+        CK(cudaMemcpy(state_.p, &st, sizeof(st), cudaMemcpyHostToDevice));
+        AllKernels::fill(kernels_, interp_);
+        CK(cudaDeviceSynchronize());
+    }
+
+    ~NonbondedPotential() {
+        if (host_stream_) {
+            cudaStreamDestroy(host_stream_);
+        }
+        if (timing_) {
+            cudaEventDestroy(ev_pair_[0]);
+            cudaEventDestroy(ev_pair_[1]);
+        }
+    }
+
+    // CUDA events around every pair-kernel launch (on the launching stream).
+    void enable_timing(bool on) {
+        if (on && !timing_) {
+            CK(cudaEventCreate(&ev_pair_[0]));
+            CK(cudaEventCreate(&ev_pair_[1]));
+        } else if (!on && timing_) {
+            CK(cudaEventDestroy(ev_pair_[0]));
+            CK(cudaEventDestroy(ev_pair_[1]));
+        }
+        timing_ = on;
+        pair_timed_ = false;
+    }
+
+    float last_pair_ms() {
+        if (!timing_ || !pair_timed_) {
+            throw Error(TMNB_ERR_INVALID_ARGUMENT, "no timed pair-kernel launch (enable timing first)");
+        }
+        CK(cudaEventSynchronize(ev_pair_[1]));
+        float ms = 0.f;
+        CK(cudaEventElapsedTime(&ms, ev_pair_[0], ev_pair_[1]));
+        return ms;
+    }
+
+    static int current_device() {
+        int d = 0;
+        CK(cudaGetDevice(&d));
+        return d;
+    }
+
+    void set_chunk(int chunk) {
+        chunk_ = std::max(1, chunk);
+        long long cap = 0;
+        for (int rb = 0; rb < RB_; rb++) {
+            cap += ((RB_ - rb) + chunk_ - 1) / chunk_;
+        }
+        items_.alloc((size_t)std::max(1LL, cap));
+    }
+
+    int num_params() const { return (interp_ ? 2 : 1) * N_ * 3; }
+    int num_atoms() const { return N_; }
+
+    const char *name() const {
+        switch (kind_) {
+        case Kind::AllPairs:
+            return "NonbondedAllPairs";
+        case Kind::PairList:
+            return "NonbondedPairList";
+        default:
+            return "Nonbonded";
+        }
+    }
+
+    void set_padding(double p) {
+        if (!(p >= 0)) {
+            throw Error(TMNB_ERR_INVALID_ARGUMENT, "padding must be non-negative");
+        }
+        padding_ = p;
+    }
+    void disable_hilbert() { hilbert_ = false; }
+
+    void execute_device(
+        int N,
+        int P,
+        const double *d_x,
+        const double *d_p,
+        const double *d_box,
+        double lambda,
+        unsigned long long *d_du_dx,
+        unsigned long long *d_du_dp,
+        unsigned long long *d_du_dl,
+        unsigned long long *d_u,
+        cudaStream_t stream) {
+        if (N != N_) {
+            throw Error(
+                TMNB_ERR_INVALID_ARGUMENT,
+                std::string(name()) + "::execute_device(): expected N == N_, got N=" + std::to_string(N) +
+                    ", N_=" + std::to_string(N_));
+        }
+        const int Mult = interp_ ? 2 : 1;
+        if (P != Mult * N_ * 3) {
+            throw Error(
+                TMNB_ERR_INVALID_ARGUMENT,
+                std::string(name()) + "::execute_device(): expected P == M*N_*3, got P=" + std::to_string(P) +
+                    ", M*N_*3=" + std::to_string(Mult * N_ * 3));
+        }
+        if (!d_x || !d_p || !d_box) {
+            throw Error(TMNB_ERR_INVALID_ARGUMENT, "x, params and box must be non-null");
+        }
+
+        PrepareArgs pa;
+        pa.N = N_;
+        pa.S = S_;
+        pa.x = d_x;
+        pa.p = d_p;
+        pa.box = d_box;
+        pa.lambda = lambda;
+        pa.cutoff = cutoff_;
+        pa.padding = padding_;
+        pa.plane = plane_.p;
+        pa.offset = offset_.p;
+        pa.interpolated = interp_ ? 1 : 0;
+        pa.slots.posw = posw_.p;
+        pa.slots.prm = prm_.p;
+        pa.slots.dprm = dprm_.p;
+
+        const int tpb = 256;
+        const int sgrid = std::max(1, std::min((S_ + tpb - 1) / tpb, 8 * num_sms()));
+        k_check_prepare<<<sgrid, tpb, 0, stream>>>(
+            pa, perm_.p, has_nblist_ ? nb_x_.p : nullptr, nb_box_.p, state_.p);
+        CK(cudaPeekAtLastError());
+
+        if (has_nblist_) {
+            SortArgs sa;
+            sa.N = N_;
+            sa.S = S_;
+            sa.x = d_x;
+            sa.box = d_box;
+            sa.set_atoms = set_atoms_.p;
+            sa.grid_bits = grid_bits_;
+            sa.hilbert = hilbert_ ? 1 : 0;
+            sa.keys = keys_.p;
+            sa.bin_count = bin_count_.p;
+            sa.bin_cursor = bin_cursor_.p;
+            k_bin_keys<<<sgrid, tpb, 0, stream>>>(sa, state_.p);
+            k_bin_scan<<<1, 1024, 0, stream>>>(sa, state_.p);
+            k_bin_scatter<<<sgrid, tpb, 0, stream>>>(sa, pa, perm_.p, slot_of_.p, nb_x_.p, nb_box_.p, state_.p);
+            const int bb_grid = std::max(1, (RB_ * 32 + tpb - 1) / tpb);
+            k_block_bounds<<<bb_grid, tpb, 0, stream>>>(S_, d_box, posw_.p, bb_ctr_.p, bb_ext_.p, state_.p);
+            TileArgs ta;
+            ta.S = S_;
+            ta.RB = RB_;
+            ta.radius = (float)(cutoff_ + padding_ + 1e-5);
+            ta.box = d_box;
+            ta.posw = posw_.p;
+            ta.bb_ctr = bb_ctr_.p;
+            ta.bb_ext = bb_ext_.p;
+            ta.tile_cols = tile_cols_.p;
+            ta.rb_ntiles = rb_ntiles_.p;
+            ta.items = items_.p;
+            ta.chunk = chunk_;
+            k_build_tiles<<<RB_, TB_WARPS * 32, 0, stream>>>(ta, state_.p);
+            CK(cudaPeekAtLastError());
+        }
+
+        const int kidx = (d_du_dp ? 1 : 0) | (d_du_dl ? 2 : 0) | (d_du_dx ? 4 : 0) | (d_u ? 8 : 0);
+        if (kidx != 0) {
+            PairArgs a;
+            a.S = S_;
+            a.posw = posw_.p;
+            a.prm = prm_.p;
+            a.dprm = dprm_.p;
+            a.box = d_box;
+            a.beta = beta_;
+            a.cutoff = cutoff_;
+            a.tile_cols = tile_cols_.p;
+            a.items = items_.p;
+            a.M = M_;
+            a.pair_idxs = pair_idxs_.p;
+            a.scales = scales_.p;
+            a.slot_of = slot_of_.p;
+            a.negated = negated_ ? 1 : 0;
+            a.acc = accum();
+            a.state = state_.p;
+            pair_kernel_t k = kernels_[kidx];
+            if (timing_) {
+                CK(cudaEventRecord(ev_pair_[0], stream));
+            }
+            k<<<pair_grid(k), 128, 0, stream>>>(a);
+            CK(cudaPeekAtLastError());
+            if (timing_) {
+                CK(cudaEventRecord(ev_pair_[1], stream));
+                pair_timed_ = true;
+            }
+
+            FinalizeArgs fa;
+            fa.N = N_;
+            fa.S = S_;
+            fa.perm = perm_.p;
+            fa.acc = accum();
+            fa.split_pair_dp = split_pair_dp_ ? 1 : 0;
+            fa.interpolated = interp_ ? 1 : 0;
+            fa.lambda = lambda;
+            fa.du_dx = d_du_dx;
+            fa.du_dp = d_du_dp;
+            fa.du_dl = d_du_dl;
+            fa.u = d_u;
+            fa.state = state_.p;
+            k_finalize<<<sgrid, tpb, 0, stream>>>(fa);
+            CK(cudaPeekAtLastError());
+        }
+    }
+
+    Accum accum() const {
+        Accum c;
+        unsigned long long *b = acc_.p;
+        const size_t S = S_;
+        c.x = b + 0 * S;
+        c.y = b + 1 * S;
+        c.z = b + 2 * S;
+        c.q = b + 3 * S;
+        c.sig = b + 4 * S;
+        c.eps = b + 5 * S;
+        c.u = b + 6 * S;
+        c.dl = b + 7 * S;
+        if (split_pair_dp_) {
+            c.pq = b + 8 * S;
+            c.psig = b + 9 * S;
+            c.peps = b + 10 * S;
+        } else {
+            c.pq = c.q;
+            c.psig = c.sig;
+            c.peps = c.eps;
+        }
+        return c;
+    }
+
+    int pair_grid(pair_kernel_t k) {
+        int per_sm = 0;
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, 128, 0));
+        return std::max(1, per_sm) * num_sms();
+    }
+
+    // Returns the sticky device error (and clears it).
+    tmnb_status check_device_error(cudaStream_t stream) {
+        CK(cudaStreamSynchronize(stream));
+        DevState st;
+        CK(cudaMemcpy(&st, state_.p, sizeof(st), cudaMemcpyDeviceToHost));
+        if (st.error != 0) {
+            int zero = 0;
+            CK(cudaMemcpy(&state_.p->error, &zero, sizeof(int), cudaMemcpyHostToDevice));
+            if (st.error == DEV_ERR_NONORTHO_BOX) {
+                throw Error(TMNB_ERR_NONORTHO_BOX, "Provided non-ortholinear box, unable to compute nonbonded energy");
+            }
+            throw Error(
+                TMNB_ERR_BOX_TOO_SMALL,
+                "Cutoff with padding is more than half of the box width, neighborlist is no longer reliable");
+        }
+        return TMNB_OK;
+    }
+
+    void stats(cudaStream_t stream, int *n_tiles, int *n_items, int *n_rebuilds) {
+        CK(cudaStreamSynchronize(stream));
+        DevState st;
+        CK(cudaMemcpy(&st, state_.p, sizeof(st), cudaMemcpyDeviceToHost));
+        if (n_tiles) {
+            *n_tiles = (int)st.total_tiles;
+        }
+        if (n_items) {
+            *n_items = st.n_items;
+        }
+        if (n_rebuilds) {
+            *n_rebuilds = st.rebuilds;
+        }
+    }
+
+    cudaStream_t host_stream() {
+        if (!host_stream_) {
+            CK(cudaStreamCreateWithFlags(&host_stream_, cudaStreamNonBlocking));
+        }
+        return host_stream_;
+    }
+
+    void execute_host(
+        int N,
+        int P,
+        const double *h_x,
+        const double *h_p,
+        const double *h_box,
+        double lambda,
+        unsigned long long *h_du_dx,
+        unsigned long long *h_du_dp,
+        unsigned long long *h_du_dl,
+        unsigned long long *h_u) {
+        cudaStream_t s = host_stream();
+        const size_t nx = 3 * (size_t)N;
+        hx_.ensure(nx);
+        hp_.ensure(std::max(1, P));
+        hbox_.ensure(9);
+        CK(cudaMemcpyAsync(hx_.p, h_x, nx * sizeof(double), cudaMemcpyHostToDevice, s));
+        if (P > 0) {
+            CK(cudaMemcpyAsync(hp_.p, h_p, (size_t)P * sizeof(double), cudaMemcpyHostToDevice, s));
+        }
+        CK(cudaMemcpyAsync(hbox_.p, h_box, 9 * sizeof(double), cudaMemcpyHostToDevice, s));
+        unsigned long long *dx = nullptr, *dp = nullptr, *dl = nullptr, *du = nullptr;
+        if (h_du_dx) {
+            hdx_.ensure(nx);
+            dx = hdx_.p;
+            CK(cudaMemsetAsync(dx, 0, nx * sizeof(*dx), s));
+        }
+        if (h_du_dp) {
+            hdp_.ensure(std::max(1, P));
+            dp = hdp_.p;
+            CK(cudaMemsetAsync(dp, 0, (size_t)P * sizeof(*dp), s));
+        }
+        if (h_du_dl) {
+            hdl_.ensure(N);
+            dl = hdl_.p;
+            CK(cudaMemsetAsync(dl, 0, (size_t)N * sizeof(*dl), s));
+        }
+        if (h_u) {
+            hu_.ensure(N);
+            du = hu_.p;
+            CK(cudaMemsetAsync(du, 0, (size_t)N * sizeof(*du), s));
+        }
+        execute_device(N, P, hx_.p, hp_.p, hbox_.p, lambda, dx, dp, dl, du, s);
+        if (h_du_dx) {
+            CK(cudaMemcpyAsync(h_du_dx, dx, nx * sizeof(*dx), cudaMemcpyDeviceToHost, s));
+        }
+        if (h_du_dp) {
+            CK(cudaMemcpyAsync(h_du_dp, dp, (size_t)P * sizeof(*dp), cudaMemcpyDeviceToHost, s));
+        }
+        if (h_du_dl) {
+            CK(cudaMemcpyAsync(h_du_dl, dl, (size_t)N * sizeof(*dl), cudaMemcpyDeviceToHost, s));
+        }
+        if (h_u) {
+            CK(cudaMemcpyAsync(h_u, du, (size_t)N * sizeof(*du), cudaMemcpyDeviceToHost, s));
+        }
+        check_device_error(s);
+    }
+
+    void du_dp_fixed_to_float(int N, int P, const unsigned long long *du_dp, double *out) const {
+        const int tuples = P / 3;
+        for (int i = 0; i < tuples; i++) {
+            out[3 * i + 0] = (double)(long long)du_dp[3 * i + 0] / (double)FX_EXPONENT;
+            out[3 * i + 1] = (double)(long long)du_dp[3 * i + 1] / (double)FX_EXPONENT_SIG;
+            out[3 * i + 2] = (double)(long long)du_dp[3 * i + 2] / (double)FX_EXPONENT_EPS;
+        }
+        (void)N;
+    }
+
+  private:
+    Kind kind_;
+    int N_;
+    int S_ = 0;
+    double beta_;
+    double cutoff_;
+    double padding_ = 0.1;
+    bool interp_;
+    bool negated_;
+    bool hilbert_ = true;
+    bool has_nblist_ = false;
+    bool split_pair_dp_ = false;
+    int M_;
+    int RB_ = 0;
+    int grid_bits_ = 4;
+    int chunk_ = 4;
+
+    DevBuf<int> plane_, offset_, set_atoms_, pair_idxs_, slot_of_;
+    DevBuf<double> scales_;
+    DevBuf<unsigned> perm_;
+    DevBuf<float4> posw_, prm_, dprm_;
+    DevBuf<unsigned long long> acc_;
+    DevBuf<double> nb_x_, nb_box_;
+    DevBuf<unsigned> keys_;
+    DevBuf<int> bin_count_, bin_cursor_;
+    DevBuf<float4> bb_ctr_, bb_ext_;
+    DevBuf<unsigned> tile_cols_;
+    DevBuf<int> rb_ntiles_;
+    DevBuf<int4> items_;
+    DevBuf<DevState> state_;
+    pair_kernel_t kernels_[16];
+
+    // pair-kernel timing
+    bool timing_ = false;
+    bool pair_timed_ = false;
+    cudaEvent_t ev_pair_[2] = {nullptr, nullptr};
+
+    // execute_host staging
+    cudaStream_t host_stream_ = nullptr;
+    DevBuf<double> hx_, hp_, hbox_;
+    DevBuf<unsigned long long> hdx_, hdp_, hdl_, hu_;
+};
+
+} // namespace tmb
+
+struct tmnb_potential {
+    std::unique_ptr<tmb::NonbondedPotential> impl;
+};
+
+namespace tmb {
+
+// FP32 FMA throughput probe: 8 independent FMA chains per thread, enough
+// resident warps to fill every SM; the denominator of the pair kernel's
+// FP32 roofline.
+__global__ void __launch_bounds__(256) k_fp32_peak(float *out, int iters, float a, float b) {
+    float v0 = threadIdx.x * 1e-7f, v1 = v0 + 1e-7f, v2 = v0 + 2e-7f, v3 = v0 + 3e-7f;
+    float v4 = v0 + 4e-7f, v5 = v0 + 5e-7f, v6 = v0 + 6e-7f, v7 = v0 + 7e-7f;
+    for (int i = 0; i < iters; i++) {
+#pragma unroll
+        for (int k = 0; k < 16; k++) {
+            v0 = fmaf(v0, a, b);
+            v1 = fmaf(v1, a, b);
+            v2 = fmaf(v2, a, b);
+            v3 = fmaf(v3, a, b);
+            v4 = fmaf(v4, a, b);
+            v5 = fmaf(v5, a, b);
+            v6 = fmaf(v6, a, b);
+            v7 = fmaf(v7, a, b);
+        }
+    }
+    const float s = v0 + v1 + v2 + v3 + v4 + v5 + v6 + v7;
+    if (s == 1.2345f) {
+        out[blockIdx.x * blockDim.x + threadIdx.x] = s; // practically never; keeps the chains live
+    }
+}
+
+double fp32_peak_tflops() {
+    const int sms = num_sms();
+    const int blocks = sms * 8;
+    const int threads = 256;
+    const int iters = 4096;
+    DevBuf<float> out;
+    out.alloc((size_t)blocks * threads);
+    cudaEvent_t e0, e1;
+    CK(cudaEventCreate(&e0));
+    CK(cudaEventCreate(&e1));
+    k_fp32_peak<<<blocks, threads>>>(out.p, 16, 0.999f, 1e-6f); // warm-up
+    CK(cudaEventRecord(e0));
+    k_fp32_peak<<<blocks, threads>>>(out.p, iters, 0.999f, 1e-6f);
+    CK(cudaEventRecord(e1));
+    CK(cudaEventSynchronize(e1));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, e0, e1));
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    const double flops = 2.0 * 8 * 16 * (double)iters * blocks * threads;
+    return flops / (ms * 1e-3) / 1e12;
+}
+
+} // namespace tmb
+
+namespace {
+
+template <typename F> tmnb_status guarded(F &&f) {
+    try {
+        f();
+        return TMNB_OK;
+    } catch (const tmb::Error &e) {
+        tmb::g_last_error = e.what();
+        return e.status;
+    } catch (const std::bad_alloc &) {
+        tmb::g_last_error = "host allocation failed";
+        return TMNB_ERR_INTERNAL;
+    } catch (const std::exception &e) {
+        tmb::g_last_error = e.what();
+        return TMNB_ERR_INTERNAL;
+    }
+}
+
+tmnb_status check_handle(const tmnb_potential *p) {
+    if (p == nullptr || !p->impl) {
+        tmb::g_last_error = "null potential handle";
+        return TMNB_ERR_INVALID_ARGUMENT;
+    }
+    return TMNB_OK;
+}
+
+tmnb_status check_precision(int precision) {
+    if (precision != 32) {
+        tmb::g_last_error = "only precision=32 (FP32 pair arithmetic) is built";
+        return TMNB_ERR_UNSUPPORTED;
+    }
+    return TMNB_OK;
+}
+
+} // namespace
+
+extern "C" {
+
+const char *tmnb_last_error(void) { return tmb::g_last_error.c_str(); }
+
+const char *tmnb_version(void) { return "tmnb 0.1 sm_100a"; }
+
+tmnb_status tmnb_all_pairs_create(
+    int N,
+    const int32_t *lambda_plane_idxs,
+    const int32_t *lambda_offset_idxs,
+    double beta,
+    double cutoff,
+    const int32_t *atom_idxs,
+    int K,
+    int interpolated,
+    int precision,
+    tmnb_potential **out) {
+    if (tmnb_status s = check_precision(precision)) {
+        return s;
+    }
+    if (!out || !lambda_plane_idxs || !lambda_offset_idxs) {
+        tmb::g_last_error = "null argument";
+        return TMNB_ERR_INVALID_ARGUMENT;
+    }
+    return guarded([&] {
+        auto h = std::make_unique<tmnb_potential>();
+        h->impl = std::make_unique<tmb::NonbondedPotential>(
+            tmb::Kind::AllPairs,
+            N,
+            lambda_plane_idxs,
+            lambda_offset_idxs,
+            beta,
+            cutoff,
+            atom_idxs,
+            K,
+            nullptr,
+            nullptr,
+            0,
+            false,
+            interpolated != 0);
+        *out = h.release();
+    });
+}
+
+tmnb_status tmnb_pair_list_create(
+    int N,
+    const int32_t *pair_idxs,
+    const double *scales,
+    int M,
+    const int32_t *lambda_plane_idxs,
+    const int32_t *lambda_offset_idxs,
+    double beta,
+    double cutoff,
+    int negated,
+    int interpolated,
+    int precision,
+    tmnb_potential **out) {
+    if (tmnb_status s = check_precision(precision)) {
+        return s;
+    }
+    if (!out || !lambda_plane_idxs || !lambda_offset_idxs || (M > 0 && (!pair_idxs || !scales)) || M < 0) {
+        tmb::g_last_error = "null argument";
+        return TMNB_ERR_INVALID_ARGUMENT;
+    }
+    return guarded([&] {
+        auto h = std::make_unique<tmnb_potential>();
+        h->impl = std::make_unique<tmb::NonbondedPotential>(
+            tmb::Kind::PairList,
+            N,
+            lambda_plane_idxs,
+            lambda_offset_idxs,
+            beta,
+            cutoff,
+            nullptr,
+            0,
+            pair_idxs,
+            scales,
+            M,
+            negated != 0,
+            interpolated != 0);
+        *out = h.release();
+    });
+}
+
+tmnb_status tmnb_nonbonded_create(
+    int N,
+    const int32_t *exclusion_idxs,
+    const double *scales,
+    int M,
+    const int32_t *lambda_plane_idxs,
+    const int32_t *lambda_offset_idxs,
+    double beta,
+    double cutoff,
+    int interpolated,
+    int precision,
+    tmnb_potential **out) {
+    if (tmnb_status s = check_precision(precision)) {
+        return s;
+    }
+    if (!out || !lambda_plane_idxs || !lambda_offset_idxs || (M > 0 && (!exclusion_idxs || !scales)) || M < 0) {
+        tmb::g_last_error = "null argument";
+        return TMNB_ERR_INVALID_ARGUMENT;
+    }
+    return guarded([&] {
+        auto h = std::make_unique<tmnb_potential>();
+        h->impl = std::make_unique<tmb::NonbondedPotential>(
+            tmb::Kind::Nonbonded,
+            N,
+            lambda_plane_idxs,
+            lambda_offset_idxs,
+            beta,
+            cutoff,
+            nullptr,
+            0,
+            exclusion_idxs,
+            scales,
+            M,
+            true,
+            interpolated != 0);
+        *out = h.release();
+    });
+}
+
+tmnb_status tmnb_potential_destroy(tmnb_potential *pot) {
+    if (pot == nullptr) {
+        return TMNB_OK;
+    }
+    return guarded([&] { delete pot; });
+}
+
+tmnb_status tmnb_potential_execute_device(
+    tmnb_potential *pot,
+    int N,
+    int P,
+    const double *d_x,
+    const double *d_p,
+    const double *d_box,
+    double lambda,
+    unsigned long long *d_du_dx,
+    unsigned long long *d_du_dp,
+    unsigned long long *d_du_dl,
+    unsigned long long *d_u,
+    void *stream) {
+    if (tmnb_status s = check_handle(pot)) {
+        return s;
+    }
+    return guarded([&] {
+        pot->impl->execute_device(
+            N, P, d_x, d_p, d_box, lambda, d_du_dx, d_du_dp, d_du_dl, d_u, static_cast<cudaStream_t>(stream));
+    });
+}
+
+tmnb_status tmnb_potential_execute_host(
+    tmnb_potential *pot,
+    int N,
+    int P,
+    const double *h_x,
+    const double *h_p,
+    const double *h_box,
+    double lambda,
+    unsigned long long *h_du_dx,
+    unsigned long long *h_du_dp,
+    unsigned long long *h_du_dl,
+    unsigned long long *h_u) {
+    if (tmnb_status s = check_handle(pot)) {
+        return s;
+    }
+    if (!h_x || !h_box || (P > 0 && !h_p)) {
+        tmb::g_last_error = "null argument";
+        return TMNB_ERR_INVALID_ARGUMENT;
+    }
+    return guarded([&] { pot->impl->execute_host(N, P, h_x, h_p, h_box, lambda, h_du_dx, h_du_dp, h_du_dl, h_u); });
+}
+
+tmnb_status tmnb_potential_execute_batch_host(
+    tmnb_potential *pot,
+    int coord_batches,
+    int N,
+    int param_batches,
+    int P,
+    int lambda_batches,
+    const double *h_x,
+    const double *h_p,
+    const double *h_boxes,
+    const double *h_lambdas,
+    unsigned long long *h_du_dx,
+    unsigned long long *h_du_dp,
+    unsigned long long *h_du_dl,
+    unsigned long long *h_u) {
+    if (tmnb_status s = check_handle(pot)) {
+        return s;
+    }
+    if (coord_batches <= 0 || param_batches <= 0 || lambda_batches <= 0 || !h_x || !h_p || !h_boxes || !h_lambdas) {
+        tmb::g_last_error = "invalid batch arguments";
+        return TMNB_ERR_INVALID_ARGUMENT;
+    }
+    return guarded([&] {
+        size_t e = 0;
+        for (int c = 0; c < coord_batches; c++) {
+            for (int p = 0; p < param_batches; p++) {
+                for (int l = 0; l < lambda_batches; l++, e++) {
+                    pot->impl->execute_host(
+                        N,
+                        P,
+                        h_x + (size_t)c * N * 3,
+                        h_p + (size_t)p * P,
+                        h_boxes + (size_t)c * 9,
+                        h_lambdas[l],
+                        h_du_dx ? h_du_dx + e * N * 3 : nullptr,
+                        h_du_dp ? h_du_dp + e * P : nullptr,
+                        h_du_dl ? h_du_dl + e * N : nullptr,
+                        h_u ? h_u + e * N : nullptr);
+                }
+            }
+        }
+    });
+}
+
+tmnb_status tmnb_potential_du_dp_fixed_to_float(
+    tmnb_potential *pot, int N, int P, const unsigned long long *du_dp, double *du_dp_float) {
+    if (tmnb_status s = check_handle(pot)) {
+        return s;
+    }
+    if (!du_dp || !du_dp_float) {
+        tmb::g_last_error = "null argument";
+        return TMNB_ERR_INVALID_ARGUMENT;
+    }
+    return guarded([&] { pot->impl->du_dp_fixed_to_float(N, P, du_dp, du_dp_float); });
+}
+
+tmnb_status tmnb_potential_set_nblist_padding(tmnb_potential *pot, double padding) {
+    if (tmnb_status s = check_handle(pot)) {
+        return s;
+    }
+    return guarded([&] { pot->impl->set_padding(padding); });
+}
+
+tmnb_status tmnb_potential_disable_hilbert_sort(tmnb_potential *pot) {
+    if (tmnb_status s = check_handle(pot)) {
+        return s;
+    }
+    return guarded([&] { pot->impl->disable_hilbert(); });
+}
+
+tmnb_status tmnb_potential_check_device_error(tmnb_potential *pot, void *stream) {
+    if (tmnb_status s = check_handle(pot)) {
+        return s;
+    }
+    return guarded([&] { pot->impl->check_device_error(static_cast<cudaStream_t>(stream)); });
+}
+
+tmnb_status tmnb_potential_nblist_stats(
+    tmnb_potential *pot, void *stream, int *n_tiles, int *n_items, int *n_rebuilds) {
+    if (tmnb_status s = check_handle(pot)) {
+        return s;
+    }
+    return guarded([&] { pot->impl->stats(static_cast<cudaStream_t>(stream), n_tiles, n_items, n_rebuilds); });
+}
+
+tmnb_status tmnb_potential_enable_timing(tmnb_potential *pot, int on) {
+    if (tmnb_status s = check_handle(pot)) {
+        return s;
+    }
+    return guarded([&] { pot->impl->enable_timing(on != 0); });
+}
+
+tmnb_status tmnb_potential_last_pair_kernel_ms(tmnb_potential *pot, float *ms) {
+    if (tmnb_status s = check_handle(pot)) {
+        return s;
+    }
+    if (!ms) {
+        tmb::g_last_error = "null argument";
+        return TMNB_ERR_INVALID_ARGUMENT;
+    }
+    return guarded([&] { *ms = pot->impl->last_pair_ms(); });
+}
+
+tmnb_status tmnb_probe_fp32_peak(double *tflops) {
+    if (!tflops) {
+        tmb::g_last_error = "null argument";
+        return TMNB_ERR_INVALID_ARGUMENT;
+    }
+    return guarded([&] { *tflops = tmb::fp32_peak_tflops(); });
+}
+
+int tmnb_potential_num_params(const tmnb_potential *pot) {
+    return (pot && pot->impl) ? pot->impl->num_params() : -1;
+}
+
+int tmnb_potential_num_atoms(const tmnb_potential *pot) {
+    return (pot && pot->impl) ? pot->impl->num_atoms() : -1;
+}
+
+} // extern "C"

@@ -1,0 +1,495 @@
+"""Nonbonded potentials with timemachine's Python surface, on the B200 kernels.
+
+Mirrors timemachine/lib/potentials.py (classes, constructor arguments,
+bind/unbound_impl/bound_impl) and the methods that
+timemachine/cpp/src/wrap_kernels.cpp:334-723 binds on the implementation
+objects (execute, execute_selective, execute_selective_batch, execute_du_dx,
+BoundPotential.execute / execute_fixed, disable_hilbert_sort,
+set_nblist_padding). Results are float64 numpy arrays decoded from the
+int64 fixed-point accumulators exactly as the reference decodes them.
+
+Device-resident use goes through ``Potential.execute_device`` on torch CUDA
+tensors (no host copies, no host synchronisation).
+"""
+
+import ctypes
+import itertools
+
+import numpy as np
+
+from . import _lib
+from .fixed_point import FIXED_EXPONENT, fixed_to_float, du_dp_fixed_to_float, sum_fixed
+
+__all__ = [
+    "CustomOpWrapper",
+    "Nonbonded",
+    "NonbondedInterpolated",
+    "NonbondedAllPairs",
+    "NonbondedAllPairsInterpolated",
+    "NonbondedPairList",
+    "NonbondedPairListNegated",
+    "NonbondedPairListInterpolated",
+    "NonbondedPairListNegatedInterpolated",
+    "Potential",
+    "BoundPotential",
+]
+
+
+def _ptr(a):
+    """Address of a contiguous numpy array (or None)."""
+    if a is None:
+        return None
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+def _precision_bits(precision):
+    if precision == np.float64:
+        return 64
+    return 32
+
+
+class Potential:
+    """Unbound implementation: one native handle (the reference's custom_ops.Potential)."""
+
+    def __init__(self, handle, name, interpolated):
+        self._h = handle
+        self._name = name
+        self.interpolated = interpolated
+        self._lib = _lib.lib()
+
+    def __del__(self):
+        h, self._h = getattr(self, "_h", None), None
+        if h:
+            try:
+                self._lib.tmnb_potential_destroy(h)
+            except Exception:
+                pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    # -- configuration (timemachine/cpp/src/nonbonded_all_pairs.cu:180-187) --
+    def set_nblist_padding(self, padding):
+        _lib.check(self._lib.tmnb_potential_set_nblist_padding(self._h, float(padding)))
+
+    def disable_hilbert_sort(self):
+        _lib.check(self._lib.tmnb_potential_disable_hilbert_sort(self._h))
+
+    def num_params(self):
+        return self._lib.tmnb_potential_num_params(self._h)
+
+    def num_atoms(self):
+        return self._lib.tmnb_potential_num_atoms(self._h)
+
+    # -- host entry points ---------------------------------------------------
+    def _execute_fixed(self, coords, params, box, lam, du_dx, du_dp, du_dl, u):
+        coords = np.ascontiguousarray(coords, dtype=np.float64)
+        params = np.ascontiguousarray(params, dtype=np.float64)
+        box = np.ascontiguousarray(box, dtype=np.float64)
+        if coords.ndim != 2 or coords.shape[1] != 3:
+            raise RuntimeError("coords must have shape (N, 3)")
+        if box.size != 9:
+            raise RuntimeError("box must have shape (3, 3)")
+        N = coords.shape[0]
+        P = params.size
+        out_dx = np.empty((N, 3), dtype=np.uint64) if du_dx else None
+        out_dp = np.empty(P, dtype=np.uint64) if du_dp else None
+        out_dl = np.empty(N, dtype=np.uint64) if du_dl else None
+        out_u = np.empty(N, dtype=np.uint64) if u else None
+        _lib.check(
+            self._lib.tmnb_potential_execute_host(
+                self._h,
+                N,
+                P,
+                _ptr(coords),
+                _ptr(params),
+                _ptr(box),
+                float(lam),
+                _ptr(out_dx),
+                _ptr(out_dp),
+                _ptr(out_dl),
+                _ptr(out_u),
+            )
+        )
+        return out_dx, out_dp, out_dl, out_u
+
+    def execute_selective(self, coords, params, box, lam, compute_du_dx, compute_du_dp, compute_du_dl, compute_u):
+        """timemachine/cpp/src/wrap_kernels.cpp:552-625: tuple with None for outputs not requested."""
+        params = np.asarray(params, dtype=np.float64)
+        fdx, fdp, fdl, fu = self._execute_fixed(
+            coords, params, box, lam, compute_du_dx, compute_du_dp, compute_du_dl, compute_u
+        )
+        du_dx = fixed_to_float(fdx) if compute_du_dx else None
+        du_dp = du_dp_fixed_to_float(fdp).reshape(params.shape) if compute_du_dp else None
+        du_dl = fixed_to_float(sum_fixed(fdl)) if compute_du_dl else None
+        u = fixed_to_float(sum_fixed(fu)) if compute_u else None
+        return du_dx, du_dp, du_dl, u
+
+    def execute(self, coords, params, box, lam):
+        """timemachine/cpp/src/wrap_kernels.cpp:339-380: (du_dx, du_dp, du_dl, u)."""
+        return self.execute_selective(coords, params, box, lam, True, True, True, True)
+
+    def execute_du_dx(self, coords, params, box, lam):
+        """timemachine/cpp/src/wrap_kernels.cpp:626-651."""
+        return self.execute_selective(coords, params, box, lam, True, False, False, False)[0]
+
+    def execute_selective_batch(
+        self, coords, params, boxes, lambdas, compute_du_dx, compute_du_dp, compute_du_dl, compute_u
+    ):
+        """timemachine/cpp/src/wrap_kernels.cpp:381-551: every (coords, params, lambda) combination."""
+        coords = np.ascontiguousarray(coords, dtype=np.float64)
+        params = np.ascontiguousarray(params, dtype=np.float64)
+        boxes = np.ascontiguousarray(boxes, dtype=np.float64)
+        lambdas = np.ascontiguousarray(np.atleast_1d(lambdas), dtype=np.float64)
+        if coords.ndim != 3 and boxes.ndim != 3:
+            raise RuntimeError("coords and boxes must have 3 dimensions")
+        if coords.shape[0] != boxes.shape[0]:
+            raise RuntimeError("number of batches of coords and boxes don't match")
+        if params.ndim < 2:
+            raise RuntimeError("parameters must have at least 2 dimensions")
+        if lambdas.size < 1:
+            raise RuntimeError("lambdas must have at least 1 value")
+        C, N, _ = coords.shape
+        Pb = params.shape[0]
+        P = params.size // Pb
+        L = lambdas.size
+        E = C * Pb * L
+        out_dx = np.empty((E, N, 3), dtype=np.uint64) if compute_du_dx else None
+        out_dp = np.empty((E, P), dtype=np.uint64) if compute_du_dp else None
+        out_dl = np.empty((E, N), dtype=np.uint64) if compute_du_dl else None
+        out_u = np.empty((E, N), dtype=np.uint64) if compute_u else None
+        _lib.check(
+            self._lib.tmnb_potential_execute_batch_host(
+                self._h,
+                C,
+                N,
+                Pb,
+                P,
+                L,
+                _ptr(coords),
+                _ptr(params),
+                _ptr(boxes),
+                _ptr(lambdas),
+                _ptr(out_dx),
+                _ptr(out_dp),
+                _ptr(out_dl),
+                _ptr(out_u),
+            )
+        )
+        res = [None, None, None, None]
+        if compute_du_dx:
+            res[0] = fixed_to_float(out_dx).reshape(C, Pb, L, N, 3)
+        if compute_du_dp:
+            res[1] = du_dp_fixed_to_float(out_dp).reshape((C, Pb, L) + params.shape[1:])
+        if compute_du_dl:
+            res[2] = np.array([fixed_to_float(sum_fixed(r)) for r in out_dl]).reshape(C, Pb, L)
+        if compute_u:
+            res[3] = np.array([fixed_to_float(sum_fixed(r)) for r in out_u]).reshape(C, Pb, L)
+        return tuple(res)
+
+    def du_dp_fixed_to_float(self, N, P, du_dp):
+        return du_dp_fixed_to_float(np.asarray(du_dp, dtype=np.uint64))
+
+    # -- device entry point (torch tensors) -----------------------------------
+    def execute_device(self, x, p, box, lam, du_dx=None, du_dp=None, du_dl=None, u=None, stream=None):
+        """Accumulate into int64 device tensors (the C-ABI device contract).
+
+        x [N,3] f64, p [P] f64, box [3,3] f64 on the same CUDA device; outputs are
+        int64 tensors that the caller zeroes. ``stream``: torch.cuda.Stream, a raw
+        cudaStream_t (int), or None for torch's current stream.
+        """
+        import torch
+
+        def addr(t):
+            if t is None:
+                return None
+            if not t.is_contiguous():
+                raise RuntimeError("device tensors must be contiguous")
+            return ctypes.c_void_p(t.data_ptr())
+
+        if stream is None:
+            stream = torch.cuda.current_stream(x.device).cuda_stream
+        elif hasattr(stream, "cuda_stream"):
+            stream = stream.cuda_stream
+        _lib.check(
+            self._lib.tmnb_potential_execute_device(
+                self._h,
+                x.shape[0],
+                p.numel(),
+                addr(x),
+                addr(p),
+                addr(box),
+                float(lam),
+                addr(du_dx),
+                addr(du_dp),
+                addr(du_dl),
+                addr(u),
+                ctypes.c_void_p(stream),
+            )
+        )
+
+    def check_device_error(self, stream=None):
+        import torch
+
+        if stream is None:
+            stream = torch.cuda.current_stream().cuda_stream
+        elif hasattr(stream, "cuda_stream"):
+            stream = stream.cuda_stream
+        _lib.check(self._lib.tmnb_potential_check_device_error(self._h, ctypes.c_void_p(stream)))
+
+    def nblist_stats(self, stream=None):
+        """(tiles, work items, rebuilds) of the last neighbour-list build (synchronises)."""
+        t, i, r = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
+        s = 0
+        if stream is not None:
+            s = stream.cuda_stream if hasattr(stream, "cuda_stream") else stream
+        _lib.check(
+            self._lib.tmnb_potential_nblist_stats(
+                self._h, ctypes.c_void_p(s), ctypes.byref(t), ctypes.byref(i), ctypes.byref(r)
+            )
+        )
+        return t.value, i.value, r.value
+
+
+class BoundPotential:
+    """timemachine/cpp/src/bound_potential.cu + wrap_kernels.cpp:654-723."""
+
+    def __init__(self, potential, params):
+        self.potential = potential
+        self.params = np.ascontiguousarray(params, dtype=np.float64)
+
+    def get_potential(self):
+        return self.potential
+
+    def size(self):
+        return self.params.size
+
+    def execute(self, coords, box, lam):
+        du_dx, _, du_dl, u = self.potential.execute_selective(coords, self.params, box, lam, True, False, True, True)
+        return du_dx, du_dl, u
+
+    def execute_fixed(self, coords, box, lam):
+        _, _, _, fu = self.potential._execute_fixed(coords, self.params, box, lam, True, False, True, True)
+        return np.array([sum_fixed(fu)], dtype=np.uint64)
+
+
+class CustomOpWrapper:
+    """timemachine/lib/potentials.py:13-39."""
+
+    def __init__(self, *args):
+        self.args = list(args)
+        self.params = None
+
+    def bind(self, params):
+        self.params = params
+        return self
+
+    def unbound_impl(self, precision):
+        raise NotImplementedError
+
+    def bound_impl(self, precision):
+        if self.params is None:
+            raise ValueError("This op has not been bound to parameters.")
+        return BoundPotential(self.unbound_impl(precision), self.params)
+
+
+def _check_precision(precision):
+    if _precision_bits(precision) != 32:
+        raise RuntimeError("only float32 pair arithmetic is built on this backend (precision=np.float32)")
+
+
+def _plane_offset(plane, offset):
+    plane = np.ascontiguousarray(plane, dtype=np.int32)
+    offset = np.ascontiguousarray(offset, dtype=np.int32)
+    if plane.shape != offset.shape:
+        raise RuntimeError("lambda offset idxs and plane idxs need to be equivalent")
+    return plane, offset
+
+
+def _pairs_scales(pair_idxs, scales):
+    pair_idxs = np.ascontiguousarray(pair_idxs, dtype=np.int32)
+    scales = np.ascontiguousarray(scales, dtype=np.float64)
+    if pair_idxs.size % 2 != 0:
+        raise RuntimeError(f"pair_idxs.size() must be even, but got {pair_idxs.size}")
+    M = pair_idxs.size // 2
+    if scales.size // 2 != M:
+        raise RuntimeError(f"expected same number of pairs and scale tuples, but got {M} != {scales.size // 2}")
+    return pair_idxs.reshape(-1, 2), scales.reshape(-1, 2), M
+
+
+class NonbondedAllPairs(CustomOpWrapper):
+    """args: (lambda_plane_idxs, lambda_offset_idxs, beta, cutoff[, atom_idxs])."""
+
+    _interpolated = False
+
+    def unbound_impl(self, precision):
+        _check_precision(precision)
+        plane, offset = _plane_offset(self.args[0], self.args[1])
+        beta, cutoff = float(self.args[2]), float(self.args[3])
+        atom_idxs = self.args[4] if len(self.args) > 4 else None
+        N = plane.size
+        aidx, K = None, 0
+        if atom_idxs is not None:
+            aidx = np.ascontiguousarray(atom_idxs, dtype=np.int32)
+            K = aidx.size
+            if len(set(aidx.tolist())) != K:
+                raise RuntimeError("atom indices must be unique")
+        h = ctypes.c_void_p()
+        lib = _lib.lib()
+        _lib.check(
+            lib.tmnb_all_pairs_create(
+                N,
+                _ptr(plane),
+                _ptr(offset),
+                beta,
+                cutoff,
+                _ptr(aidx),
+                K,
+                1 if self._interpolated else 0,
+                32,
+                ctypes.byref(h),
+            )
+        )
+        return Potential(h, "NonbondedAllPairs", self._interpolated)
+
+
+class NonbondedAllPairsInterpolated(NonbondedAllPairs):
+    _interpolated = True
+
+
+class NonbondedPairList(CustomOpWrapper):
+    """args: (pair_idxs, scales, lambda_plane_idxs, lambda_offset_idxs, beta, cutoff)."""
+
+    _interpolated = False
+    _negated = False
+
+    def unbound_impl(self, precision):
+        _check_precision(precision)
+        pairs, scales, M = _pairs_scales(self.args[0], self.args[1])
+        plane, offset = _plane_offset(self.args[2], self.args[3])
+        h = ctypes.c_void_p()
+        lib = _lib.lib()
+        _lib.check(
+            lib.tmnb_pair_list_create(
+                plane.size,
+                _ptr(pairs),
+                _ptr(scales),
+                M,
+                _ptr(plane),
+                _ptr(offset),
+                float(self.args[4]),
+                float(self.args[5]),
+                1 if self._negated else 0,
+                1 if self._interpolated else 0,
+                32,
+                ctypes.byref(h),
+            )
+        )
+        return Potential(h, "NonbondedPairList", self._interpolated)
+
+
+class NonbondedPairListNegated(NonbondedPairList):
+    _negated = True
+
+
+class NonbondedPairListInterpolated(NonbondedPairList):
+    _interpolated = True
+
+
+class NonbondedPairListNegatedInterpolated(NonbondedPairList):
+    _negated = True
+    _interpolated = True
+
+
+class Nonbonded(CustomOpWrapper):
+    """timemachine/lib/potentials.py:269-344.
+
+    args: (exclusion_idxs, scale_factors, lambda_plane_idxs, lambda_offset_idxs, beta, cutoff)
+    """
+
+    _interpolated = False
+
+    def __init__(self, *args):
+        exclusion_idxs = np.asarray(args[0])
+        exclusion_set = set()
+        for src, dst in exclusion_idxs.reshape(-1, 2).tolist():
+            src, dst = sorted((src, dst))
+            exclusion_set.add((src, dst))
+        assert len(exclusion_set) == exclusion_idxs.reshape(-1, 2).shape[0]
+        super().__init__(*args)
+
+    def unbound_impl(self, precision):
+        _check_precision(precision)
+        pairs, scales, M = _pairs_scales(self.get_exclusion_idxs(), self.get_scale_factors())
+        plane, offset = _plane_offset(self.get_lambda_plane_idxs(), self.get_lambda_offset_idxs())
+        h = ctypes.c_void_p()
+        lib = _lib.lib()
+        _lib.check(
+            lib.tmnb_nonbonded_create(
+                plane.size,
+                _ptr(pairs),
+                _ptr(scales),
+                M,
+                _ptr(plane),
+                _ptr(offset),
+                float(self.get_beta()),
+                float(self.get_cutoff()),
+                1 if self._interpolated else 0,
+                32,
+                ctypes.byref(h),
+            )
+        )
+        return Potential(h, "Nonbonded", self._interpolated)
+
+    def set_exclusion_idxs(self, x):
+        self.args[0] = x
+
+    def get_exclusion_idxs(self):
+        return self.args[0]
+
+    def set_scale_factors(self, x):
+        self.args[1] = x
+
+    def get_scale_factors(self):
+        return self.args[1]
+
+    def get_lambda_plane_idxs(self):
+        return self.args[2]
+
+    def get_lambda_offset_idxs(self):
+        return self.args[3]
+
+    def set_lambda_plane_idxs(self, val):
+        self.args[2] = val
+
+    def set_lambda_offset_idxs(self, val):
+        self.args[3] = val
+
+    def get_beta(self):
+        return self.args[4]
+
+    def get_cutoff(self):
+        return self.args[5]
+
+    def interpolate(self):
+        return NonbondedInterpolated(
+            self.get_exclusion_idxs(),
+            self.get_scale_factors(),
+            self.get_lambda_plane_idxs(),
+            self.get_lambda_offset_idxs(),
+            self.get_beta(),
+            self.get_cutoff(),
+        )
+
+
+class NonbondedInterpolated(Nonbonded):
+    _interpolated = True
+
+
+def all_flag_combinations():
+    """The 16 (du_dx, du_dp, du_dl, u) request combinations (tests/common.py:451)."""
+    return list(itertools.product([False, True], repeat=4))
+
+
+__all__ += ["all_flag_combinations", "FIXED_EXPONENT"]
