@@ -53,7 +53,39 @@ def parse():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--impl", default="tmnb", choices=["tmnb", "reference"])
+    ap.add_argument(
+        "--profile",
+        type=int,
+        default=0,
+        help="run only this many evaluations of the workload (one per lambda window, cycling) and exit; "
+        "the command profiled by ncu for the committed kernel summaries",
+    )
+    ap.add_argument("--profile-outputs", default="all", choices=["all", "du_dx", "u"])
     return ap.parse_args()
+
+
+def run_profile(args, local):
+    import torch
+
+    from timemachine_b200 import potentials as P
+
+    s, x, p, lambdas = build_workload(0)
+    impl = P.Nonbonded(s.exclusion_idxs, s.scales, s.lambda_plane_idxs, s.lambda_offset_idxs, s.beta, s.cutoff)
+    impl = impl.unbound_impl(np.float32)
+    dev = torch.device("cuda", local)
+    dx = torch.as_tensor(x, device=dev)
+    dp = torch.as_tensor(p, device=dev).reshape(-1)
+    db = torch.as_tensor(s.box, device=dev)
+    N = s.N
+    want = args.profile_outputs
+    o_dx = torch.zeros((N, 3), dtype=torch.int64, device=dev) if want in ("all", "du_dx") else None
+    o_dp = torch.zeros(p.size, dtype=torch.int64, device=dev) if want == "all" else None
+    o_dl = torch.zeros(N, dtype=torch.int64, device=dev) if want == "all" else None
+    o_u = torch.zeros(N, dtype=torch.int64, device=dev) if want in ("all", "u") else None
+    for k in range(args.profile):
+        impl.execute_device(dx, dp, db, float(lambdas[k % N_WINDOWS]), o_dx, o_dp, o_dl, o_u)
+    torch.cuda.synchronize()
+    print(json.dumps({"profile_evals": args.profile, "outputs": want, "nblist": impl.nblist_stats()}))
 
 
 def dist_setup():
@@ -336,7 +368,110 @@ def run_tmnb(args, world, rank, local):
         },
         "clocks": clk.summary(),
     }
+    try:
+        result["md"] = run_md_tmnb()
+        result["ns_per_day"] = result["md"]["ns_per_day"]
+    except Exception as e:  # report, do not hide the evaluation numbers
+        result["md"] = {"error": str(e)[:300]}
     return result
+
+
+MD_STEPS = 10000
+MD_DT = 2.5e-3
+MD_EQ_STEPS = 2000
+MD_EQ_DT = 0.5e-3
+MD_LAMBDA = 0.5
+MD_TEMPERATURE = 300.0
+MD_BARO_INTERVAL = 25
+
+
+def md_system():
+    from timemachine_b200 import testsystems
+
+    return testsystems.water_ligand_23k(seed=SEED, hmr=True)
+
+
+def md_groups(s):
+    return [np.flatnonzero(s.group_of == g) for g in range(int(s.group_of.max()) + 1)]
+
+
+def md_v0(s, seed=SEED):
+    rng = np.random.default_rng(seed)
+    return rng.normal(size=(s.N, 3)) * np.sqrt(0.008314462618 * MD_TEMPERATURE / s.masses)[:, None]
+
+
+def run_md_tmnb(steps=MD_STEPS):
+    """configs[1] MD: 10,000 Langevin steps at 2.5 fs (HMR, H = 3 amu), MC barostat
+    every 25 steps at 1 bar, lambda 0.5, from a state equilibrated at 0.5 fs."""
+    from timemachine_b200 import md
+    from timemachine_b200 import potentials as P
+
+    s = md_system()
+    nb = P.Nonbonded(s.exclusion_idxs, s.scales, s.lambda_plane_idxs, s.lambda_offset_idxs, s.beta, s.cutoff)
+    bps = [
+        P.HarmonicBond(s.bond_idxs).bind(s.bond_params).bound_impl(np.float32),
+        P.HarmonicAngle(s.angle_idxs).bind(s.angle_params).bound_impl(np.float32),
+        nb.bind(s.params).bound_impl(np.float32),
+    ]
+    baro = md.MonteCarloBarostat(s.N, 1.0, MD_TEMPERATURE, md_groups(s), MD_BARO_INTERVAL, SEED + 1)
+    eq = md.Context(s.x, md_v0(s), s.box, md.LangevinIntegrator(MD_TEMPERATURE, MD_EQ_DT, 1.0, s.masses, SEED), bps, baro)
+    eq.multiple_steps(np.full(MD_EQ_STEPS, MD_LAMBDA))
+    x, v, box = eq.get_x_t(), eq.get_v_t(), eq.get_box()
+    del eq
+    ctx = md.Context(x, v, box, md.LangevinIntegrator(MD_TEMPERATURE, MD_DT, 1.0, s.masses, SEED + 7), bps, baro)
+    ctx.multiple_steps(np.full(200, MD_LAMBDA))  # warm-up (graph capture)
+    lam = np.full(steps, MD_LAMBDA)
+    t0 = time.perf_counter()
+    ctx.multiple_steps(lam)
+    dt_wall = time.perf_counter() - t0
+    xf = ctx.get_x_t()
+    acc, att, _ = ctx.barostat_stats()
+    steps_per_s = steps / dt_wall
+    return {
+        "ns_per_day": steps_per_s * MD_DT * 86400 / 1000,
+        "steps_per_s": steps_per_s,
+        "steps": steps,
+        "dt_ps": MD_DT,
+        "lambda": MD_LAMBDA,
+        "barostat": {"interval": MD_BARO_INTERVAL, "attempted": att, "accepted": acc},
+        "finite": bool(np.all(np.isfinite(xf))),
+        "timing": "wall clock around Context.multiple_steps (ends with a stream synchronise)",
+        "potentials": "HarmonicBond + HarmonicAngle + Nonbonded (22,840 atoms)",
+    }
+
+
+def run_md_reference(steps=MD_STEPS):
+    """The same MD through the reference runtime (Context/LangevinIntegrator/MonteCarloBarostat)."""
+    from oracle.refgpu import refgpu
+    from timemachine_b200.md import langevin_coefficients
+
+    s = md_system()
+    ref = refgpu.RefNonbonded(s.exclusion_idxs, s.scales, s.lambda_plane_idxs, s.lambda_offset_idxs, s.beta, s.cutoff)
+    group_of = s.group_of
+
+    def make(x, v, box, dt, seed):
+        ca, cb, cc = langevin_coefficients(MD_TEMPERATURE, dt, 1.0, s.masses)
+        return refgpu.RefMD(
+            ref, s.params, x, v, box, dt, ca, -cb, cc, seed, 1.0, MD_TEMPERATURE, group_of, MD_BARO_INTERVAL,
+            s.bond_idxs, s.bond_params, s.angle_idxs, s.angle_params,
+        )
+
+    eq = make(s.x, md_v0(s), s.box, MD_EQ_DT, SEED)
+    x, box = eq.run(MD_EQ_STEPS, MD_LAMBDA)
+    del eq
+    m = make(x, md_v0(s, SEED + 3), box, MD_DT, SEED + 7)
+    m.run(200, MD_LAMBDA)
+    t0 = time.perf_counter()
+    xf, _ = m.run(steps, MD_LAMBDA)
+    dt_wall = time.perf_counter() - t0
+    steps_per_s = steps / dt_wall
+    return {
+        "ns_per_day": steps_per_s * MD_DT * 86400 / 1000,
+        "steps_per_s": steps_per_s,
+        "steps": steps,
+        "finite": bool(np.all(np.isfinite(xf))),
+        "timing": "wall clock around Context.multiple_steps",
+    }
 
 
 def cpu_baseline(x, p, s, lambdas, n_evals=2):
@@ -447,11 +582,16 @@ def reference_gpu(s, x, p, lambdas, args):
         for lam in lambdas:
             ref.execute_host_fixed(x, p, s.box, float(lam))
     t1 = time.perf_counter()
+    try:
+        md_ref = run_md_reference()
+    except Exception as e:
+        md_ref = {"error": str(e)[:300]}
     return {
         "value": args.steps * N_WINDOWS / (total_ms / 1e3),
         "unit": "evals/s",
         "ms_per_step": total_ms / args.steps,
         "e2e_value": n_host * N_WINDOWS / (t1 - t0),
+        "md": md_ref,
         "source": "reference timemachine CUDA sources built for sm_100a (FanoutSummedPotential[NonbondedAllPairs_f32, NonbondedPairList_f32_negated])",
     }
 
@@ -459,6 +599,9 @@ def reference_gpu(s, x, p, lambdas, args):
 def main():
     args = parse()
     world, rank, local = dist_setup()
+    if args.profile:
+        run_profile(args, local)
+        return
     if args.impl == "reference":
         res = run_reference(args, world, rank, local)
     else:

@@ -196,6 +196,16 @@ tmnb_status tmnb_potential_check_device_error(tmnb_potential *pot, void *stream)
 tmnb_status tmnb_potential_nblist_stats(
     tmnb_potential *pot, void *stream, int *n_tiles, int *n_items, int *n_rebuilds);
 
+/* Neighbour-list introspection (timemachine/cpp/src/neighborlist.cu:81-124
+ * get_nblist_host serves the same tests): S slots, RB = ceil(S/32) row
+ * blocks, tile storage of tile_capacity tiles. copy_nblist synchronises and
+ * copies the slot order perm[S] (slot -> atom), the tile count of every row
+ * block [RB] and the column slots of all tiles [tile_capacity*32]; row block
+ * rb owns the tiles starting at rb*RB - rb*(rb-1)/2. Any pointer may be NULL. */
+tmnb_status tmnb_potential_nblist_shape(tmnb_potential *pot, int *S, int *RB, long long *tile_capacity);
+tmnb_status tmnb_potential_copy_nblist(
+    tmnb_potential *pot, void *stream, unsigned *perm, int *row_block_ntiles, unsigned *tile_cols);
+
 /* Instrumentation (no reference counterpart): CUDA events around every
  * pair-kernel launch on the launching stream, and the duration of the last
  * one (synchronises on its end event). */
@@ -205,6 +215,79 @@ tmnb_status tmnb_potential_last_pair_kernel_ms(tmnb_potential *pot, float *ms);
 /* Measured FP32 FMA throughput of the current device in TFLOP/s (the
  * denominator of the pair kernel's FP32 roofline; no reference counterpart). */
 tmnb_status tmnb_probe_fp32_peak(double *tflops);
+
+/*
+ * MD context: replaces timemachine's Context (timemachine/cpp/src/context.hpp:12-45)
+ * with its LangevinIntegrator (timemachine/cpp/src/integrator.hpp:29) and
+ * MonteCarloBarostat (timemachine/cpp/src/barostat.hpp:26-33). The context
+ * copies x0/v0/box0 and the parameters to the device; the potentials stay
+ * owned by the caller and must outlive the context. ca/cbs/ccs are the
+ * reference's Langevin coefficients (timemachine/integrator.py:32-46 with
+ * cbs = -dt/m, timemachine/lib/__init__.py:13-17).
+ */
+typedef struct tmnb_context tmnb_context;
+
+tmnb_status tmnb_context_create(
+    int N,
+    const double *x0,   /* [N,3] host */
+    const double *v0,   /* [N,3] host */
+    const double *box0, /* [3,3] host */
+    double dt,
+    double ca,
+    const double *cbs, /* [N] host */
+    const double *ccs, /* [N] host */
+    unsigned long long seed,
+    int n_potentials,
+    tmnb_potential *const *potentials,
+    const double *const *params, /* per potential, host */
+    const int *param_sizes,
+    tmnb_context **out);
+
+/* Isotropic MC barostat every `interval` steps; group_of[i] is the molecule
+ * of atom i (-1: not rescaled). */
+tmnb_status tmnb_context_set_barostat(
+    tmnb_context *ctx, double pressure_bar, double temperature_k, const int32_t *group_of, int interval,
+    unsigned long long seed);
+
+/* Context::multiple_steps (timemachine/cpp/src/context.cu:55-137): runs
+ * n_steps steps at lambda_schedule[i]; du_dl is stored every
+ * store_du_dl_interval steps into du_dl_out[n_steps/interval] (host),
+ * coordinates/box every store_x_interval steps into x_out/box_out (host);
+ * intervals <= 0 store nothing. use_graphs != 0 replays each step as a CUDA
+ * graph (one per distinct lambda). */
+tmnb_status tmnb_context_multiple_steps(
+    tmnb_context *ctx,
+    int n_steps,
+    const double *lambda_schedule,
+    int store_du_dl_interval,
+    double *du_dl_out,
+    int store_x_interval,
+    double *x_out,
+    double *box_out,
+    int use_graphs);
+
+/* State accessors (timemachine/cpp/src/context.cu:284-304). */
+tmnb_status tmnb_context_get_x(tmnb_context *ctx, double *out);
+tmnb_status tmnb_context_get_v(tmnb_context *ctx, double *out);
+tmnb_status tmnb_context_get_box(tmnb_context *ctx, double *out);
+tmnb_status tmnb_context_set_x(tmnb_context *ctx, const double *in);
+tmnb_status tmnb_context_set_v(tmnb_context *ctx, const double *in);
+tmnb_status tmnb_context_set_box(tmnb_context *ctx, const double *in);
+tmnb_status tmnb_context_barostat_stats(tmnb_context *ctx, int *accepted, int *attempted, double *volume_scale);
+tmnb_status tmnb_context_destroy(tmnb_context *ctx);
+
+/*
+ * Bonded terms the MD drivers need alongside the nonbonded potential:
+ * HarmonicBond (timemachine/cpp/src/harmonic_bond.cu, U = kb/2 (r - b0)^2,
+ * params [B,2]) and HarmonicAngle (timemachine/cpp/src/harmonic_angle.cu,
+ * U = ka/2 (cos theta - cos a0)^2, params [A,2], angle_idxs [A,3] with the
+ * vertex in the middle). Each term is scaled by lambda_offset + lambda_mult *
+ * lambda (NULL: offset 1, mult 0).
+ */
+tmnb_status tmnb_harmonic_bond_create(
+    int N, int B, const int32_t *bond_idxs, const int32_t *lambda_mult, const int32_t *lambda_offset, tmnb_potential **out);
+tmnb_status tmnb_harmonic_angle_create(
+    int N, int A, const int32_t *angle_idxs, const int32_t *lambda_mult, const int32_t *lambda_offset, tmnb_potential **out);
 
 /* Expected parameter count P (N*3, or 2*N*3 when interpolated). */
 int tmnb_potential_num_params(const tmnb_potential *pot);

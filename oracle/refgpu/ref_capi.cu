@@ -16,6 +16,8 @@
 #include "barostat.hpp"
 #include "context.hpp"
 #include "fanout_summed_potential.hpp"
+#include "harmonic_angle.hpp"
+#include "harmonic_bond.hpp"
 #include "integrator.hpp"
 #include "nonbonded_all_pairs.hpp"
 #include "nonbonded_pair_list.hpp"
@@ -68,6 +70,7 @@ template <typename F> int guarded(F &&f) {
 struct RefMD {
     std::unique_ptr<timemachine::LangevinIntegrator> intg;
     std::unique_ptr<timemachine::BoundPotential> bp;
+    std::vector<std::unique_ptr<timemachine::BoundPotential>> bonded;
     std::unique_ptr<timemachine::MonteCarloBarostat> baro;
     std::unique_ptr<timemachine::Context> ctx;
 };
@@ -192,14 +195,33 @@ void *tmref_md_create(
     double pressure,     // bar; <= 0: no barostat
     double temperature,  // K
     const int *group_of, // [N] molecule id of each atom (barostat groups)
-    int barostat_interval) {
+    int barostat_interval,
+    const int *bond_idxs, // [B,2]
+    int B,
+    const double *bond_params, // [B,2]
+    const int *angle_idxs,     // [A,3]
+    int A,
+    const double *angle_params) { // [A,2]
     RefMD *h = nullptr;
     auto *nb = static_cast<RefNonbonded *>(nonbonded);
     int rc = guarded([&] {
         auto m = std::make_unique<RefMD>();
         m->intg = std::make_unique<timemachine::LangevinIntegrator>(N, dt, ca, cbs, ccs, seed);
         m->bp = std::make_unique<timemachine::BoundPotential>(nb->fanout, std::vector<int>{P / 3, 3}, params);
-        std::vector<timemachine::BoundPotential *> bps{m->bp.get()};
+        std::vector<timemachine::BoundPotential *> bps;
+        if (B > 0) {
+            auto hb = std::make_shared<timemachine::HarmonicBond<float>>(
+                std::vector<int>(bond_idxs, bond_idxs + 2 * (size_t)B), std::vector<int>(), std::vector<int>());
+            m->bonded.push_back(std::make_unique<timemachine::BoundPotential>(hb, std::vector<int>{B, 2}, bond_params));
+            bps.push_back(m->bonded.back().get());
+        }
+        if (A > 0) {
+            auto ha = std::make_shared<timemachine::HarmonicAngle<float>>(
+                std::vector<int>(angle_idxs, angle_idxs + 3 * (size_t)A), std::vector<int>(), std::vector<int>());
+            m->bonded.push_back(std::make_unique<timemachine::BoundPotential>(ha, std::vector<int>{A, 2}, angle_params));
+            bps.push_back(m->bonded.back().get());
+        }
+        bps.push_back(m->bp.get());
         if (pressure > 0) {
             int ngroups = 0;
             for (int i = 0; i < N; i++) {

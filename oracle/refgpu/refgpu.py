@@ -48,7 +48,7 @@ def lib():
         L.tmref_execute_device.argtypes = [vp, i, i, vp, vp, vp, d, vp, vp, vp, vp, vp]
         L.tmref_execute_host.argtypes = [vp, i, i, vp, vp, vp, d, vp, vp, vp, vp]
         L.tmref_md_create.restype = vp
-        L.tmref_md_create.argtypes = [vp, i, vp, i, vp, vp, vp, d, d, vp, vp, i, d, d, vp, i]
+        L.tmref_md_create.argtypes = [vp, i, vp, i, vp, vp, vp, d, d, vp, vp, i, d, d, vp, i, vp, i, vp, vp, i, vp]
         L.tmref_md_run.argtypes = [vp, i, d, vp, vp]
         L.tmref_md_destroy.argtypes = [vp]
         _lib = L
@@ -124,7 +124,10 @@ class RefNonbonded:
 class RefMD:
     """Reference Context(LangevinIntegrator, [Nonbonded], MonteCarloBarostat)."""
 
-    def __init__(self, nb, params, x0, v0, box, dt, ca, cbs, ccs, seed, pressure, temperature, group_of, interval):
+    def __init__(
+        self, nb, params, x0, v0, box, dt, ca, cbs, ccs, seed, pressure, temperature, group_of, interval,
+        bond_idxs=None, bond_params=None, angle_idxs=None, angle_params=None,
+    ):
         L = lib()
         self._keep = [
             np.ascontiguousarray(params, dtype=np.float64),
@@ -136,11 +139,16 @@ class RefMD:
             np.ascontiguousarray(group_of, dtype=np.int32),
         ]
         pp, xx, vv, bb, cb, cc, gg = self._keep
+        bi = np.ascontiguousarray(np.zeros((0, 2)) if bond_idxs is None else bond_idxs, dtype=np.int32)
+        bpar = np.ascontiguousarray(np.zeros((0, 2)) if bond_params is None else bond_params, dtype=np.float64)
+        ai = np.ascontiguousarray(np.zeros((0, 3)) if angle_idxs is None else angle_idxs, dtype=np.int32)
+        apar = np.ascontiguousarray(np.zeros((0, 2)) if angle_params is None else angle_params, dtype=np.float64)
+        self._keep += [bi, bpar, ai, apar]
         self.nb = nb
         self.N = xx.shape[0]
         self._h = L.tmref_md_create(
             nb._h, self.N, _p(pp), pp.size, _p(xx), _p(vv), _p(bb), dt, ca, _p(cb), _p(cc), seed, pressure,
-            temperature, _p(gg), interval,
+            temperature, _p(gg), interval, _p(bi), bi.shape[0], _p(bpar), _p(ai), ai.shape[0], _p(apar),
         )
         if not self._h:
             raise RuntimeError(L.tmref_last_error().decode())

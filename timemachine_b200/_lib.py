@@ -25,7 +25,7 @@ NVCC_FLAGS = [
     "-shared",
 ]
 
-SOURCES = ["nonbonded.cu"]
+SOURCES = ["nonbonded.cu", "md.cu", "bonded.cu"]
 
 
 def build(verbose: bool = False) -> str:
@@ -71,9 +71,23 @@ def _declare(lib):
     lib.tmnb_potential_disable_hilbert_sort.argtypes = [vp]
     lib.tmnb_potential_check_device_error.argtypes = [vp, vp]
     lib.tmnb_potential_nblist_stats.argtypes = [vp, vp, c_int_p, c_int_p, c_int_p]
+    lib.tmnb_potential_nblist_shape.argtypes = [vp, c_int_p, c_int_p, ctypes.POINTER(ctypes.c_longlong)]
+    lib.tmnb_potential_copy_nblist.argtypes = [vp, vp, vp, vp, vp]
+    lib.tmnb_potential_nblist_shape.restype = ctypes.c_int
+    lib.tmnb_potential_copy_nblist.restype = ctypes.c_int
     lib.tmnb_potential_enable_timing.argtypes = [vp, i]
     lib.tmnb_potential_last_pair_kernel_ms.argtypes = [vp, ctypes.POINTER(ctypes.c_float)]
     lib.tmnb_probe_fp32_peak.argtypes = [ctypes.POINTER(ctypes.c_double)]
+    ull = ctypes.c_ulonglong
+    lib.tmnb_context_create.argtypes = [i, vp, vp, vp, d, d, vp, vp, ull, i, vp, vp, vp, ctypes.POINTER(vp)]
+    lib.tmnb_context_set_barostat.argtypes = [vp, d, d, vp, i, ull]
+    lib.tmnb_context_multiple_steps.argtypes = [vp, i, vp, i, vp, i, vp, vp, i]
+    for nm in ["get_x", "get_v", "get_box", "set_x", "set_v", "set_box"]:
+        getattr(lib, "tmnb_context_" + nm).argtypes = [vp, vp]
+    lib.tmnb_context_barostat_stats.argtypes = [vp, c_int_p, c_int_p, c_double_p]
+    lib.tmnb_context_destroy.argtypes = [vp]
+    lib.tmnb_harmonic_bond_create.argtypes = [i, i, vp, vp, vp, ctypes.POINTER(vp)]
+    lib.tmnb_harmonic_angle_create.argtypes = [i, i, vp, vp, vp, ctypes.POINTER(vp)]
     lib.tmnb_potential_num_params.argtypes = [vp]
     lib.tmnb_potential_num_atoms.argtypes = [vp]
     for name in [
@@ -92,6 +106,19 @@ def _declare(lib):
         "tmnb_potential_enable_timing",
         "tmnb_potential_last_pair_kernel_ms",
         "tmnb_probe_fp32_peak",
+        "tmnb_context_create",
+        "tmnb_context_set_barostat",
+        "tmnb_context_multiple_steps",
+        "tmnb_context_get_x",
+        "tmnb_context_get_v",
+        "tmnb_context_get_box",
+        "tmnb_context_set_x",
+        "tmnb_context_set_v",
+        "tmnb_context_set_box",
+        "tmnb_context_barostat_stats",
+        "tmnb_context_destroy",
+        "tmnb_harmonic_bond_create",
+        "tmnb_harmonic_angle_create",
     ]:
         getattr(lib, name).restype = ctypes.c_int
     lib.tmnb_potential_num_params.restype = ctypes.c_int

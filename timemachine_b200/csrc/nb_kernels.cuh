@@ -663,17 +663,17 @@ __device__ __forceinline__ void sweep_tile(
     const int src = (lane + 1) & 31;
 #pragma unroll 2
     for (int round = 0; round < TILE; round++) {
-        Real delta_x = ci_x - cj_x;
-        Real delta_y = ci_y - cj_y;
-        Real delta_z = ci_z - cj_z;
+        Real delta_x = fsub(ci_x, cj_x);
+        Real delta_y = fsub(ci_y, cj_y);
+        Real delta_z = fsub(ci_z, cj_z);
         delta_x = min_image(delta_x, box_x, inv_box_x);
         delta_y = min_image(delta_y, box_y, inv_box_y);
         delta_z = min_image(delta_z, box_z, inv_box_z);
-        Real d2 = delta_x * delta_x + delta_y * delta_y + delta_z * delta_z;
+        Real d2 = dist2(delta_x, delta_y, delta_z);
         Real delta_w;
         if (ALCH) {
-            delta_w = ci_w - cj_w;
-            d2 += delta_w * delta_w;
+            delta_w = fsub(ci_w, cj_w);
+            d2 = add_w2(d2, delta_w);
         }
         const bool valid = i < S && j < S && i < j;
         if (valid && d2 < cutoff_squared) {
@@ -683,29 +683,33 @@ __device__ __forceinline__ void sweep_tile(
             Real d;
             Real inv_d;
             Real inv_d2;
-            electrostatics<Real, U>(1.0, qi, qj, d2, beta, d, inv_d, inv_d2, erfc_bd, prefactor, u);
+            Real qij_inv;
+            Real factor;
+            electrostatics<Real, U>(
+                (Real)1, qi, qj, d2, beta, d, inv_d, inv_d2, erfc_bd, prefactor, u, qij_inv, factor);
             Real real_du_dl = 0;
             if (eps_i != 0 && eps_j != 0) {
                 Real sig_grad;
                 Real eps_grad;
-                lennard_jones<Real, U>(1.0, eps_i, eps_j, sig_i, sig_j, inv_d, inv_d2, u, prefactor, sig_grad, eps_grad);
+                lennard_jones<Real, U>(
+                    (Real)1, eps_i, eps_j, sig_i, sig_j, inv_d, inv_d2, qij_inv, factor, erfc_bd, u, prefactor,
+                    sig_grad, eps_grad);
                 if (DP) {
                     const unsigned long long gs = to_fixed(sig_grad, FX_EXPONENT_SIG);
                     g_sigi += gs;
                     g_sigj += gs;
-                    g_epsi += to_fixed(eps_grad * eps_j, FX_EXPONENT_EPS);
-                    g_epsj += to_fixed(eps_grad * eps_i, FX_EXPONENT_EPS);
+                    g_epsi += to_fixed(fmul(eps_grad, eps_j), FX_EXPONENT_EPS);
+                    g_epsj += to_fixed(fmul(eps_grad, eps_i), FX_EXPONENT_EPS);
                 }
                 if (DL && ALCH && INTERP) {
-                    real_du_dl += sig_grad * (dsig_dl_i + dsig_dl_j);
-                    Real term = eps_grad * sum_of_products_rn(eps_j, deps_dl_i, eps_i, deps_dl_j);
-                    real_du_dl += term;
+                    real_du_dl = ffma(sig_grad, fadd(dsig_dl_i, dsig_dl_j), real_du_dl);
+                    real_du_dl = ffma(eps_grad, sum_of_products_rn(eps_j, deps_dl_i, eps_i, deps_dl_j), real_du_dl);
                 }
             }
             if (DX) {
-                const unsigned long long fx = to_fixed(prefactor * delta_x, FX_EXPONENT);
-                const unsigned long long fy = to_fixed(prefactor * delta_y, FX_EXPONENT);
-                const unsigned long long fz = to_fixed(prefactor * delta_z, FX_EXPONENT);
+                const unsigned long long fx = to_fixed(fmul(prefactor, delta_x), FX_EXPONENT);
+                const unsigned long long fy = to_fixed(fmul(prefactor, delta_y), FX_EXPONENT);
+                const unsigned long long fz = to_fixed(fmul(prefactor, delta_z), FX_EXPONENT);
                 gi_x += fx;
                 gi_y += fy;
                 gi_z += fz;
@@ -714,13 +718,13 @@ __device__ __forceinline__ void sweep_tile(
                 gj_z -= fz;
             }
             if (DP) {
-                g_qi += to_fixed(qj * inv_d * erfc_bd, FX_EXPONENT);
-                g_qj += to_fixed(qi * inv_d * erfc_bd, FX_EXPONENT);
+                g_qi += to_fixed(fmul(fmul(qj, inv_d), erfc_bd), FX_EXPONENT);
+                g_qj += to_fixed(fmul(fmul(qi, inv_d), erfc_bd), FX_EXPONENT);
             }
             if (DL && ALCH) {
-                real_du_dl += delta_w * prefactor * (dw_dl_i - dw_dl_j);
+                real_du_dl = ffma(fmul(delta_w, prefactor), fsub(dw_dl_i, dw_dl_j), real_du_dl);
                 if (INTERP) {
-                    real_du_dl += inv_d * erfc_bd * sum_of_products_rn(qj, dq_dl_i, qi, dq_dl_j);
+                    real_du_dl = ffma(fmul(inv_d, erfc_bd), sum_of_products_rn(qj, dq_dl_i, qi, dq_dl_j), real_du_dl);
                 }
                 du_dl += to_fixed(real_du_dl, FX_EXPONENT);
             }
@@ -787,14 +791,14 @@ __device__ __forceinline__ void scaled_pair(const PairArgs &a, int pair, const R
     const Real charge_scale = a.scales[2 * pair + 0];
     const Real lj_scale = a.scales[2 * pair + 1];
 
-    Real delta_x = ci_x - cj_x;
-    Real delta_y = ci_y - cj_y;
-    Real delta_z = ci_z - cj_z;
+    Real delta_x = fsub(ci_x, cj_x);
+    Real delta_y = fsub(ci_y, cj_y);
+    Real delta_z = fsub(ci_z, cj_z);
     delta_x = min_image(delta_x, box_x, inv_box_x);
     delta_y = min_image(delta_y, box_y, inv_box_y);
     delta_z = min_image(delta_z, box_z, inv_box_z);
-    const Real delta_w = ci_w - cj_w;
-    const Real d2 = delta_x * delta_x + delta_y * delta_y + delta_z * delta_z + delta_w * delta_w;
+    const Real delta_w = fsub(ci_w, cj_w);
+    const Real d2 = add_w2(dist2(delta_x, delta_y, delta_z), delta_w);
 
     const bool is_vanilla = (ci_w == 0 && dq_dl_i == 0 && dsig_dl_i == 0 && deps_dl_i == 0 && cj_w == 0 &&
                              dq_dl_j == 0 && dsig_dl_j == 0 && deps_dl_j == 0);
@@ -807,28 +811,32 @@ __device__ __forceinline__ void scaled_pair(const PairArgs &a, int pair, const R
     Real d;
     Real inv_d;
     Real inv_d2;
-    electrostatics<Real, true>(charge_scale, qi, qj, d2, beta, d, inv_d, inv_d2, erfc_bd, prefactor, u);
+    Real qij_inv;
+    Real factor;
+    electrostatics<Real, true>(
+        charge_scale, qi, qj, d2, beta, d, inv_d, inv_d2, erfc_bd, prefactor, u, qij_inv, factor);
     Real real_du_dl = 0;
     unsigned long long g_sig = 0, g_epsi = 0, g_epsj = 0;
     if (eps_i != 0 && eps_j != 0) {
         Real sig_grad;
         Real eps_grad;
-        lennard_jones<Real, true>(lj_scale, eps_i, eps_j, sig_i, sig_j, inv_d, inv_d2, u, prefactor, sig_grad, eps_grad);
+        lennard_jones<Real, true>(
+            lj_scale, eps_i, eps_j, sig_i, sig_j, inv_d, inv_d2, qij_inv, factor, erfc_bd, u, prefactor, sig_grad,
+            eps_grad);
         g_sig = to_fixed(sig_grad, FX_EXPONENT_SIG);
-        g_epsi = to_fixed(eps_grad * eps_j, FX_EXPONENT_EPS);
-        g_epsj = to_fixed(eps_grad * eps_i, FX_EXPONENT_EPS);
+        g_epsi = to_fixed(fmul(eps_grad, eps_j), FX_EXPONENT_EPS);
+        g_epsj = to_fixed(fmul(eps_grad, eps_i), FX_EXPONENT_EPS);
         if (INTERP) {
-            real_du_dl += sig_grad * (dsig_dl_i + dsig_dl_j);
-            Real term = eps_grad * sum_of_products_rn(eps_j, deps_dl_i, eps_i, deps_dl_j);
-            real_du_dl += term;
+            real_du_dl = ffma(sig_grad, fadd(dsig_dl_i, dsig_dl_j), real_du_dl);
+            real_du_dl = ffma(eps_grad, sum_of_products_rn(eps_j, deps_dl_i, eps_i, deps_dl_j), real_du_dl);
         }
     }
     const bool neg = a.negated != 0;
     auto acc = [neg](unsigned long long *p, unsigned long long v) { red_add(p, neg ? (0ULL - v) : v); };
     if (DX) {
-        const unsigned long long fx = to_fixed(prefactor * delta_x, FX_EXPONENT);
-        const unsigned long long fy = to_fixed(prefactor * delta_y, FX_EXPONENT);
-        const unsigned long long fz = to_fixed(prefactor * delta_z, FX_EXPONENT);
+        const unsigned long long fx = to_fixed(fmul(prefactor, delta_x), FX_EXPONENT);
+        const unsigned long long fy = to_fixed(fmul(prefactor, delta_y), FX_EXPONENT);
+        const unsigned long long fz = to_fixed(fmul(prefactor, delta_z), FX_EXPONENT);
         acc(a.acc.x + si, fx);
         acc(a.acc.y + si, fy);
         acc(a.acc.z + si, fz);
@@ -837,17 +845,18 @@ __device__ __forceinline__ void scaled_pair(const PairArgs &a, int pair, const R
         acc(a.acc.z + sj, 0ULL - fz);
     }
     if (DP) {
-        acc(a.acc.pq + si, to_fixed(charge_scale * qj * inv_d * erfc_bd, FX_EXPONENT));
-        acc(a.acc.pq + sj, to_fixed(charge_scale * qi * inv_d * erfc_bd, FX_EXPONENT));
+        acc(a.acc.pq + si, to_fixed(fmul(fmul(fmul(charge_scale, qj), inv_d), erfc_bd), FX_EXPONENT));
+        acc(a.acc.pq + sj, to_fixed(fmul(fmul(fmul(charge_scale, qi), inv_d), erfc_bd), FX_EXPONENT));
         acc(a.acc.psig + si, g_sig);
         acc(a.acc.peps + si, g_epsi);
         acc(a.acc.psig + sj, g_sig);
         acc(a.acc.peps + sj, g_epsj);
     }
     if (DL && !is_vanilla) {
-        real_du_dl += delta_w * prefactor * (dw_dl_i - dw_dl_j);
+        real_du_dl = ffma(fmul(delta_w, prefactor), fsub(dw_dl_i, dw_dl_j), real_du_dl);
         if (INTERP) {
-            real_du_dl += charge_scale * inv_d * erfc_bd * sum_of_products_rn(qj, dq_dl_i, qi, dq_dl_j);
+            real_du_dl = ffma(
+                fmul(fmul(charge_scale, inv_d), erfc_bd), sum_of_products_rn(qj, dq_dl_i, qi, dq_dl_j), real_du_dl);
         }
         acc(a.acc.dl + si, to_fixed(real_du_dl, FX_EXPONENT));
     }

@@ -5,20 +5,58 @@
 // Bit-exactness contract. The int64 accumulators are sums of per-pair
 // fixed-point integers, so they are order-independent; they equal the
 // reference kernel's accumulators exactly when every per-pair FP32 value is
-// bit-identical. The expressions below therefore keep the reference's
-// expression trees (operand order and association) so that nvcc forms the
-// same fused multiply-adds:
+// bit-identical. Every FP32 operation below is therefore written with an
+// explicit rounding intrinsic (__fmaf_rn, __fmul_rn, __fadd_rn, __fsub_rn):
+// the compiler cannot contract or re-associate them, so each pair gets the
+// same rounding in every kernel, loop copy and output variant, and the fused
+// multiply-adds sit where the reference's compiled expressions put them.
+// The expression trees follow
 //   - pair arithmetic: timemachine/cpp/src/kernels/nonbonded_common.cuh:38-48
 //     (erfc factor), :78-102 (electrostatics), :108-140 (Lennard-Jones);
+//   - distances and minimum image: timemachine/cpp/src/kernels/k_nonbonded.cuh:426-442;
 //   - fixed-point encoding: timemachine/cpp/src/fixed_point.hpp:3-8 and
 //     timemachine/cpp/src/kernels/k_fixed_point.cuh:51-65 (llrint(v * 2^e));
-//   - periodic minimum image: timemachine/cpp/src/kernels/k_nonbonded.cuh:430-432;
-//   - the two-product sum with pinned rounding:
-//     timemachine/cpp/src/kernels/kernel_utils.cuh:92-98.
+//   - the two-product sum: timemachine/cpp/src/kernels/kernel_utils.cuh:92-98.
+// TMNB_DAG_* select, at each point where a multiply feeds an add, which of
+// the two rounding patterns is used (1 = fused multiply-add).
 #pragma once
 
 #include <cuda_runtime.h>
 #include <stdint.h>
+
+#ifndef TMNB_DAG_D2
+#define TMNB_DAG_D2 0 // 0: fma(dz,dz,fma(dx,dx,dy*dy)); 1: fma(dz,dz,fma(dy,dy,dx*dx)); 2: unfused
+#endif
+#ifndef TMNB_DAG_MINIMG
+#define TMNB_DAG_MINIMG 1 // d - box*n: 1 fused, 0 unfused
+#endif
+#ifndef TMNB_DAG_DEN
+#define TMNB_DAG_DEN 1 // 1 + 0.3275911*bd: 1 fused, 0 unfused
+#endif
+#ifndef TMNB_DAG_POLY
+#define TMNB_DAG_POLY 1 // Horner steps: 1 fused, 0 unfused
+#endif
+#ifndef TMNB_DAG_ERF
+#define TMNB_DAG_ERF 1 // c*bd*e + erfc: 1 fma((c*bd), e, erfc); 0 unfused; 2 fma(erfc_factors, e, c*bd*e)
+#endif
+#ifndef TMNB_DAG_PRE
+#define TMNB_DAG_PRE 1 // es_pref - lj_pref: 1 fma(-X,Y,es); 0 unfused; 2 fma(qij_inv, factor, -(X*Y))
+#endif
+#ifndef TMNB_DAG_LJP
+#define TMNB_DAG_LJP 1 // s6*48 - 24: 1 fused, 0 unfused
+#endif
+#ifndef TMNB_DAG_U
+#define TMNB_DAG_U 1 // u_es + A*s6: 1 fma(A,s6,u_es); 0 unfused; 2 fma(qij_inv, erfc, A*s6)
+#endif
+#ifndef TMNB_DAG_S6M1
+#define TMNB_DAG_S6M1 0 // s6 - 1: 0 fsub(s6,1); 1 fma(s4,s2,-1)
+#endif
+#ifndef TMNB_DAG_2S6M1
+#define TMNB_DAG_2S6M1 0 // 2*s6 - 1: 0 fma(2,s6,-1) (= fl(2 s6 - 1)); 1 fl(fma(s4,s2,s6) - 1)
+#endif
+#ifndef TMNB_DAG_D4
+#define TMNB_DAG_D4 1 // d2 + dw*dw: 1 fused, 0 unfused
+#endif
 
 namespace tmb {
 
@@ -28,19 +66,29 @@ constexpr unsigned long long FX_EXPONENT_SIG = 0x2000000000ULL; // 2^37: du_dsig
 constexpr unsigned long long FX_EXPONENT_EPS = 0x4000000000ULL; // 2^38: du_deps
 
 __device__ __forceinline__ unsigned long long to_fixed(float v, unsigned long long exponent) {
-    return static_cast<unsigned long long>(llrintf(v * exponent));
+    return static_cast<unsigned long long>(llrintf(__fmul_rn(v, static_cast<float>(exponent))));
 }
 __device__ __forceinline__ unsigned long long to_fixed(double v, unsigned long long exponent) {
     return static_cast<unsigned long long>(llrint(v * exponent));
 }
 
-// a*b + c*d with both products rounded before the sum (no contraction).
-__device__ __forceinline__ float sum_of_products_rn(float a, float b, float c, float d) {
-    return __fmul_rn(a, b) + __fmul_rn(c, d);
+// explicit-rounding FP32 helpers
+__device__ __forceinline__ float fmul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float fadd(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float fsub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float ffma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double fmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double fadd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double fsub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double ffma(double a, double b, double c) { return __fma_rn(a, b, c); }
+
+// a*b + c*d with both products rounded before the sum.
+template <typename Real> __device__ __forceinline__ Real sum_of_products_rn(Real a, Real b, Real c, Real d) {
+    return fadd(fmul(a, b), fmul(c, d));
 }
-__device__ __forceinline__ double sum_of_products_rn(double a, double b, double c, double d) {
-    return __dmul_rn(a, b) + __dmul_rn(c, d);
-}
+
+// acc + a*b with the reference's fused rounding
+template <typename Real> __device__ __forceinline__ Real mul_add(Real a, Real b, Real acc) { return ffma(a, b, acc); }
 
 __device__ __forceinline__ float inv_sqrt(float x) { return rsqrtf(x); }
 __device__ __forceinline__ double inv_sqrt(double x) { return rsqrt(x); }
@@ -55,31 +103,73 @@ __device__ __forceinline__ float round_half_even(float t) {
 }
 __device__ __forceinline__ double round_half_even(double t) { return nearbyint(t); }
 
-// Minimum-image displacement along one axis of an orthorhombic box.
+// Minimum-image displacement along one axis of an orthorhombic box:
+// delta - box * nearbyint(delta / box).
 template <typename Real> __device__ __forceinline__ Real min_image(Real delta, Real box, Real inv_box) {
-    delta -= box * round_half_even(delta * inv_box);
-    return delta;
+    const Real n = round_half_even(fmul(delta, inv_box));
+#if TMNB_DAG_MINIMG
+    return ffma(-box, n, delta);
+#else
+    return fsub(delta, fmul(box, n));
+#endif
+}
+
+// squared 3D distance
+template <typename Real> __device__ __forceinline__ Real dist2(Real dx, Real dy, Real dz) {
+#if TMNB_DAG_D2 == 0
+    return ffma(dz, dz, ffma(dx, dx, fmul(dy, dy)));
+#elif TMNB_DAG_D2 == 1
+    return ffma(dz, dz, ffma(dy, dy, fmul(dx, dx)));
+#else
+    return fadd(fadd(fmul(dx, dx), fmul(dy, dy)), fmul(dz, dz));
+#endif
+}
+
+template <typename Real> __device__ __forceinline__ Real add_w2(Real d2, Real dw) {
+#if TMNB_DAG_D4
+    return ffma(dw, dw, d2);
+#else
+    return fadd(d2, fmul(dw, dw));
+#endif
+}
+
+template <typename Real> __device__ __forceinline__ Real madd(Real a, Real b, Real c, int fused) {
+    return fused ? ffma(a, b, c) : fadd(fmul(a, b), c);
 }
 
 // Derivative factor of qq*erfc(beta d)/d w.r.t. d (divided by d), FP32 form:
 // erfc from Abramowitz & Stegun 7.1.26 (five-term rational-exponential fit,
-// |error| <= 1.5e-7), reusing exp(-(beta d)^2) for the chain rule.
+// |error| <= 1.5e-7), reusing exp(-(beta d)^2) for the chain rule. The IEEE
+// reciprocal __frcp_rn equals the correctly rounded 1.0f/x of the reference.
 __device__ __forceinline__ float es_factor(float beta, float d, float inv_d2, float &erfc_bd) {
-    float bd = beta * d;
-    float e = __expf(-bd * bd);
-    float t = 1.0f / (1.0f + 0.3275911f * bd);
-    erfc_bd = (0.254829592f + (-0.284496736f + (1.421413741f + (-1.453152027f + 1.061405429f * t) * t) * t) * t) * t * e;
-    return -inv_d2 * (static_cast<float>(1.128379167095512595889238330988549829708) * bd * e + erfc_bd);
+    const float bd = fmul(beta, d);
+    const float e = __expf(fmul(-bd, bd));
+    const float t = __frcp_rn(madd(0.3275911f, bd, 1.0f, TMNB_DAG_DEN));
+    float poly = madd(1.061405429f, t, -1.453152027f, TMNB_DAG_POLY);
+    poly = madd(poly, t, 1.421413741f, TMNB_DAG_POLY);
+    poly = madd(poly, t, -0.284496736f, TMNB_DAG_POLY);
+    poly = madd(poly, t, 0.254829592f, TMNB_DAG_POLY);
+    erfc_bd = fmul(fmul(poly, t), e);
+    const float cbd = fmul(static_cast<float>(1.128379167095512595889238330988549829708), bd);
+#if TMNB_DAG_ERF == 1
+    const float s = ffma(cbd, e, erfc_bd);
+#elif TMNB_DAG_ERF == 0
+    const float s = fadd(fmul(cbd, e), erfc_bd);
+#else
+    const float s = ffma(fmul(poly, t), e, fmul(cbd, e));
+#endif
+    return fmul(-inv_d2, s);
 }
 __device__ __forceinline__ double es_factor(double beta, double d, double inv_d2, double &erfc_bd) {
-    double bd = beta * d;
-    double e = exp(-bd * bd);
+    const double bd = beta * d;
+    const double e = exp(-bd * bd);
     erfc_bd = erfc(bd);
     return -inv_d2 * (static_cast<double>(1.128379167095512595889238330988549829708) * bd * e + erfc_bd);
 }
 
-// Electrostatic part of one pair (charge-scaled): fills the distance terms,
-// the erfc value, the force prefactor and (if requested) the energy.
+// Electrostatic part of one pair (charge-scaled): distance terms, the erfc
+// value, the force prefactor and (if requested) the energy. `qij_inv` is
+// (charge_scale * q_i q_j) / d, shared by prefactor and energy.
 template <typename Real, bool COMPUTE_U>
 __device__ __forceinline__ void electrostatics(
     const Real charge_scale,
@@ -92,14 +182,18 @@ __device__ __forceinline__ void electrostatics(
     Real &inv_d2,
     Real &erfc_bd,
     Real &prefactor,
-    Real &u) {
+    Real &u,
+    Real &qij_inv,
+    Real &factor) {
     inv_d = inv_sqrt(d2);
-    d = d2 * inv_d;
-    inv_d2 = inv_d * inv_d;
-    Real qij = qi * qj;
-    prefactor = charge_scale * qij * inv_d * es_factor(beta, d, inv_d2, erfc_bd);
+    d = fmul(d2, inv_d);
+    inv_d2 = fmul(inv_d, inv_d);
+    const Real qij = fmul(qi, qj);
+    qij_inv = fmul(fmul(charge_scale, qij), inv_d);
+    factor = es_factor(beta, d, inv_d2, erfc_bd);
+    prefactor = fmul(qij_inv, factor);
     if (COMPUTE_U) {
-        u = charge_scale * qij * inv_d * erfc_bd;
+        u = fmul(qij_inv, erfc_bd);
     }
 }
 
@@ -114,28 +208,52 @@ __device__ __forceinline__ void lennard_jones(
     const Real sig_j,
     const Real inv_d,
     const Real inv_d2,
+    const Real qij_inv,
+    const Real factor,
+    const Real erfc_bd,
     Real &u,
     Real &prefactor,
     Real &sig_grad,
     Real &eps_grad) {
-    Real eps_ij = eps_i * eps_j;
-    Real sig_ij = sig_i + sig_j;
-
-    Real s1 = sig_ij * inv_d;
-    Real s2 = s1 * s1;
-    Real s4 = s2 * s2;
-    Real s6 = s4 * s2;
-    Real s6_inv_d2 = s6 * inv_d2;
-    Real s5_inv_d = sig_ij * s4 * inv_d2;
-
-    Real lj_prefactor = lj_scale * eps_ij * s6_inv_d2 * (s6 * 48 - 24);
+    const Real eps_ij = fmul(eps_i, eps_j);
+    const Real sig_ij = fadd(sig_i, sig_j);
+    const Real s1 = fmul(sig_ij, inv_d);
+    const Real s2 = fmul(s1, s1);
+    const Real s4 = fmul(s2, s2);
+    const Real s6 = fmul(s4, s2);
+    const Real s6_inv_d2 = fmul(s6, inv_d2);
+    const Real s5_inv_d = fmul(fmul(sig_ij, s4), inv_d2);
+#if TMNB_DAG_S6M1
+    const Real s6m1 = ffma(s4, s2, (Real)-1);
+#else
+    const Real s6m1 = fsub(s6, (Real)1);
+#endif
+    const Real ljx = fmul(fmul(lj_scale, eps_ij), s6_inv_d2);
+    const Real ljy = madd(s6, (Real)48, (Real)-24, TMNB_DAG_LJP);
+#if TMNB_DAG_PRE == 1
+    prefactor = ffma(-ljx, ljy, prefactor);
+#elif TMNB_DAG_PRE == 0
+    prefactor = fsub(prefactor, fmul(ljx, ljy));
+#else
+    prefactor = ffma(qij_inv, factor, -fmul(ljx, ljy));
+#endif
     if (COMPUTE_U) {
-        u += lj_scale * 4 * eps_ij * (s6 - 1) * s6;
+        const Real A = fmul(fmul(fmul(lj_scale, (Real)4), eps_ij), s6m1);
+#if TMNB_DAG_U == 1
+        u = ffma(A, s6, u);
+#elif TMNB_DAG_U == 0
+        u = fadd(u, fmul(A, s6));
+#else
+        u = ffma(qij_inv, erfc_bd, fmul(A, s6));
+#endif
     }
-    prefactor -= lj_prefactor;
-
-    sig_grad = lj_scale * 24 * eps_ij * s5_inv_d * (2 * s6 - 1);
-    eps_grad = lj_scale * 4 * (s6 - 1) * s6;
+#if TMNB_DAG_2S6M1
+    const Real two_s6_m1 = fsub(ffma(s4, s2, s6), (Real)1);
+#else
+    const Real two_s6_m1 = ffma((Real)2, s6, (Real)-1);
+#endif
+    sig_grad = fmul(fmul(fmul(fmul(lj_scale, (Real)24), eps_ij), s5_inv_d), two_s6_m1);
+    eps_grad = fmul(fmul(fmul(lj_scale, (Real)4), s6m1), s6);
 }
 
 } // namespace tmb

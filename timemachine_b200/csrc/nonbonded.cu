@@ -7,8 +7,8 @@
 //   Nonbonded (timemachine/lib/potentials.py:269-301: AllPairs + negated
 //              PairList of the exclusions), evaluated as ONE pipeline whose
 //              exclusion pairs run inside the pair kernel's launch.
+#include "engine.hpp"
 #include "nb_kernels.cuh"
-#include "tmnb.h"
 
 #include <algorithm>
 #include <cmath>
@@ -20,74 +20,6 @@
 #include <vector>
 
 namespace tmb {
-
-namespace {
-
-thread_local std::string g_last_error;
-
-struct Error : std::runtime_error {
-    tmnb_status status;
-    Error(tmnb_status s, const std::string &msg) : std::runtime_error(msg), status(s) {}
-};
-
-void cuda_check(cudaError_t e, const char *what) {
-    if (e != cudaSuccess) {
-        throw Error(TMNB_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
-    }
-}
-#define CK(call) cuda_check((call), #call)
-
-template <typename T> struct DevBuf {
-    T *p = nullptr;
-    size_t n = 0;
-    DevBuf() = default;
-    DevBuf(const DevBuf &) = delete;
-    DevBuf &operator=(const DevBuf &) = delete;
-    ~DevBuf() { release(); }
-    void release() {
-        if (p) {
-            cudaFree(p);
-        }
-        p = nullptr;
-        n = 0;
-    }
-    void alloc(size_t count) {
-        release();
-        if (count == 0) {
-            return;
-        }
-        CK(cudaMalloc(&p, count * sizeof(T)));
-        n = count;
-    }
-    void ensure(size_t count) {
-        if (count > n) {
-            alloc(count);
-        }
-    }
-    void upload(const T *h, size_t count) {
-        alloc(count);
-        if (count) {
-            CK(cudaMemcpy(p, h, count * sizeof(T), cudaMemcpyHostToDevice));
-        }
-    }
-    void zero() {
-        if (n) {
-            CK(cudaMemset(p, 0, n * sizeof(T)));
-        }
-    }
-};
-
-int num_sms() {
-    static int sms = -1;
-    if (sms < 0) {
-        int dev = 0;
-        CK(cudaGetDevice(&dev));
-        CK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
-    }
-    return sms;
-}
-
-} // namespace
 
 enum class Kind { AllPairs, PairList, Nonbonded };
 
@@ -113,7 +45,7 @@ template <int... Is> struct KernelList {
 };
 using AllKernels = KernelList<0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 14, 15>;
 
-class NonbondedPotential {
+class NonbondedPotential : public PotentialBase {
   public:
     NonbondedPotential(
         Kind kind,
@@ -129,7 +61,11 @@ class NonbondedPotential {
         int M,
         bool negated,
         bool interpolated)
-        : kind_(kind), N_(N), beta_(beta), cutoff_(cutoff), interp_(interpolated), negated_(negated), M_(M) {
+        : kind_(kind), N_(N), beta_(beta), cutoff_(cutoff), interp_(interpolated), negated_(negated), M_(M),
+          h_plane_(plane, plane + N), h_offset_(offset, offset + N),
+          h_atom_idxs_(atom_idxs ? std::vector<int>(atom_idxs, atom_idxs + K) : std::vector<int>()),
+          h_pairs_(pair_idxs ? std::vector<int>(pair_idxs, pair_idxs + 2 * (size_t)M) : std::vector<int>()),
+          h_scales_(scales ? std::vector<double>(scales, scales + 2 * (size_t)M) : std::vector<double>()) {
         if (N <= 0) {
             throw Error(TMNB_ERR_INVALID_ARGUMENT, "N must be positive");
         }
@@ -234,9 +170,6 @@ class NonbondedPotential {
     }
 
     ~NonbondedPotential() {
-        if (host_stream_) {
-            cudaStreamDestroy(host_stream_);
-        }
         if (timing_) {
             cudaEventDestroy(ev_pair_[0]);
             cudaEventDestroy(ev_pair_[1]);
@@ -281,8 +214,29 @@ class NonbondedPotential {
         items_.alloc((size_t)std::max(1LL, cap));
     }
 
-    int num_params() const { return (interp_ ? 2 : 1) * N_ * 3; }
-    int num_atoms() const { return N_; }
+    int num_params() const override { return (interp_ ? 2 : 1) * N_ * 3; }
+    int num_atoms() const override { return N_; }
+
+    std::unique_ptr<PotentialBase> clone() const override {
+        auto c = std::make_unique<NonbondedPotential>(
+            kind_,
+            N_,
+            h_plane_.data(),
+            h_offset_.data(),
+            beta_,
+            cutoff_,
+            h_atom_idxs_.empty() ? nullptr : h_atom_idxs_.data(),
+            (int)h_atom_idxs_.size(),
+            h_pairs_.empty() ? nullptr : h_pairs_.data(),
+            h_scales_.empty() ? nullptr : h_scales_.data(),
+            M_,
+            negated_,
+            interp_);
+        c->padding_ = padding_;
+        c->hilbert_ = hilbert_;
+        c->set_chunk(chunk_);
+        return c;
+    }
 
     const char *name() const {
         switch (kind_) {
@@ -314,7 +268,7 @@ class NonbondedPotential {
         unsigned long long *d_du_dp,
         unsigned long long *d_du_dl,
         unsigned long long *d_u,
-        cudaStream_t stream) {
+        cudaStream_t stream) override {
         if (N != N_) {
             throw Error(
                 TMNB_ERR_INVALID_ARGUMENT,
@@ -466,7 +420,7 @@ class NonbondedPotential {
     }
 
     // Returns the sticky device error (and clears it).
-    tmnb_status check_device_error(cudaStream_t stream) {
+    tmnb_status check_device_error(cudaStream_t stream) override {
         CK(cudaStreamSynchronize(stream));
         DevState st;
         CK(cudaMemcpy(&st, state_.p, sizeof(st), cudaMemcpyDeviceToHost));
@@ -481,6 +435,38 @@ class NonbondedPotential {
                 "Cutoff with padding is more than half of the box width, neighborlist is no longer reliable");
         }
         return TMNB_OK;
+    }
+
+    // Copies the neighbour list of the last rebuild: slot order (perm, [S]),
+    // tiles per row block ([RB]) and the fixed-stride tile storage
+    // ([tile_offset(RB) * 32] column slots; row block rb owns tiles
+    // tile_offset(rb) .. + rb_ntiles[rb]).
+    void copy_nblist(cudaStream_t stream, unsigned *perm, int *rb_ntiles, unsigned *tile_cols) {
+        if (!has_nblist_) {
+            throw Error(TMNB_ERR_INVALID_ARGUMENT, "potential has no neighbour list");
+        }
+        CK(cudaStreamSynchronize(stream));
+        if (perm) {
+            CK(cudaMemcpy(perm, perm_.p, S_ * sizeof(unsigned), cudaMemcpyDeviceToHost));
+        }
+        if (rb_ntiles) {
+            CK(cudaMemcpy(rb_ntiles, rb_ntiles_.p, RB_ * sizeof(int), cudaMemcpyDeviceToHost));
+        }
+        if (tile_cols) {
+            CK(cudaMemcpy(tile_cols, tile_cols_.p, tile_cols_.n * sizeof(unsigned), cudaMemcpyDeviceToHost));
+        }
+    }
+
+    void nblist_shape(int *S, int *RB, long long *tile_capacity) const {
+        if (S) {
+            *S = S_;
+        }
+        if (RB) {
+            *RB = RB_;
+        }
+        if (tile_capacity) {
+            *tile_capacity = has_nblist_ ? tile_offset(RB_, RB_) : 0;
+        }
     }
 
     void stats(cudaStream_t stream, int *n_tiles, int *n_items, int *n_rebuilds) {
@@ -498,72 +484,7 @@ class NonbondedPotential {
         }
     }
 
-    cudaStream_t host_stream() {
-        if (!host_stream_) {
-            CK(cudaStreamCreateWithFlags(&host_stream_, cudaStreamNonBlocking));
-        }
-        return host_stream_;
-    }
-
-    void execute_host(
-        int N,
-        int P,
-        const double *h_x,
-        const double *h_p,
-        const double *h_box,
-        double lambda,
-        unsigned long long *h_du_dx,
-        unsigned long long *h_du_dp,
-        unsigned long long *h_du_dl,
-        unsigned long long *h_u) {
-        cudaStream_t s = host_stream();
-        const size_t nx = 3 * (size_t)N;
-        hx_.ensure(nx);
-        hp_.ensure(std::max(1, P));
-        hbox_.ensure(9);
-        CK(cudaMemcpyAsync(hx_.p, h_x, nx * sizeof(double), cudaMemcpyHostToDevice, s));
-        if (P > 0) {
-            CK(cudaMemcpyAsync(hp_.p, h_p, (size_t)P * sizeof(double), cudaMemcpyHostToDevice, s));
-        }
-        CK(cudaMemcpyAsync(hbox_.p, h_box, 9 * sizeof(double), cudaMemcpyHostToDevice, s));
-        unsigned long long *dx = nullptr, *dp = nullptr, *dl = nullptr, *du = nullptr;
-        if (h_du_dx) {
-            hdx_.ensure(nx);
-            dx = hdx_.p;
-            CK(cudaMemsetAsync(dx, 0, nx * sizeof(*dx), s));
-        }
-        if (h_du_dp) {
-            hdp_.ensure(std::max(1, P));
-            dp = hdp_.p;
-            CK(cudaMemsetAsync(dp, 0, (size_t)P * sizeof(*dp), s));
-        }
-        if (h_du_dl) {
-            hdl_.ensure(N);
-            dl = hdl_.p;
-            CK(cudaMemsetAsync(dl, 0, (size_t)N * sizeof(*dl), s));
-        }
-        if (h_u) {
-            hu_.ensure(N);
-            du = hu_.p;
-            CK(cudaMemsetAsync(du, 0, (size_t)N * sizeof(*du), s));
-        }
-        execute_device(N, P, hx_.p, hp_.p, hbox_.p, lambda, dx, dp, dl, du, s);
-        if (h_du_dx) {
-            CK(cudaMemcpyAsync(h_du_dx, dx, nx * sizeof(*dx), cudaMemcpyDeviceToHost, s));
-        }
-        if (h_du_dp) {
-            CK(cudaMemcpyAsync(h_du_dp, dp, (size_t)P * sizeof(*dp), cudaMemcpyDeviceToHost, s));
-        }
-        if (h_du_dl) {
-            CK(cudaMemcpyAsync(h_du_dl, dl, (size_t)N * sizeof(*dl), cudaMemcpyDeviceToHost, s));
-        }
-        if (h_u) {
-            CK(cudaMemcpyAsync(h_u, du, (size_t)N * sizeof(*du), cudaMemcpyDeviceToHost, s));
-        }
-        check_device_error(s);
-    }
-
-    void du_dp_fixed_to_float(int N, int P, const unsigned long long *du_dp, double *out) const {
+    void du_dp_fixed_to_float(int N, int P, const unsigned long long *du_dp, double *out) const override {
         const int tuples = P / 3;
         for (int i = 0; i < tuples; i++) {
             out[3 * i + 0] = (double)(long long)du_dp[3 * i + 0] / (double)FX_EXPONENT;
@@ -590,6 +511,9 @@ class NonbondedPotential {
     int grid_bits_ = 4;
     int chunk_ = 4;
 
+    std::vector<int> h_plane_, h_offset_, h_atom_idxs_, h_pairs_;
+    std::vector<double> h_scales_;
+
     DevBuf<int> plane_, offset_, set_atoms_, pair_idxs_, slot_of_;
     DevBuf<double> scales_;
     DevBuf<unsigned> perm_;
@@ -610,17 +534,9 @@ class NonbondedPotential {
     bool pair_timed_ = false;
     cudaEvent_t ev_pair_[2] = {nullptr, nullptr};
 
-    // execute_host staging
-    cudaStream_t host_stream_ = nullptr;
-    DevBuf<double> hx_, hp_, hbox_;
-    DevBuf<unsigned long long> hdx_, hdp_, hdl_, hu_;
 };
 
 } // namespace tmb
-
-struct tmnb_potential {
-    std::unique_ptr<tmb::NonbondedPotential> impl;
-};
 
 namespace tmb {
 
@@ -676,20 +592,12 @@ double fp32_peak_tflops() {
 
 namespace {
 
-template <typename F> tmnb_status guarded(F &&f) {
-    try {
-        f();
-        return TMNB_OK;
-    } catch (const tmb::Error &e) {
-        tmb::g_last_error = e.what();
-        return e.status;
-    } catch (const std::bad_alloc &) {
-        tmb::g_last_error = "host allocation failed";
-        return TMNB_ERR_INTERNAL;
-    } catch (const std::exception &e) {
-        tmb::g_last_error = e.what();
-        return TMNB_ERR_INTERNAL;
+tmb::NonbondedPotential *as_nb(tmnb_potential *p) {
+    auto *nb = dynamic_cast<tmb::NonbondedPotential *>(p->impl.get());
+    if (!nb) {
+        throw tmb::Error(TMNB_ERR_INVALID_ARGUMENT, "operation only defined for nonbonded potentials");
     }
+    return nb;
 }
 
 tmnb_status check_handle(const tmnb_potential *p) {
@@ -734,7 +642,7 @@ tmnb_status tmnb_all_pairs_create(
         tmb::g_last_error = "null argument";
         return TMNB_ERR_INVALID_ARGUMENT;
     }
-    return guarded([&] {
+    return tmb::guarded([&] {
         auto h = std::make_unique<tmnb_potential>();
         h->impl = std::make_unique<tmb::NonbondedPotential>(
             tmb::Kind::AllPairs,
@@ -774,7 +682,7 @@ tmnb_status tmnb_pair_list_create(
         tmb::g_last_error = "null argument";
         return TMNB_ERR_INVALID_ARGUMENT;
     }
-    return guarded([&] {
+    return tmb::guarded([&] {
         auto h = std::make_unique<tmnb_potential>();
         h->impl = std::make_unique<tmb::NonbondedPotential>(
             tmb::Kind::PairList,
@@ -813,7 +721,7 @@ tmnb_status tmnb_nonbonded_create(
         tmb::g_last_error = "null argument";
         return TMNB_ERR_INVALID_ARGUMENT;
     }
-    return guarded([&] {
+    return tmb::guarded([&] {
         auto h = std::make_unique<tmnb_potential>();
         h->impl = std::make_unique<tmb::NonbondedPotential>(
             tmb::Kind::Nonbonded,
@@ -837,7 +745,7 @@ tmnb_status tmnb_potential_destroy(tmnb_potential *pot) {
     if (pot == nullptr) {
         return TMNB_OK;
     }
-    return guarded([&] { delete pot; });
+    return tmb::guarded([&] { delete pot; });
 }
 
 tmnb_status tmnb_potential_execute_device(
@@ -856,7 +764,7 @@ tmnb_status tmnb_potential_execute_device(
     if (tmnb_status s = check_handle(pot)) {
         return s;
     }
-    return guarded([&] {
+    return tmb::guarded([&] {
         pot->impl->execute_device(
             N, P, d_x, d_p, d_box, lambda, d_du_dx, d_du_dp, d_du_dl, d_u, static_cast<cudaStream_t>(stream));
     });
@@ -881,7 +789,7 @@ tmnb_status tmnb_potential_execute_host(
         tmb::g_last_error = "null argument";
         return TMNB_ERR_INVALID_ARGUMENT;
     }
-    return guarded([&] { pot->impl->execute_host(N, P, h_x, h_p, h_box, lambda, h_du_dx, h_du_dp, h_du_dl, h_u); });
+    return tmb::guarded([&] { pot->impl->execute_host(N, P, h_x, h_p, h_box, lambda, h_du_dx, h_du_dp, h_du_dl, h_u); });
 }
 
 tmnb_status tmnb_potential_execute_batch_host(
@@ -906,7 +814,7 @@ tmnb_status tmnb_potential_execute_batch_host(
         tmb::g_last_error = "invalid batch arguments";
         return TMNB_ERR_INVALID_ARGUMENT;
     }
-    return guarded([&] {
+    return tmb::guarded([&] {
         size_t e = 0;
         for (int c = 0; c < coord_batches; c++) {
             for (int p = 0; p < param_batches; p++) {
@@ -937,28 +845,28 @@ tmnb_status tmnb_potential_du_dp_fixed_to_float(
         tmb::g_last_error = "null argument";
         return TMNB_ERR_INVALID_ARGUMENT;
     }
-    return guarded([&] { pot->impl->du_dp_fixed_to_float(N, P, du_dp, du_dp_float); });
+    return tmb::guarded([&] { pot->impl->du_dp_fixed_to_float(N, P, du_dp, du_dp_float); });
 }
 
 tmnb_status tmnb_potential_set_nblist_padding(tmnb_potential *pot, double padding) {
     if (tmnb_status s = check_handle(pot)) {
         return s;
     }
-    return guarded([&] { pot->impl->set_padding(padding); });
+    return tmb::guarded([&] { as_nb(pot)->set_padding(padding); });
 }
 
 tmnb_status tmnb_potential_disable_hilbert_sort(tmnb_potential *pot) {
     if (tmnb_status s = check_handle(pot)) {
         return s;
     }
-    return guarded([&] { pot->impl->disable_hilbert(); });
+    return tmb::guarded([&] { as_nb(pot)->disable_hilbert(); });
 }
 
 tmnb_status tmnb_potential_check_device_error(tmnb_potential *pot, void *stream) {
     if (tmnb_status s = check_handle(pot)) {
         return s;
     }
-    return guarded([&] { pot->impl->check_device_error(static_cast<cudaStream_t>(stream)); });
+    return tmb::guarded([&] { pot->impl->check_device_error(static_cast<cudaStream_t>(stream)); });
 }
 
 tmnb_status tmnb_potential_nblist_stats(
@@ -966,14 +874,30 @@ tmnb_status tmnb_potential_nblist_stats(
     if (tmnb_status s = check_handle(pot)) {
         return s;
     }
-    return guarded([&] { pot->impl->stats(static_cast<cudaStream_t>(stream), n_tiles, n_items, n_rebuilds); });
+    return tmb::guarded([&] { as_nb(pot)->stats(static_cast<cudaStream_t>(stream), n_tiles, n_items, n_rebuilds); });
+}
+
+tmnb_status tmnb_potential_nblist_shape(tmnb_potential *pot, int *S, int *RB, long long *tile_capacity) {
+    if (tmnb_status s = check_handle(pot)) {
+        return s;
+    }
+    return tmb::guarded([&] { as_nb(pot)->nblist_shape(S, RB, tile_capacity); });
+}
+
+tmnb_status tmnb_potential_copy_nblist(
+    tmnb_potential *pot, void *stream, unsigned *perm, int *row_block_ntiles, unsigned *tile_cols) {
+    if (tmnb_status s = check_handle(pot)) {
+        return s;
+    }
+    return tmb::guarded(
+        [&] { as_nb(pot)->copy_nblist(static_cast<cudaStream_t>(stream), perm, row_block_ntiles, tile_cols); });
 }
 
 tmnb_status tmnb_potential_enable_timing(tmnb_potential *pot, int on) {
     if (tmnb_status s = check_handle(pot)) {
         return s;
     }
-    return guarded([&] { pot->impl->enable_timing(on != 0); });
+    return tmb::guarded([&] { as_nb(pot)->enable_timing(on != 0); });
 }
 
 tmnb_status tmnb_potential_last_pair_kernel_ms(tmnb_potential *pot, float *ms) {
@@ -984,7 +908,7 @@ tmnb_status tmnb_potential_last_pair_kernel_ms(tmnb_potential *pot, float *ms) {
         tmb::g_last_error = "null argument";
         return TMNB_ERR_INVALID_ARGUMENT;
     }
-    return guarded([&] { *ms = pot->impl->last_pair_ms(); });
+    return tmb::guarded([&] { *ms = as_nb(pot)->last_pair_ms(); });
 }
 
 tmnb_status tmnb_probe_fp32_peak(double *tflops) {
@@ -992,7 +916,7 @@ tmnb_status tmnb_probe_fp32_peak(double *tflops) {
         tmb::g_last_error = "null argument";
         return TMNB_ERR_INVALID_ARGUMENT;
     }
-    return guarded([&] { *tflops = tmb::fp32_peak_tflops(); });
+    return tmb::guarded([&] { *tflops = tmb::fp32_peak_tflops(); });
 }
 
 int tmnb_potential_num_params(const tmnb_potential *pot) {

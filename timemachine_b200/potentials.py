@@ -238,6 +238,26 @@ class Potential:
             stream = stream.cuda_stream
         _lib.check(self._lib.tmnb_potential_check_device_error(self._h, ctypes.c_void_p(stream)))
 
+    def get_nblist(self, stream=None):
+        """(perm [S] slot -> atom, tiles) of the last rebuild; tiles[rb] is an
+        array of the atom indices interacting with row block rb (slots rb*32..)."""
+        S, RB, cap = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_longlong()
+        _lib.check(self._lib.tmnb_potential_nblist_shape(self._h, ctypes.byref(S), ctypes.byref(RB), ctypes.byref(cap)))
+        perm = np.zeros(S.value, dtype=np.uint32)
+        nt = np.zeros(RB.value, dtype=np.int32)
+        cols = np.zeros(cap.value * 32, dtype=np.uint32)
+        s = 0
+        if stream is not None:
+            s = stream.cuda_stream if hasattr(stream, "cuda_stream") else stream
+        _lib.check(self._lib.tmnb_potential_copy_nblist(self._h, ctypes.c_void_p(s), _ptr(perm), _ptr(nt), _ptr(cols)))
+        R = RB.value
+        tiles = []
+        for rb in range(R):
+            off = rb * R - (rb * (rb - 1)) // 2
+            c = cols[off * 32 : (off + nt[rb]) * 32]
+            tiles.append(c[c < S.value])
+        return perm, tiles
+
     def nblist_stats(self, stream=None):
         """(tiles, work items, rebuilds) of the last neighbour-list build (synchronises)."""
         t, i, r = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
@@ -487,9 +507,39 @@ class NonbondedInterpolated(Nonbonded):
     _interpolated = True
 
 
+class _BondedWrapper(CustomOpWrapper):
+    """timemachine/lib/potentials.py:162-196: args (idxs, lambda_mult=None, lambda_offset=None)."""
+
+    _arity = 2
+    _ctor = "tmnb_harmonic_bond_create"
+
+    def unbound_impl(self, precision):
+        _check_precision(precision)
+        idxs = np.ascontiguousarray(self.args[0], dtype=np.int32).reshape(-1, self._arity)
+        T = idxs.shape[0]
+        mult = self.args[1] if len(self.args) > 1 else None
+        off = self.args[2] if len(self.args) > 2 else None
+        mult = None if mult is None else np.ascontiguousarray(mult, dtype=np.int32)
+        off = None if off is None else np.ascontiguousarray(off, dtype=np.int32)
+        h = ctypes.c_void_p()
+        lib = _lib.lib()
+        _lib.check(getattr(lib, self._ctor)(0, T, _ptr(idxs), _ptr(mult), _ptr(off), ctypes.byref(h)))
+        return Potential(h, type(self).__name__, False)
+
+
+class HarmonicBond(_BondedWrapper):
+    _arity = 2
+    _ctor = "tmnb_harmonic_bond_create"
+
+
+class HarmonicAngle(_BondedWrapper):
+    _arity = 3
+    _ctor = "tmnb_harmonic_angle_create"
+
+
 def all_flag_combinations():
     """The 16 (du_dx, du_dp, du_dl, u) request combinations (tests/common.py:451)."""
     return list(itertools.product([False, True], repeat=4))
 
 
-__all__ += ["all_flag_combinations", "FIXED_EXPONENT"]
+__all__ += ["all_flag_combinations", "FIXED_EXPONENT", "HarmonicBond", "HarmonicAngle"]

@@ -29,6 +29,13 @@ O_EPS = 0.636386
 MASS_O = 15.999
 MASS_H = 1.008
 MASS_LIG = 12.011
+# flexible-water and ligand bonded constants (cosine-angle force constants)
+WATER_KB = 345000.0
+WATER_KA = 400.0
+LIG_KB = 250000.0
+LIG_B0 = 0.15
+LIG_KA = 300.0
+LIG_A0 = np.deg2rad(109.5)
 # volume per water molecule at 1 g/cm^3 (nm^3): 18.015 g/mol / (602.214 nm^3 g/cm^3 per mol)
 WATER_VOLUME = 18.015 / 602.214076
 
@@ -48,6 +55,11 @@ class System:
     ligand_idxs: np.ndarray = field(default_factory=lambda: np.zeros(0, dtype=np.int32))
     beta: float = 2.0
     cutoff: float = 1.2
+    # bonded terms (HarmonicBond [B,2] (kb, b0), HarmonicAngle [A,3] vertex-middle (ka, a0))
+    bond_idxs: np.ndarray = field(default_factory=lambda: np.zeros((0, 2), dtype=np.int32))
+    bond_params: np.ndarray = field(default_factory=lambda: np.zeros((0, 2)))
+    angle_idxs: np.ndarray = field(default_factory=lambda: np.zeros((0, 3), dtype=np.int32))
+    angle_params: np.ndarray = field(default_factory=lambda: np.zeros((0, 2)))
 
     @property
     def N(self):
@@ -205,6 +217,21 @@ def build_system(
     else:
         x, params, excl, scales, masses, group_of = xw, pw, ew.astype(np.int32), sw, mw, gw
         lig_idxs = np.zeros(0, dtype=np.int32)
+    # bonded terms: O-H bonds and the H-O-H angle of every water; chain bonds/angles of the ligand
+    bw = np.concatenate([np.stack([base, base + 1], 1), np.stack([base, base + 2], 1)]).astype(np.int32)
+    bpw = np.tile([WATER_KB, WATER_BOND], (bw.shape[0], 1))
+    aw = np.stack([base + 1, base, base + 2], 1).astype(np.int32)
+    apw = np.tile([WATER_KA, WATER_ANGLE], (aw.shape[0], 1))
+    if lig is not None:
+        li = np.arange(n_ligand, dtype=np.int32) + N_w
+        bl = np.stack([li[:-1], li[1:]], 1)
+        al = np.stack([li[:-2], li[1:-1], li[2:]], 1)
+        bond_idxs = np.concatenate([bw, bl])
+        bond_params = np.concatenate([bpw, np.tile([LIG_KB, LIG_B0], (bl.shape[0], 1))])
+        angle_idxs = np.concatenate([aw, al])
+        angle_params = np.concatenate([apw, np.tile([LIG_KA, LIG_A0], (al.shape[0], 1))])
+    else:
+        bond_idxs, bond_params, angle_idxs, angle_params = bw, bpw, aw, apw
     N = x.shape[0]
     plane = np.zeros(N, dtype=np.int32)
     offset = np.zeros(N, dtype=np.int32)
@@ -223,6 +250,10 @@ def build_system(
         ligand_idxs=lig_idxs,
         beta=beta,
         cutoff=cutoff,
+        bond_idxs=np.ascontiguousarray(bond_idxs, dtype=np.int32),
+        bond_params=np.ascontiguousarray(bond_params, dtype=np.float64),
+        angle_idxs=np.ascontiguousarray(angle_idxs, dtype=np.int32),
+        angle_params=np.ascontiguousarray(angle_params, dtype=np.float64),
     )
 
 
