@@ -4,9 +4,11 @@
 Workload (one "step"): the 12 lambda windows (evenly spaced on [0, 1]) of the
 22,840-atom water + ligand box (7,600 TIP3P-like waters + a 40-atom ligand
 decoupled through w = 1.2 nm * lambda), each window one full nonbonded
-evaluation (u, du_dx, du_dp, du_dl) through the C ABI on device-resident
-inputs. Synthetic, seeded inputs stand in for the reference's DHFR system
-(which needs OpenMM to parametrise).
+evaluation (u, du_dx, du_dp, du_dl), all 12 through ONE multi-window call of
+the C ABI (tmnb_potential_execute_windows_device) on device-resident inputs.
+The same 12 windows as 12 single-window calls are reported beside it.
+Synthetic, seeded inputs stand in for the reference's DHFR system (which
+needs OpenMM to parametrise).
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl tmnb|reference]
 
@@ -57,10 +59,16 @@ def parse():
         "--profile",
         type=int,
         default=0,
-        help="run only this many evaluations of the workload (one per lambda window, cycling) and exit; "
+        help="run only this many steps of the workload and exit; "
         "the command profiled by ncu for the committed kernel summaries",
     )
     ap.add_argument("--profile-outputs", default="all", choices=["all", "du_dx", "u"])
+    ap.add_argument(
+        "--profile-mode",
+        default="windows",
+        choices=["windows", "single"],
+        help="windows: one 12-window call per step; single: one single-window call per step (cycling lambdas)",
+    )
     return ap.parse_args()
 
 
@@ -77,15 +85,19 @@ def run_profile(args, local):
     dp = torch.as_tensor(p, device=dev).reshape(-1)
     db = torch.as_tensor(s.box, device=dev)
     N = s.N
+    K = N_WINDOWS if args.profile_mode == "windows" else 1
     want = args.profile_outputs
-    o_dx = torch.zeros((N, 3), dtype=torch.int64, device=dev) if want in ("all", "du_dx") else None
-    o_dp = torch.zeros(p.size, dtype=torch.int64, device=dev) if want == "all" else None
-    o_dl = torch.zeros(N, dtype=torch.int64, device=dev) if want == "all" else None
-    o_u = torch.zeros(N, dtype=torch.int64, device=dev) if want in ("all", "u") else None
+    o_dx = torch.zeros((K, N, 3), dtype=torch.int64, device=dev) if want in ("all", "du_dx") else None
+    o_dp = torch.zeros((K, p.size), dtype=torch.int64, device=dev) if want == "all" else None
+    o_dl = torch.zeros((K, N), dtype=torch.int64, device=dev) if want == "all" else None
+    o_u = torch.zeros((K, N), dtype=torch.int64, device=dev) if want in ("all", "u") else None
     for k in range(args.profile):
-        impl.execute_device(dx, dp, db, float(lambdas[k % N_WINDOWS]), o_dx, o_dp, o_dl, o_u)
+        if K > 1:
+            impl.execute_windows_device(dx, dp, db, lambdas, o_dx, o_dp, o_dl, o_u)
+        else:
+            impl.execute_device(dx, dp, db, float(lambdas[k % N_WINDOWS]), o_dx, o_dp, o_dl, o_u)
     torch.cuda.synchronize()
-    print(json.dumps({"profile_evals": args.profile, "outputs": want, "nblist": impl.nblist_stats()}))
+    print(json.dumps({"profile_steps": args.profile, "mode": args.profile_mode, "outputs": want, "nblist": impl.nblist_stats()}))
 
 
 def dist_setup():
@@ -143,7 +155,7 @@ class ClockSampler:
             os.close(fd)
             self.proc = subprocess.Popen(
                 ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.QUERY}", "--format=csv,noheader,nounits",
-                 "-lms", "200"],
+                 "-lms", "100"],
                 stdout=open(self.path, "w"),
                 stderr=subprocess.DEVNULL,
             )
@@ -198,7 +210,9 @@ def build_workload(rank):
 
 
 def count_pairs(s, x, lambdas):
-    """In-cutoff pairs (4D distance < cutoff) per window, and how many carry LJ."""
+    """In-cutoff pairs (4D distance < cutoff) per window, and how many carry LJ;
+    plus the pairs one multi-window evaluation computes: pairs of two
+    lambda-independent atoms once, the others once per window."""
     from scipy.spatial import cKDTree
 
     L = np.diag(s.box)
@@ -211,12 +225,19 @@ def count_pairs(s, x, lambdas):
     d2 = (d * d).sum(1)
     lj = (s.params[i, 2] != 0) & (s.params[j, 2] != 0)
     excl = set(map(tuple, np.sort(s.exclusion_idxs, axis=1).tolist()))
+    dep_atom = s.lambda_offset_idxs != 0
+    dep = dep_atom[i] | dep_atom[j]
     out = []
-    for lam in lambdas:
+    shared = [0, 0]
+    for k, lam in enumerate(lambdas):
         w = s.cutoff * (s.lambda_plane_idxs + s.lambda_offset_idxs * lam)
         keep = d2 + (w[i] - w[j]) ** 2 < s.cutoff**2
         out.append((int(keep.sum()), int((keep & lj).sum())))
-    return out, len(excl)
+        if k == 0:
+            shared = [int((keep & ~dep).sum()), int((keep & ~dep & lj).sum())]
+        shared[0] += int((keep & dep).sum())
+        shared[1] += int((keep & dep & lj).sum())
+    return out, len(excl), tuple(shared)
 
 
 def measured_peaks():
@@ -242,78 +263,101 @@ def run_tmnb(args, world, rank, local):
     dx = torch.as_tensor(x, device=dev)
     dp = torch.as_tensor(p, device=dev).reshape(-1)
     db = torch.as_tensor(s.box, device=dev)
-    o_dx = torch.zeros((N, 3), dtype=torch.int64, device=dev)
-    o_dp = torch.zeros(p.size, dtype=torch.int64, device=dev)
-    o_dl = torch.zeros(N, dtype=torch.int64, device=dev)
-    o_u = torch.zeros(N, dtype=torch.int64, device=dev)
+    K = N_WINDOWS
+    o_dx = torch.zeros((K, N, 3), dtype=torch.int64, device=dev)
+    o_dp = torch.zeros((K, p.size), dtype=torch.int64, device=dev)
+    o_dl = torch.zeros((K, N), dtype=torch.int64, device=dev)
+    o_u = torch.zeros((K, N), dtype=torch.int64, device=dev)
     flush = torch.empty(256 << 20, dtype=torch.uint8, device=dev)
     stream = torch.cuda.current_stream(dev)
     lib = _lib.lib()
 
     def one_step():
-        for lam in lambdas:
-            o_dx.zero_()
-            o_dp.zero_()
-            o_dl.zero_()
-            o_u.zero_()
-            impl.execute_device(dx, dp, db, float(lam), o_dx, o_dp, o_dl, o_u, stream=stream)
+        o_dx.zero_()
+        o_dp.zero_()
+        o_dl.zero_()
+        o_u.zero_()
+        impl.execute_windows_device(dx, dp, db, lambdas, o_dx, o_dp, o_dl, o_u, stream=stream)
 
-    for _ in range(args.warmup):
-        one_step()
-    torch.cuda.synchronize()
-    tiles, items, rebuilds = impl.nblist_stats()
+    def one_step_sequential():
+        for k, lam in enumerate(lambdas):
+            o_dx[k].zero_()
+            o_dp[k].zero_()
+            o_dl[k].zero_()
+            o_u[k].zero_()
+            impl.execute_device(dx, dp, db, float(lam), o_dx[k], o_dp[k], o_dl[k], o_u[k], stream=stream)
 
-    # timed region: K steps, L2 flushed before each, events around each step
-    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    barrier(world)
-    torch.cuda.synchronize()
-    with ClockSampler(local) as clk:
+    def timed(step_fn):
+        for _ in range(args.warmup):
+            step_fn()
+        torch.cuda.synchronize()
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+        barrier(world)
+        torch.cuda.synchronize()
         for k in range(args.steps):
             flush.zero_()
             evs[k][0].record(stream)
-            one_step()
+            step_fn()
             evs[k][1].record(stream)
         torch.cuda.synchronize()
-    barrier(world)
-    total_ms = sum(a.elapsed_time(b) for a, b in evs)
-    total_ms = max_over_ranks(total_ms, world)
+        barrier(world)
+        return max_over_ranks(sum(a.elapsed_time(b) for a, b in evs), world)
+
+    # timed region: K steps, L2 flushed before each, events around each step
+    clk = ClockSampler(local).__enter__()  # sampled through the timed evaluations and the MD run
+    total_ms = timed(one_step)
+    tiles, items, rebuilds = impl.nblist_stats()
+    seq_ms = timed(one_step_sequential)
     ms_per_step = total_ms / args.steps
     evals = args.steps * N_WINDOWS * world
     value = evals / (total_ms / 1e3)
+    seq_value = evals / (seq_ms / 1e3)
 
-    # pair-kernel duration (events on the launching stream) for the roofline
+    # pair-kernel duration of the multi-window launch (events on the launching stream)
     _lib.check(lib.tmnb_potential_enable_timing(impl.handle, 1))
     pair_ms = []
-    for _ in range(3):
+    for _ in range(5):
+        flush.zero_()
+        one_step()
+        ms = ctypes.c_float()
+        _lib.check(lib.tmnb_potential_last_pair_kernel_ms(impl.handle, ctypes.byref(ms)))
+        pair_ms.append(ms.value)
+    pair_ms_single = []
+    for _ in range(2):
         for lam in lambdas:
             flush.zero_()
-            impl.execute_device(dx, dp, db, float(lam), o_dx, o_dp, o_dl, o_u, stream=stream)
+            impl.execute_device(dx, dp, db, float(lam), o_dx[0], o_dp[0], o_dl[0], o_u[0], stream=stream)
             ms = ctypes.c_float()
             _lib.check(lib.tmnb_potential_last_pair_kernel_ms(impl.handle, ctypes.byref(ms)))
-            pair_ms.append(ms.value)
+            pair_ms_single.append(ms.value)
     _lib.check(lib.tmnb_potential_enable_timing(impl.handle, 0))
     peak = ctypes.c_double()
     _lib.check(lib.tmnb_probe_fp32_peak(ctypes.byref(peak)))
-    counts, n_excl = count_pairs(s, x, lambdas)
-    flops_per_window = [c * FLOPS_PER_PAIR + lj * FLOPS_PER_LJ_PAIR for c, lj in counts]
-    flops_eval = float(np.mean(flops_per_window))
+    counts, n_excl, (shared_pairs, shared_lj) = count_pairs(s, x, lambdas)
+    flops_launch = shared_pairs * FLOPS_PER_PAIR + shared_lj * FLOPS_PER_LJ_PAIR
     pair_s = float(np.mean(pair_ms)) / 1e3
-    achieved = flops_eval / pair_s / 1e12
+    achieved = flops_launch / pair_s / 1e12
+    flops_single = float(np.mean([c * FLOPS_PER_PAIR + lj * FLOPS_PER_LJ_PAIR for c, lj in counts]))
+    achieved_single = flops_single / (float(np.mean(pair_ms_single)) / 1e3) / 1e12
 
     # end to end through the C-ABI host entry (pinned host buffers, copies inside)
     hx = torch.as_tensor(x).pin_memory().numpy()
     hp = torch.as_tensor(p).pin_memory().numpy()
     hb = torch.as_tensor(s.box).pin_memory().numpy()
-    outs = [torch.zeros(sh, dtype=torch.int64).pin_memory().numpy().view(np.uint64) for sh in [(N, 3), (p.size,), (N,), (N,)]]
+    hl = torch.as_tensor(lambdas).pin_memory().numpy()
+    outs = [
+        torch.zeros(sh, dtype=torch.int64).pin_memory().numpy().view(np.uint64)
+        for sh in [(K, N, 3), (K, p.size), (K, N), (K, N)]
+    ]
 
     def host_step():
-        for lam in lambdas:
-            _lib.check(
-                lib.tmnb_potential_execute_host(
-                    impl.handle, N, p.size, hx.ctypes.data_as(ctypes.c_void_p), hp.ctypes.data_as(ctypes.c_void_p),
-                    hb.ctypes.data_as(ctypes.c_void_p), float(lam), *[o.ctypes.data_as(ctypes.c_void_p) for o in outs],
-                )
+        _lib.check(
+            lib.tmnb_potential_execute_windows_host(
+                impl.handle, N, p.size, hx.ctypes.data_as(ctypes.c_void_p), hp.ctypes.data_as(ctypes.c_void_p),
+                hb.ctypes.data_as(ctypes.c_void_p), K, hl.ctypes.data_as(ctypes.c_void_p),
+                *[o.ctypes.data_as(ctypes.c_void_p) for o in outs],
             )
+        )
 
     for _ in range(max(1, args.warmup)):
         host_step()
@@ -326,10 +370,10 @@ def run_tmnb(args, world, rank, local):
     barrier(world)
     e2e_s = max_over_ranks(t1 - t0, world)
     e2e_value = e2e_steps * N_WINDOWS * world / e2e_s
-    h2d = N_WINDOWS * (hx.nbytes + hp.nbytes + hb.nbytes)
-    d2h = N_WINDOWS * sum(o.nbytes for o in outs)
+    h2d = hx.nbytes + hp.nbytes + hb.nbytes + hl.nbytes
+    d2h = sum(o.nbytes for o in outs)
 
-    launches_per_eval = 8  # check/prepare, 5 rebuild-path kernels (early exit unless rebuilding), pair, finalize
+    launches_per_step = 8  # check/prepare, 5 rebuild-path kernels (early exit unless rebuilding), pair, finalize
     result = {
         "metric": "nonbonded evals/s at 22,840 atoms (u, du_dx, du_dp, du_dl; 12 lambda windows per step)",
         "value": value,
@@ -344,7 +388,7 @@ def run_tmnb(args, world, rank, local):
         "dtype": "f32 pair arithmetic, int64 fixed-point accumulation",
         "data": "synthetic (seeded water + ligand box; DHFR needs OpenMM)",
         "config": {
-            "workload": "water_ligand_22840: 7,600 waters + 40-atom ligand, 6.1 nm box, cutoff 1.2, beta 2.0, 12 lambda windows",
+            "workload": "water_ligand_22840: 7,600 waters + 40-atom ligand, 6.1 nm box, cutoff 1.2, beta 2.0, 12 lambda windows in one multi-window call",
             "atoms": N,
             "exclusions": int(n_excl),
             "pairs_in_cutoff_per_eval": int(np.mean([c for c, _ in counts])),
@@ -352,9 +396,10 @@ def run_tmnb(args, world, rank, local):
             "nblist_items": items,
             "l2": "flushed before every timed step (256 MiB write)",
             "parallelism": f"replicas x{world}",
+            "pairs_per_multi_window_launch": int(shared_pairs),
         },
         "e2e": {"value": e2e_value, "unit": "evals/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
-        "gpu_launches": launches_per_eval * N_WINDOWS * args.steps,
+        "gpu_launches": launches_per_step * args.steps,
         "roofline": {
             "bound": "fp32",
             "achieved": achieved,
@@ -362,17 +407,27 @@ def run_tmnb(args, world, rank, local):
             "unit": "TFLOP/s",
             "frac": achieved / peak.value,
             "traffic": None,
-            "kernel": "k_pair (full variant)",
+            "kernel": "k_pair (full variant, 12 windows in one launch)",
             "pair_kernel_ms": float(np.mean(pair_ms)),
+            "flops_per_launch": float(flops_launch),
             "peak_source": "measured by tmnb_probe_fp32_peak (FMA chains) on this GPU",
         },
-        "clocks": clk.summary(),
+        "single_window_calls": {
+            "value": seq_value,
+            "unit": "evals/s",
+            "ms_per_step": seq_ms / args.steps,
+            "pair_kernel_ms": float(np.mean(pair_ms_single)),
+            "achieved_tflops": achieved_single,
+            "note": "the same 12 windows as 12 tmnb_potential_execute_device calls",
+        },
     }
     try:
         result["md"] = run_md_tmnb()
         result["ns_per_day"] = result["md"]["ns_per_day"]
     except Exception as e:  # report, do not hide the evaluation numbers
         result["md"] = {"error": str(e)[:300]}
+    clk.__exit__()
+    result["clocks"] = clk.summary()
     return result
 
 

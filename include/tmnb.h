@@ -35,6 +35,9 @@ extern "C" {
 
 typedef struct tmnb_potential tmnb_potential;
 
+/* Lambda windows evaluated together by one multi-window call. */
+#define TMNB_MAX_WINDOWS 32
+
 typedef enum tmnb_status {
     TMNB_OK = 0,
     TMNB_ERR_INVALID_ARGUMENT = 1,
@@ -157,10 +160,57 @@ tmnb_status tmnb_potential_execute_host(
     unsigned long long *h_u);
 
 /*
+ * Multi-window device entry (no single reference counterpart: replaces the
+ * loop over lambda windows that execute_selective_batch
+ * (timemachine/cpp/src/wrap_kernels.cpp:381-551) and multiple_steps_U
+ * (timemachine/cpp/src/context.cu:71-147) run with one execute_device per
+ * window). Evaluates K lambda windows (1 <= K <= TMNB_MAX_WINDOWS) of the same coordinates
+ * and parameters in one launch sequence; window k's outputs start at
+ * d_du_dx + 3*N*k, d_du_dp + P*k, d_du_dl + N*k, d_u + N*k and ACCUMULATE
+ * (+=), as execute_device does. Each window's result equals that of
+ * tmnb_potential_execute_device at lambdas[k], bit for bit. `lambdas` is a
+ * HOST array.
+ */
+tmnb_status tmnb_potential_execute_windows_device(
+    tmnb_potential *pot,
+    int N,
+    int P,
+    const double *d_x,
+    const double *d_p,
+    const double *d_box,
+    int K,
+    const double *lambdas,       /* [K], host memory */
+    unsigned long long *d_du_dx, /* [K,N,3] or NULL */
+    unsigned long long *d_du_dp, /* [K,P] or NULL */
+    unsigned long long *d_du_dl, /* [K,N] or NULL */
+    unsigned long long *d_u,     /* [K,N] or NULL */
+    void *stream);
+
+/*
+ * Host form of tmnb_potential_execute_windows_device, with the copy-in /
+ * overwrite / copy-out / synchronise behaviour of tmnb_potential_execute_host.
+ */
+tmnb_status tmnb_potential_execute_windows_host(
+    tmnb_potential *pot,
+    int N,
+    int P,
+    const double *h_x,
+    const double *h_p,
+    const double *h_box,
+    int K,
+    const double *lambdas,       /* [K] */
+    unsigned long long *h_du_dx, /* [K,N,3] or NULL */
+    unsigned long long *h_du_dp, /* [K,P] or NULL */
+    unsigned long long *h_du_dl, /* [K,N] or NULL */
+    unsigned long long *h_u);    /* [K,N] or NULL */
+
+/*
  * Batched host entry: replaces Potential::execute_batch_host behind
  * execute_selective_batch (timemachine/cpp/src/wrap_kernels.cpp:381-551).
  * Executes every (coords, params, lambda) combination; outputs have the
- * leading shape [coord_batches, param_batches, lambda_batches].
+ * leading shape [coord_batches, param_batches, lambda_batches]. The lambda
+ * windows of one (coords, params) pair run as one multi-window evaluation
+ * (32 windows at a time).
  */
 tmnb_status tmnb_potential_execute_batch_host(
     tmnb_potential *pot,
@@ -262,6 +312,27 @@ tmnb_status tmnb_context_multiple_steps(
     int store_du_dl_interval,
     double *du_dl_out,
     int store_x_interval,
+    double *x_out,
+    double *box_out,
+    int use_graphs);
+
+/* Context::multiple_steps_U (timemachine/cpp/src/context.cu:139-234): runs
+ * n_steps steps at `lambda`; every store_u_interval steps stores the total
+ * potential energy at each of the n_windows lambda_windows into
+ * u_out[n_steps/store_u_interval][n_windows] (host), computed with one
+ * multi-window evaluation per potential (TMNB_MAX_WINDOWS windows at a time);
+ * coordinates/box every store_x_interval steps into x_out/box_out (host).
+ * Both intervals must be positive ("store_u_interval <= 0" /
+ * "store_x_interval <= 0" otherwise, as the reference throws). */
+tmnb_status tmnb_context_multiple_steps_U(
+    tmnb_context *ctx,
+    double lambda,
+    int n_steps,
+    int n_windows,
+    const double *lambda_windows,
+    int store_u_interval,
+    int store_x_interval,
+    double *u_out,
     double *x_out,
     double *box_out,
     int use_graphs);

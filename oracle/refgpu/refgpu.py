@@ -69,6 +69,13 @@ class RefNonbonded:
 
     def __init__(self, exclusion_idxs, scales, plane, offset, beta, cutoff, interpolated=False):
         L = lib()
+        exclusion_idxs = np.asarray(exclusion_idxs).reshape(-1, 2)
+        scales = np.asarray(scales).reshape(-1, 2)
+        if exclusion_idxs.shape[0] == 0:
+            # the reference's pair-list launch has an empty grid for zero pairs
+            # (invalid configuration -> exit); a zero-scale pair contributes 0
+            exclusion_idxs = np.array([[0, 1]])
+            scales = np.zeros((1, 2))
         self._keep = [
             np.ascontiguousarray(exclusion_idxs, dtype=np.int32).reshape(-1, 2),
             np.ascontiguousarray(scales, dtype=np.float64).reshape(-1, 2),

@@ -65,6 +65,8 @@ def _declare(lib):
     lib.tmnb_potential_destroy.argtypes = [vp]
     lib.tmnb_potential_execute_device.argtypes = [vp, i, i, vp, vp, vp, d, vp, vp, vp, vp, vp]
     lib.tmnb_potential_execute_host.argtypes = [vp, i, i, vp, vp, vp, d, vp, vp, vp, vp]
+    lib.tmnb_potential_execute_windows_device.argtypes = [vp, i, i, vp, vp, vp, i, vp, vp, vp, vp, vp, vp]
+    lib.tmnb_potential_execute_windows_host.argtypes = [vp, i, i, vp, vp, vp, i, vp, vp, vp, vp, vp]
     lib.tmnb_potential_execute_batch_host.argtypes = [vp, i, i, i, i, i, vp, vp, vp, vp, vp, vp, vp, vp]
     lib.tmnb_potential_du_dp_fixed_to_float.argtypes = [vp, i, i, vp, vp]
     lib.tmnb_potential_set_nblist_padding.argtypes = [vp, d]
@@ -82,6 +84,7 @@ def _declare(lib):
     lib.tmnb_context_create.argtypes = [i, vp, vp, vp, d, d, vp, vp, ull, i, vp, vp, vp, ctypes.POINTER(vp)]
     lib.tmnb_context_set_barostat.argtypes = [vp, d, d, vp, i, ull]
     lib.tmnb_context_multiple_steps.argtypes = [vp, i, vp, i, vp, i, vp, vp, i]
+    lib.tmnb_context_multiple_steps_U.argtypes = [vp, d, i, i, vp, i, i, vp, vp, vp, i]
     for nm in ["get_x", "get_v", "get_box", "set_x", "set_v", "set_box"]:
         getattr(lib, "tmnb_context_" + nm).argtypes = [vp, vp]
     lib.tmnb_context_barostat_stats.argtypes = [vp, c_int_p, c_int_p, c_double_p]
@@ -98,6 +101,8 @@ def _declare(lib):
         "tmnb_potential_execute_device",
         "tmnb_potential_execute_host",
         "tmnb_potential_execute_batch_host",
+        "tmnb_potential_execute_windows_device",
+        "tmnb_potential_execute_windows_host",
         "tmnb_potential_du_dp_fixed_to_float",
         "tmnb_potential_set_nblist_padding",
         "tmnb_potential_disable_hilbert_sort",
@@ -109,6 +114,7 @@ def _declare(lib):
         "tmnb_context_create",
         "tmnb_context_set_barostat",
         "tmnb_context_multiple_steps",
+        "tmnb_context_multiple_steps_U",
         "tmnb_context_get_x",
         "tmnb_context_get_v",
         "tmnb_context_get_box",

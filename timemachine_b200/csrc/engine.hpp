@@ -106,6 +106,38 @@ class PotentialBase {
         }
     }
 
+    // K lambda windows on the same coordinates and parameters; output k of
+    // each array starts at k * (3N | P | N). Potentials without a fused
+    // multi-window path evaluate the windows one after the other.
+    virtual void execute_windows_device(
+        int N,
+        int P,
+        const double *d_x,
+        const double *d_p,
+        const double *d_box,
+        int K,
+        const double *lambdas,
+        unsigned long long *d_du_dx,
+        unsigned long long *d_du_dp,
+        unsigned long long *d_du_dl,
+        unsigned long long *d_u,
+        cudaStream_t stream) {
+        for (int k = 0; k < K; k++) {
+            execute_device(
+                N,
+                P,
+                d_x,
+                d_p,
+                d_box,
+                lambdas[k],
+                d_du_dx ? d_du_dx + (size_t)k * 3 * N : nullptr,
+                d_du_dp ? d_du_dp + (size_t)k * P : nullptr,
+                d_du_dl ? d_du_dl + (size_t)k * N : nullptr,
+                d_u ? d_u + (size_t)k * N : nullptr,
+                stream);
+        }
+    }
+
     // Potential::execute_host (timemachine/cpp/src/potential.cu:110-185): copy in,
     // zero and compute the selected outputs, copy out, synchronise. The device
     // staging buffers are kept by the instance and reused.
@@ -120,12 +152,30 @@ class PotentialBase {
         unsigned long long *h_du_dp,
         unsigned long long *h_du_dl,
         unsigned long long *h_u) {
+        execute_windows_host(N, P, h_x, h_p, h_box, 1, &lambda, h_du_dx, h_du_dp, h_du_dl, h_u);
+    }
+
+    // execute_host over K lambda windows (outputs laid out as in
+    // execute_windows_device).
+    void execute_windows_host(
+        int N,
+        int P,
+        const double *h_x,
+        const double *h_p,
+        const double *h_box,
+        int K,
+        const double *lambdas,
+        unsigned long long *h_du_dx,
+        unsigned long long *h_du_dp,
+        unsigned long long *h_du_dl,
+        unsigned long long *h_u) {
         if (!host_stream_) {
             CK(cudaStreamCreateWithFlags(&host_stream_, cudaStreamNonBlocking));
         }
         cudaStream_t s = host_stream_;
         const size_t nx = 3 * (size_t)N;
         const size_t np = P > 0 ? (size_t)P : 1;
+        const size_t kk = K > 0 ? (size_t)K : 1;
         hx_.ensure(nx);
         hp_.ensure(np);
         hbox_.ensure(9);
@@ -136,37 +186,37 @@ class PotentialBase {
         CK(cudaMemcpyAsync(hbox_.p, h_box, 9 * sizeof(double), cudaMemcpyHostToDevice, s));
         unsigned long long *dx = nullptr, *dp = nullptr, *dl = nullptr, *du = nullptr;
         if (h_du_dx) {
-            hdx_.ensure(nx);
+            hdx_.ensure(kk * nx);
             dx = hdx_.p;
-            CK(cudaMemsetAsync(dx, 0, nx * sizeof(*dx), s));
+            CK(cudaMemsetAsync(dx, 0, kk * nx * sizeof(*dx), s));
         }
         if (h_du_dp) {
-            hdp_.ensure(np);
+            hdp_.ensure(kk * np);
             dp = hdp_.p;
-            CK(cudaMemsetAsync(dp, 0, np * sizeof(*dp), s));
+            CK(cudaMemsetAsync(dp, 0, kk * np * sizeof(*dp), s));
         }
         if (h_du_dl) {
-            hdl_.ensure(N);
+            hdl_.ensure(kk * N);
             dl = hdl_.p;
-            CK(cudaMemsetAsync(dl, 0, (size_t)N * sizeof(*dl), s));
+            CK(cudaMemsetAsync(dl, 0, kk * N * sizeof(*dl), s));
         }
         if (h_u) {
-            hu_.ensure(N);
+            hu_.ensure(kk * N);
             du = hu_.p;
-            CK(cudaMemsetAsync(du, 0, (size_t)N * sizeof(*du), s));
+            CK(cudaMemsetAsync(du, 0, kk * N * sizeof(*du), s));
         }
-        execute_device(N, P, hx_.p, hp_.p, hbox_.p, lambda, dx, dp, dl, du, s);
+        execute_windows_device(N, P, hx_.p, hp_.p, hbox_.p, K, lambdas, dx, dp, dl, du, s);
         if (h_du_dx) {
-            CK(cudaMemcpyAsync(h_du_dx, dx, nx * sizeof(*dx), cudaMemcpyDeviceToHost, s));
+            CK(cudaMemcpyAsync(h_du_dx, dx, kk * nx * sizeof(*dx), cudaMemcpyDeviceToHost, s));
         }
         if (h_du_dp) {
-            CK(cudaMemcpyAsync(h_du_dp, dp, (size_t)P * sizeof(*dp), cudaMemcpyDeviceToHost, s));
+            CK(cudaMemcpyAsync(h_du_dp, dp, kk * (size_t)P * sizeof(*dp), cudaMemcpyDeviceToHost, s));
         }
         if (h_du_dl) {
-            CK(cudaMemcpyAsync(h_du_dl, dl, (size_t)N * sizeof(*dl), cudaMemcpyDeviceToHost, s));
+            CK(cudaMemcpyAsync(h_du_dl, dl, kk * N * sizeof(*dl), cudaMemcpyDeviceToHost, s));
         }
         if (h_u) {
-            CK(cudaMemcpyAsync(h_u, du, (size_t)N * sizeof(*du), cudaMemcpyDeviceToHost, s));
+            CK(cudaMemcpyAsync(h_u, du, kk * N * sizeof(*du), cudaMemcpyDeviceToHost, s));
         }
         CK(cudaStreamSynchronize(s));
         check_device_error(s);

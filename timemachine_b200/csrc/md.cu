@@ -119,6 +119,32 @@ __global__ void k_langevin(
     }
 }
 
+// Per-window sums of a [K][N] per-atom buffer into out[0..K) (one block per
+// window); zeroes the buffer.
+__global__ void k_reduce_windows(int N, unsigned long long *__restrict__ buf, unsigned long long *__restrict__ out) {
+    __shared__ unsigned long long part[32];
+    unsigned long long *row = buf + (size_t)blockIdx.x * N;
+    unsigned long long acc = 0;
+    for (int i = threadIdx.x; i < N; i += blockDim.x) {
+        acc += row[i];
+        row[i] = 0;
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    }
+    if ((threadIdx.x & 31) == 0) {
+        part[threadIdx.x >> 5] = acc;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long t = 0;
+        for (int w = 0; w < (int)(blockDim.x >> 5); w++) {
+            t += part[w];
+        }
+        out[blockIdx.x] = t;
+    }
+}
+
 // Sum of the per-atom du_dl buffer into the next output slot; zeroes the buffer.
 __global__ void k_reduce_dl(int N, unsigned long long *__restrict__ buf, unsigned long long *__restrict__ out, MDState *st) {
     __shared__ unsigned long long part[32];
@@ -503,28 +529,9 @@ class Context {
         for (int i = 1; i <= n_steps; i++) {
             const double lam = lambdas[i - 1];
             unsigned long long *dl_slot_base = (dl_interval > 0 && i % dl_interval == 0) ? dl_dev.p : nullptr;
-            if (use_graphs) {
-                CK(cudaGraphLaunch(graph_for(0, lam, dl_slot_base), stream_));
-            } else {
-                record_step(lam, dl_slot_base);
-            }
-            if (has_baro_) {
-                baro_step_++;
-                if (baro_step_ % baro_interval_ == 0) {
-                    if (use_graphs) {
-                        CK(cudaGraphLaunch(graph_for(1, lam, nullptr), stream_));
-                    } else {
-                        record_barostat(lam);
-                    }
-                }
-            }
+            advance(lam, dl_slot_base, use_graphs);
             if (x_interval > 0 && i % x_interval == 0 && x_out_host) {
-                CK(cudaMemcpyAsync(
-                    x_out_host + (size_t)frame * N_ * 3, x_.p, 3 * (size_t)N_ * sizeof(double), cudaMemcpyDeviceToHost,
-                    stream_));
-                if (box_out_host) {
-                    CK(cudaMemcpyAsync(box_out_host + (size_t)frame * 9, box_.p, 9 * sizeof(double), cudaMemcpyDeviceToHost, stream_));
-                }
+                store_frame(frame, x_out_host, box_out_host);
                 frame++;
             }
         }
@@ -534,6 +541,75 @@ class Context {
             CK(cudaStreamSynchronize(stream_));
             for (int k = 0; k < n_dl; k++) {
                 dl_out_host[k] = static_cast<double>(static_cast<long long>(h[k])) / FX_EXPONENT;
+            }
+        }
+        CK(cudaStreamSynchronize(stream_));
+        for (auto &b : bps_) {
+            b->pot->check_device_error(stream_);
+        }
+    }
+
+    // Context::multiple_steps_U (timemachine/cpp/src/context.cu:139-234):
+    // n_steps at `lambda`; every u_interval steps the total potential energy
+    // at each of the K lambda windows, from one multi-window evaluation per
+    // potential; x and box every x_interval steps.
+    void multiple_steps_U(
+        double lambda,
+        int n_steps,
+        int K,
+        const double *windows,
+        int u_interval,
+        int x_interval,
+        double *u_out_host,
+        double *x_out_host,
+        double *box_out_host,
+        bool use_graphs) {
+        if (n_steps < 0) {
+            throw Error(TMNB_ERR_INVALID_ARGUMENT, "n_steps must be >= 0");
+        }
+        if (u_interval <= 0) {
+            throw Error(TMNB_ERR_INVALID_ARGUMENT, "store_u_interval <= 0");
+        }
+        if (x_interval <= 0) {
+            throw Error(TMNB_ERR_INVALID_ARGUMENT, "store_x_interval <= 0");
+        }
+        if (K < 0 || (K > 0 && !windows)) {
+            throw Error(TMNB_ERR_INVALID_ARGUMENT, "invalid lambda windows");
+        }
+        const int n_u = n_steps / u_interval;
+        DevBuf<unsigned long long> u_dev, u_win;
+        if (n_u > 0 && K > 0) {
+            u_dev.alloc((size_t)n_u * K);
+            u_win.alloc((size_t)std::min(K, TMNB_MAX_WINDOWS) * N_);
+            CK(cudaMemsetAsync(u_win.p, 0, u_win.n * sizeof(unsigned long long), stream_));
+        }
+        int frame = 0;
+        for (int i = 1; i <= n_steps; i++) {
+            advance(lambda, nullptr, use_graphs);
+            if (i % x_interval == 0 && x_out_host) {
+                store_frame(frame, x_out_host, box_out_host);
+                frame++;
+            }
+            if (i % u_interval == 0 && K > 0) {
+                unsigned long long *row = u_dev.p + (size_t)(i / u_interval - 1) * K;
+                for (int w = 0; w < K; w += TMNB_MAX_WINDOWS) {
+                    const int kc = std::min(TMNB_MAX_WINDOWS, K - w);
+                    for (auto &b : bps_) {
+                        b->pot->execute_windows_device(
+                            N_, b->P, x_.p, b->params.p, box_.p, kc, windows + w, nullptr, nullptr, nullptr, u_win.p,
+                            stream_);
+                    }
+                    k_reduce_windows<<<kc, 1024, 0, stream_>>>(N_, u_win.p, row + w);
+                    CK(cudaPeekAtLastError());
+                }
+            }
+        }
+        if (n_u > 0 && K > 0 && u_out_host) {
+            std::vector<unsigned long long> h((size_t)n_u * K);
+            CK(cudaMemcpyAsync(h.data(), u_dev.p, h.size() * sizeof(unsigned long long), cudaMemcpyDeviceToHost, stream_));
+            CK(cudaStreamSynchronize(stream_));
+            for (size_t k = 0; k < h.size(); k++) {
+                u_out_host[k] = static_cast<double>(static_cast<long long>(h[k])) / FX_EXPONENT;
             }
         }
         CK(cudaStreamSynchronize(stream_));
@@ -572,6 +648,34 @@ class Context {
     cudaStream_t stream() const { return stream_; }
 
   private:
+    // One integrator step (with the barostat move on its interval), as
+    // Context::_step (timemachine/cpp/src/context.cu:240-282).
+    void advance(double lam, unsigned long long *dl_slot_base, bool use_graphs) {
+        if (use_graphs) {
+            CK(cudaGraphLaunch(graph_for(0, lam, dl_slot_base), stream_));
+        } else {
+            record_step(lam, dl_slot_base);
+        }
+        if (has_baro_) {
+            baro_step_++;
+            if (baro_step_ % baro_interval_ == 0) {
+                if (use_graphs) {
+                    CK(cudaGraphLaunch(graph_for(1, lam, nullptr), stream_));
+                } else {
+                    record_barostat(lam);
+                }
+            }
+        }
+    }
+
+    void store_frame(int frame, double *x_out_host, double *box_out_host) {
+        CK(cudaMemcpyAsync(
+            x_out_host + (size_t)frame * N_ * 3, x_.p, 3 * (size_t)N_ * sizeof(double), cudaMemcpyDeviceToHost, stream_));
+        if (box_out_host) {
+            CK(cudaMemcpyAsync(box_out_host + (size_t)frame * 9, box_.p, 9 * sizeof(double), cudaMemcpyDeviceToHost, stream_));
+        }
+    }
+
     int N_;
     double dt_, ca_;
     uint2 key_;
@@ -677,6 +781,28 @@ tmnb_status tmnb_context_multiple_steps(
     return tmb::guarded([&] {
         ctx->impl->multiple_steps(
             n_steps, lambda_schedule, store_du_dl_interval, du_dl_out, store_x_interval, x_out, box_out, use_graphs != 0);
+    });
+}
+
+tmnb_status tmnb_context_multiple_steps_U(
+    tmnb_context *ctx,
+    double lambda,
+    int n_steps,
+    int n_windows,
+    const double *lambda_windows,
+    int store_u_interval,
+    int store_x_interval,
+    double *u_out,
+    double *x_out,
+    double *box_out,
+    int use_graphs) {
+    if (tmnb_status s = check_ctx(ctx)) {
+        return s;
+    }
+    return tmb::guarded([&] {
+        ctx->impl->multiple_steps_U(
+            lambda, n_steps, n_windows, lambda_windows, store_u_interval, store_x_interval, u_out, x_out, box_out,
+            use_graphs != 0);
     });
 }
 

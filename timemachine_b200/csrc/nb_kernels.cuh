@@ -21,6 +21,7 @@
 #pragma once
 
 #include "nb_pair_math.cuh"
+#include "tmnb.h"
 
 namespace tmb {
 
@@ -43,10 +44,14 @@ struct DevState {
 constexpr int DEV_ERR_NONORTHO_BOX = 3;
 constexpr int DEV_ERR_BOX_TOO_SMALL = 4;
 
+// Up to this many lambda windows are evaluated together (one launch sequence).
+constexpr int MAX_WINDOWS = TMNB_MAX_WINDOWS;
+
 struct SlotArrays {
-    float4 *posw;  // [S] x, y, z, w
-    float4 *prm;   // [S] q, sig, eps, dw/dlambda
-    float4 *dprm;  // [S] dq/dl, dsig/dl, deps/dl, 0 (interpolated only)
+    float4 *posw;            // [K][S] x, y, z, w(lambda_k)
+    float4 *prm;             // [K][S] q, sig, eps, dw/dlambda (parameters at lambda_k)
+    float4 *dprm;            // [S] dq/dl, dsig/dl, deps/dl, 0 (interpolated only)
+    unsigned char *lamdep;   // [S] 1 when the atom's staged values depend on lambda
 };
 
 struct PrepareArgs {
@@ -55,7 +60,8 @@ struct PrepareArgs {
     const double *x;            // [N,3]
     const double *p;            // [N,3] or [2N,3] (interpolated)
     const double *box;          // [3,3]
-    double lambda;
+    int K;                      // lambda windows
+    double lambdas[MAX_WINDOWS];
     double cutoff;
     double padding;
     const int *plane;           // [N]
@@ -64,34 +70,44 @@ struct PrepareArgs {
     SlotArrays slots;
 };
 
-// Stage one atom into its slot. w = cutoff*(plane + offset*lambda),
+// Stage one atom into its slot, for every window. w = cutoff*(plane + offset*lambda),
 // dw/dlambda = offset*cutoff (timemachine/cpp/src/kernels/k_lambda_transformer_jit.cuh:25-55
 // with the identity lambda transform); interpolated parameters
 // p = (1-lambda) p0 + lambda p1, dp/dlambda = p1 - p0 (same file :57-98).
+// An atom is lambda-dependent when its w or its parameters change with lambda
+// (offset != 0, or p0 != p1); pairs of lambda-independent atoms give the same
+// per-pair values in every window.
 __device__ __forceinline__ void prepare_slot(const PrepareArgs &a, int s, int atom) {
-    const double lambda = a.lambda;
     const int plane = a.plane[atom];
     const int offset = a.offset[atom];
-    const double f_lambda = lambda;
     const double f_lambda_grad = 1.0;
-    const double w = (plane + offset * f_lambda) * a.cutoff;
     const double dw_dl = offset * f_lambda_grad * a.cutoff;
     const double *xa = a.x + 3 * (size_t)atom;
-    a.slots.posw[s] = make_float4((float)xa[0], (float)xa[1], (float)xa[2], (float)w);
+    const float fx = (float)xa[0], fy = (float)xa[1], fz = (float)xa[2];
+    bool dep = offset != 0;
+    const double *p0 = a.p + 3 * (size_t)atom;
+    const double *p1 = a.p + 3 * ((size_t)a.N + atom);
     if (a.interpolated) {
-        const double *p0 = a.p + 3 * (size_t)atom;
-        const double *p1 = a.p + 3 * ((size_t)a.N + atom);
-        double pq = (1 - f_lambda) * p0[0] + f_lambda * p1[0];
-        double ps = (1 - f_lambda) * p0[1] + f_lambda * p1[1];
-        double pe = (1 - f_lambda) * p0[2] + f_lambda * p1[2];
         double dq = f_lambda_grad * (p1[0] - p0[0]);
         double ds = f_lambda_grad * (p1[1] - p0[1]);
         double de = f_lambda_grad * (p1[2] - p0[2]);
-        a.slots.prm[s] = make_float4((float)pq, (float)ps, (float)pe, (float)dw_dl);
         a.slots.dprm[s] = make_float4((float)dq, (float)ds, (float)de, 0.0f);
-    } else {
-        const double *pa = a.p + 3 * (size_t)atom;
-        a.slots.prm[s] = make_float4((float)pa[0], (float)pa[1], (float)pa[2], (float)dw_dl);
+        dep = dep || p0[0] != p1[0] || p0[1] != p1[1] || p0[2] != p1[2];
+    }
+    a.slots.lamdep[s] = dep ? 1 : 0;
+    for (int k = 0; k < a.K; k++) {
+        const double f_lambda = a.lambdas[k];
+        const double w = (plane + offset * f_lambda) * a.cutoff;
+        const size_t o = (size_t)k * a.S + s;
+        a.slots.posw[o] = make_float4(fx, fy, fz, (float)w);
+        if (a.interpolated) {
+            double pq = (1 - f_lambda) * p0[0] + f_lambda * p1[0];
+            double ps = (1 - f_lambda) * p0[1] + f_lambda * p1[1];
+            double pe = (1 - f_lambda) * p0[2] + f_lambda * p1[2];
+            a.slots.prm[o] = make_float4((float)pq, (float)ps, (float)pe, (float)dw_dl);
+        } else {
+            a.slots.prm[o] = make_float4((float)p0[0], (float)p0[1], (float)p0[2], (float)dw_dl);
+        }
     }
 }
 
@@ -582,11 +598,32 @@ struct Accum {
     unsigned long long *pq, *psig, *peps; // du_dp of the scaled-pair part (interpolated), else == q/sig/eps
 };
 
+// Accumulator block b (0: contributions shared by all windows, 1 + k: window k)
+// lies `block` elements after block 0.
+__device__ __forceinline__ Accum acc_block(const Accum &a, size_t block, int b) {
+    const size_t o = block * (size_t)b;
+    Accum r;
+    r.x = a.x + o;
+    r.y = a.y + o;
+    r.z = a.z + o;
+    r.q = a.q + o;
+    r.sig = a.sig + o;
+    r.eps = a.eps + o;
+    r.u = a.u + o;
+    r.dl = a.dl + o;
+    r.pq = a.pq + o;
+    r.psig = a.psig + o;
+    r.peps = a.peps + o;
+    return r;
+}
+
 struct PairArgs {
     int S;
-    const float4 *posw;
-    const float4 *prm;
-    const float4 *dprm;
+    int K;                      // lambda windows
+    const float4 *posw;         // [K][S]
+    const float4 *prm;          // [K][S]
+    const float4 *dprm;         // [S]
+    const unsigned char *lamdep; // [S]
     const double *box;
     double beta;
     double cutoff;
@@ -598,7 +635,8 @@ struct PairArgs {
     const double *scales;  // [M,2]
     const int *slot_of;    // [N] atom -> slot, nullptr: identity
     int negated;
-    Accum acc;
+    Accum acc;             // block 0
+    size_t acc_block;      // elements between accumulator blocks
     DevState *state;
 };
 
@@ -707,15 +745,16 @@ __device__ __forceinline__ void sweep_tile(
                 }
             }
             if (DX) {
-                const unsigned long long fx = to_fixed(fmul(prefactor, delta_x), FX_EXPONENT);
-                const unsigned long long fy = to_fixed(fmul(prefactor, delta_y), FX_EXPONENT);
-                const unsigned long long fz = to_fixed(fmul(prefactor, delta_z), FX_EXPONENT);
+                unsigned long long fx, fy, fz, nx, ny, nz;
+                to_fixed_pair(fmul(prefactor, delta_x), FX_EXPONENT, fx, nx);
+                to_fixed_pair(fmul(prefactor, delta_y), FX_EXPONENT, fy, ny);
+                to_fixed_pair(fmul(prefactor, delta_z), FX_EXPONENT, fz, nz);
                 gi_x += fx;
                 gi_y += fy;
                 gi_z += fz;
-                gj_x -= fx;
-                gj_y -= fy;
-                gj_z -= fz;
+                gj_x += nx;
+                gj_y += ny;
+                gj_z += nz;
             }
             if (DP) {
                 g_qi += to_fixed(fmul(fmul(qj, inv_d), erfc_bd), FX_EXPONENT);
@@ -764,17 +803,25 @@ __device__ __forceinline__ void sweep_tile(
 // One scaled pair (exclusion / 1-4 correction), arithmetic of
 // timemachine/cpp/src/kernels/k_nonbonded_pair_list.cuh:103-215.
 template <typename Real, bool U, bool DX, bool DL, bool DP, bool INTERP>
-__device__ __forceinline__ void scaled_pair(const PairArgs &a, int pair, const Real box_x, const Real box_y,
-                                            const Real box_z, const Real inv_box_x, const Real inv_box_y,
-                                            const Real inv_box_z, const Real cutoff_squared) {
-    const int atom_i = a.pair_idxs[2 * pair + 0];
-    const int atom_j = a.pair_idxs[2 * pair + 1];
-    const int si = a.slot_of ? a.slot_of[atom_i] : atom_i;
-    const int sj = a.slot_of ? a.slot_of[atom_j] : atom_j;
-    const float4 pwi = a.posw[si];
-    const float4 pwj = a.posw[sj];
-    const float4 pri = a.prm[si];
-    const float4 prj = a.prm[sj];
+__device__ __forceinline__ void scaled_pair(
+    const PairArgs &a,
+    int pair,
+    int si,
+    int sj,
+    int window,
+    const Accum &acc_out,
+    const Real box_x,
+    const Real box_y,
+    const Real box_z,
+    const Real inv_box_x,
+    const Real inv_box_y,
+    const Real inv_box_z,
+    const Real cutoff_squared) {
+    const size_t wo = (size_t)window * a.S;
+    const float4 pwi = a.posw[wo + si];
+    const float4 pwj = a.posw[wo + sj];
+    const float4 pri = a.prm[wo + si];
+    const float4 prj = a.prm[wo + sj];
     float4 dpi = make_float4(0.f, 0.f, 0.f, 0.f);
     float4 dpj = dpi;
     if (INTERP) {
@@ -834,23 +881,24 @@ __device__ __forceinline__ void scaled_pair(const PairArgs &a, int pair, const R
     const bool neg = a.negated != 0;
     auto acc = [neg](unsigned long long *p, unsigned long long v) { red_add(p, neg ? (0ULL - v) : v); };
     if (DX) {
-        const unsigned long long fx = to_fixed(fmul(prefactor, delta_x), FX_EXPONENT);
-        const unsigned long long fy = to_fixed(fmul(prefactor, delta_y), FX_EXPONENT);
-        const unsigned long long fz = to_fixed(fmul(prefactor, delta_z), FX_EXPONENT);
-        acc(a.acc.x + si, fx);
-        acc(a.acc.y + si, fy);
-        acc(a.acc.z + si, fz);
-        acc(a.acc.x + sj, 0ULL - fx);
-        acc(a.acc.y + sj, 0ULL - fy);
-        acc(a.acc.z + sj, 0ULL - fz);
+        unsigned long long fx, fy, fz, nx, ny, nz;
+        to_fixed_pair(fmul(prefactor, delta_x), FX_EXPONENT, fx, nx);
+        to_fixed_pair(fmul(prefactor, delta_y), FX_EXPONENT, fy, ny);
+        to_fixed_pair(fmul(prefactor, delta_z), FX_EXPONENT, fz, nz);
+        acc(acc_out.x + si, fx);
+        acc(acc_out.y + si, fy);
+        acc(acc_out.z + si, fz);
+        acc(acc_out.x + sj, nx);
+        acc(acc_out.y + sj, ny);
+        acc(acc_out.z + sj, nz);
     }
     if (DP) {
-        acc(a.acc.pq + si, to_fixed(fmul(fmul(fmul(charge_scale, qj), inv_d), erfc_bd), FX_EXPONENT));
-        acc(a.acc.pq + sj, to_fixed(fmul(fmul(fmul(charge_scale, qi), inv_d), erfc_bd), FX_EXPONENT));
-        acc(a.acc.psig + si, g_sig);
-        acc(a.acc.peps + si, g_epsi);
-        acc(a.acc.psig + sj, g_sig);
-        acc(a.acc.peps + sj, g_epsj);
+        acc(acc_out.pq + si, to_fixed(fmul(fmul(fmul(charge_scale, qj), inv_d), erfc_bd), FX_EXPONENT));
+        acc(acc_out.pq + sj, to_fixed(fmul(fmul(fmul(charge_scale, qi), inv_d), erfc_bd), FX_EXPONENT));
+        acc(acc_out.psig + si, g_sig);
+        acc(acc_out.peps + si, g_epsi);
+        acc(acc_out.psig + sj, g_sig);
+        acc(acc_out.peps + sj, g_epsj);
     }
     if (DL && !is_vanilla) {
         real_du_dl = ffma(fmul(delta_w, prefactor), fsub(dw_dl_i, dw_dl_j), real_du_dl);
@@ -858,14 +906,123 @@ __device__ __forceinline__ void scaled_pair(const PairArgs &a, int pair, const R
             real_du_dl = ffma(
                 fmul(fmul(charge_scale, inv_d), erfc_bd), sum_of_products_rn(qj, dq_dl_i, qi, dq_dl_j), real_du_dl);
         }
-        acc(a.acc.dl + si, to_fixed(real_du_dl, FX_EXPONENT));
+        acc(acc_out.dl + si, to_fixed(real_du_dl, FX_EXPONENT));
     }
     if (U) {
-        acc(a.acc.u + si, to_fixed(u, FX_EXPONENT));
+        acc(acc_out.u + si, to_fixed(u, FX_EXPONENT));
     }
 }
 
+// One tile of row block rows (lane = row slot i) against the 32 column slots
+// j, for one window: load, sweep, column atomics. Row accumulators are
+// returned to the caller.
 template <typename Real, bool U, bool DX, bool DL, bool DP, bool INTERP>
+__device__ __forceinline__ void tile_pass(
+    const PairArgs &a,
+    const int lane,
+    const unsigned S,
+    const unsigned i,
+    const unsigned j,
+    const int window,
+    const Accum &acc_out,
+    const Real box_x,
+    const Real box_y,
+    const Real box_z,
+    const Real inv_box_x,
+    const Real inv_box_y,
+    const Real inv_box_z,
+    const Real cutoff_squared,
+    const Real beta,
+    unsigned long long &gi_x,
+    unsigned long long &gi_y,
+    unsigned long long &gi_z,
+    unsigned long long &g_qi,
+    unsigned long long &g_sigi,
+    unsigned long long &g_epsi,
+    unsigned long long &du_dl,
+    unsigned long long &energy) {
+    const size_t wo = (size_t)window * a.S;
+    const bool row_ok = i < S;
+    const bool col_ok = j < S;
+    const float4 pwi = row_ok ? a.posw[wo + i] : make_float4(0.f, 0.f, 0.f, 0.f);
+    const float4 pri = row_ok ? a.prm[wo + i] : make_float4(0.f, 0.f, 0.f, 0.f);
+    const float4 pwj = col_ok ? a.posw[wo + j] : make_float4(0.f, 0.f, 0.f, 0.f);
+    const float4 prj = col_ok ? a.prm[wo + j] : make_float4(0.f, 0.f, 0.f, 0.f);
+    float4 dpi = make_float4(0.f, 0.f, 0.f, 0.f);
+    float4 dpj = dpi;
+    if (INTERP) {
+        if (row_ok) {
+            dpi = a.dprm[i];
+        }
+        if (col_ok) {
+            dpj = a.dprm[j];
+        }
+    }
+    const bool row_alch = pwi.w != 0.f || (INTERP && (dpi.x != 0.f || dpi.y != 0.f || dpi.z != 0.f));
+    const bool col_alch = pwj.w != 0.f || (INTERP && (dpj.x != 0.f || dpj.y != 0.f || dpj.z != 0.f));
+    const bool alch = __any_sync(FULL_MASK, row_alch || col_alch);
+    unsigned long long gj_x = 0, gj_y = 0, gj_z = 0, g_qj = 0, g_sigj = 0, g_epsj = 0;
+    if (alch) {
+        sweep_tile<Real, U, DX, DL, DP, INTERP, true>(
+            lane, S, i, j, pwi.x, pwi.y, pwi.z, pwi.w, pri.x, pri.y, pri.z, pri.w, dpi.x, dpi.y, dpi.z, pwj.x, pwj.y,
+            pwj.z, pwj.w, prj.x, prj.y, prj.z, prj.w, dpj.x, dpj.y, dpj.z, box_x, box_y, box_z, inv_box_x, inv_box_y,
+            inv_box_z, cutoff_squared, beta, gi_x, gi_y, gi_z, g_qi, g_sigi, g_epsi, du_dl, energy, gj_x, gj_y, gj_z,
+            g_qj, g_sigj, g_epsj);
+    } else {
+        sweep_tile<Real, U, DX, DL, DP, INTERP, false>(
+            lane, S, i, j, pwi.x, pwi.y, pwi.z, pwi.w, pri.x, pri.y, pri.z, pri.w, dpi.x, dpi.y, dpi.z, pwj.x, pwj.y,
+            pwj.z, pwj.w, prj.x, prj.y, prj.z, prj.w, dpj.x, dpj.y, dpj.z, box_x, box_y, box_z, inv_box_x, inv_box_y,
+            inv_box_z, cutoff_squared, beta, gi_x, gi_y, gi_z, g_qi, g_sigi, g_epsi, du_dl, energy, gj_x, gj_y, gj_z,
+            g_qj, g_sigj, g_epsj);
+    }
+    if (col_ok) {
+        if (DX) {
+            red_add(acc_out.x + j, gj_x);
+            red_add(acc_out.y + j, gj_y);
+            red_add(acc_out.z + j, gj_z);
+        }
+        if (DP) {
+            red_add(acc_out.q + j, g_qj);
+            red_add(acc_out.sig + j, g_sigj);
+            red_add(acc_out.eps + j, g_epsj);
+        }
+    }
+}
+
+template <bool U, bool DX, bool DL, bool DP>
+__device__ __forceinline__ void flush_row(
+    const Accum &acc_out,
+    unsigned i,
+    unsigned long long gi_x,
+    unsigned long long gi_y,
+    unsigned long long gi_z,
+    unsigned long long g_qi,
+    unsigned long long g_sigi,
+    unsigned long long g_epsi,
+    unsigned long long du_dl,
+    unsigned long long energy) {
+    if (DX) {
+        red_add(acc_out.x + i, gi_x);
+        red_add(acc_out.y + i, gi_y);
+        red_add(acc_out.z + i, gi_z);
+    }
+    if (DP) {
+        red_add(acc_out.q + i, g_qi);
+        red_add(acc_out.sig + i, g_sigi);
+        red_add(acc_out.eps + i, g_epsi);
+    }
+    if (DL) {
+        red_add(acc_out.dl + i, du_dl);
+    }
+    if (U) {
+        red_add(acc_out.u + i, energy);
+    }
+}
+
+// Persistent pair kernel. MULTI: K > 1 lambda windows; tiles and scaled pairs
+// whose atoms are all lambda-independent are evaluated once into the shared
+// accumulator block, the others once per window into the window's block.
+template <typename Real, bool U, bool DX, bool DL, bool DP, bool INTERP, bool MULTI>
 __global__ void __launch_bounds__(128) k_pair(PairArgs a) {
     if (a.state->error) {
         return;
@@ -896,86 +1053,59 @@ __global__ void __launch_bounds__(128) k_pair(PairArgs a) {
         if (item >= n_items) {
             const int pair = (item - n_items) * TILE + lane;
             if (pair < a.M) {
-                scaled_pair<Real, U, DX, DL, DP, INTERP>(a, pair, box_x, box_y, box_z, inv_box_x, inv_box_y,
-                                                         inv_box_z, cutoff_squared);
+                const int atom_i = a.pair_idxs[2 * pair + 0];
+                const int atom_j = a.pair_idxs[2 * pair + 1];
+                const int si = a.slot_of ? a.slot_of[atom_i] : atom_i;
+                const int sj = a.slot_of ? a.slot_of[atom_j] : atom_j;
+                if (!MULTI || !(a.lamdep[si] || a.lamdep[sj])) {
+                    scaled_pair<Real, U, DX, DL, DP, INTERP>(
+                        a, pair, si, sj, 0, a.acc, box_x, box_y, box_z, inv_box_x, inv_box_y, inv_box_z,
+                        cutoff_squared);
+                } else {
+                    for (int k = 0; k < a.K; k++) {
+                        scaled_pair<Real, U, DX, DL, DP, INTERP>(
+                            a, pair, si, sj, k, acc_block(a.acc, a.acc_block, 1 + k), box_x, box_y, box_z, inv_box_x,
+                            inv_box_y, inv_box_z, cutoff_squared);
+                    }
+                }
             }
             continue;
         }
         const int4 it = a.items[item];
         const unsigned i = (unsigned)(it.x * TILE + lane);
-        const bool row_ok = i < S;
-        const float4 pwi = row_ok ? a.posw[i] : make_float4(0.f, 0.f, 0.f, 0.f);
-        const float4 pri = row_ok ? a.prm[i] : make_float4(0.f, 0.f, 0.f, 0.f);
-        float4 dpi = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (INTERP && row_ok) {
-            dpi = a.dprm[i];
-        }
-        const bool row_alch = pwi.w != 0.f || (INTERP && (dpi.x != 0.f || dpi.y != 0.f || dpi.z != 0.f));
-
+        const bool row_dep = MULTI && i < S && a.lamdep[i];
         unsigned long long gi_x = 0, gi_y = 0, gi_z = 0, g_qi = 0, g_sigi = 0, g_epsi = 0, du_dl = 0, energy = 0;
         for (int t = 0; t < it.z; t++) {
             const long long tile = (long long)it.y + t;
             const unsigned j = a.tile_cols[tile * TILE + lane];
-            const bool col_ok = j < S;
-            const float4 pwj = col_ok ? a.posw[j] : make_float4(0.f, 0.f, 0.f, 0.f);
-            const float4 prj = col_ok ? a.prm[j] : make_float4(0.f, 0.f, 0.f, 0.f);
-            float4 dpj = make_float4(0.f, 0.f, 0.f, 0.f);
-            if (INTERP && col_ok) {
-                dpj = a.dprm[j];
-            }
-            const bool col_alch = pwj.w != 0.f || (INTERP && (dpj.x != 0.f || dpj.y != 0.f || dpj.z != 0.f));
-            const bool alch = __any_sync(FULL_MASK, row_alch || col_alch);
-            unsigned long long gj_x = 0, gj_y = 0, gj_z = 0, g_qj = 0, g_sigj = 0, g_epsj = 0;
-            if (alch) {
-                sweep_tile<Real, U, DX, DL, DP, INTERP, true>(
-                    lane, S, i, j, pwi.x, pwi.y, pwi.z, pwi.w, pri.x, pri.y, pri.z, pri.w, dpi.x, dpi.y, dpi.z, pwj.x,
-                    pwj.y, pwj.z, pwj.w, prj.x, prj.y, prj.z, prj.w, dpj.x, dpj.y, dpj.z, box_x, box_y, box_z,
-                    inv_box_x, inv_box_y, inv_box_z, cutoff_squared, beta, gi_x, gi_y, gi_z, g_qi, g_sigi, g_epsi,
-                    du_dl, energy, gj_x, gj_y, gj_z, g_qj, g_sigj, g_epsj);
+            const bool dep = MULTI && __any_sync(FULL_MASK, row_dep || (j < S && a.lamdep[j]));
+            if (!dep) {
+                tile_pass<Real, U, DX, DL, DP, INTERP>(
+                    a, lane, S, i, j, 0, a.acc, box_x, box_y, box_z, inv_box_x, inv_box_y, inv_box_z, cutoff_squared,
+                    beta, gi_x, gi_y, gi_z, g_qi, g_sigi, g_epsi, du_dl, energy);
             } else {
-                sweep_tile<Real, U, DX, DL, DP, INTERP, false>(
-                    lane, S, i, j, pwi.x, pwi.y, pwi.z, pwi.w, pri.x, pri.y, pri.z, pri.w, dpi.x, dpi.y, dpi.z, pwj.x,
-                    pwj.y, pwj.z, pwj.w, prj.x, prj.y, prj.z, prj.w, dpj.x, dpj.y, dpj.z, box_x, box_y, box_z,
-                    inv_box_x, inv_box_y, inv_box_z, cutoff_squared, beta, gi_x, gi_y, gi_z, g_qi, g_sigi, g_epsi,
-                    du_dl, energy, gj_x, gj_y, gj_z, g_qj, g_sigj, g_epsj);
-            }
-            if (col_ok) {
-                if (DX) {
-                    red_add(a.acc.x + j, gj_x);
-                    red_add(a.acc.y + j, gj_y);
-                    red_add(a.acc.z + j, gj_z);
-                }
-                if (DP) {
-                    red_add(a.acc.q + j, g_qj);
-                    red_add(a.acc.sig + j, g_sigj);
-                    red_add(a.acc.eps + j, g_epsj);
+                for (int k = 0; k < a.K; k++) {
+                    const Accum wk = acc_block(a.acc, a.acc_block, 1 + k);
+                    unsigned long long wx = 0, wy = 0, wz = 0, wq = 0, ws = 0, we = 0, wl = 0, wu = 0;
+                    tile_pass<Real, U, DX, DL, DP, INTERP>(
+                        a, lane, S, i, j, k, wk, box_x, box_y, box_z, inv_box_x, inv_box_y, inv_box_z, cutoff_squared,
+                        beta, wx, wy, wz, wq, ws, we, wl, wu);
+                    if (i < S) {
+                        flush_row<U, DX, DL, DP>(wk, i, wx, wy, wz, wq, ws, we, wl, wu);
+                    }
                 }
             }
         }
-        if (row_ok) {
-            if (DX) {
-                red_add(a.acc.x + i, gi_x);
-                red_add(a.acc.y + i, gi_y);
-                red_add(a.acc.z + i, gi_z);
-            }
-            if (DP) {
-                red_add(a.acc.q + i, g_qi);
-                red_add(a.acc.sig + i, g_sigi);
-                red_add(a.acc.eps + i, g_epsi);
-            }
-            if (DL) {
-                red_add(a.acc.dl + i, du_dl);
-            }
-            if (U) {
-                red_add(a.acc.u + i, energy);
-            }
+        if (i < S) {
+            flush_row<U, DX, DL, DP>(a.acc, i, gi_x, gi_y, gi_z, g_qi, g_sigi, g_epsi, du_dl, energy);
         }
     }
 }
 
 // ---------------------------------------------------------------------------
 // Scatter of the slot-ordered accumulators into the caller's outputs (which
-// accumulate, +=), and reset of the accumulators.
+// accumulate, +=), and reset of the accumulators. Window k's result is the
+// shared block plus block 1 + k (one window: block 0 only).
 // du_dp of interpolated potentials is split into the lambda=0 and lambda=1
 // halves per potential part, with the rounding of
 // timemachine/cpp/src/kernels/k_lambda_transformer_jit.cuh:100-137.
@@ -983,15 +1113,18 @@ __global__ void __launch_bounds__(128) k_pair(PairArgs a) {
 struct FinalizeArgs {
     int N;
     int S;
+    int K;
+    double lambdas[MAX_WINDOWS];
     const unsigned *perm;
     Accum acc;
+    size_t acc_block;
     int split_pair_dp; // 1: acc.pq/psig/peps are separate buffers
     int interpolated;
-    double lambda;
-    unsigned long long *du_dx;
-    unsigned long long *du_dp;
-    unsigned long long *du_dl;
-    unsigned long long *u;
+    unsigned long long *du_dx; // [K][N,3] (window stride out_stride_x)
+    unsigned long long *du_dp; // [K][P]
+    unsigned long long *du_dl; // [K][N]
+    unsigned long long *u;     // [K][N]
+    size_t stride_x, stride_p, stride_n;
     const DevState *state;
 };
 
@@ -1000,60 +1133,79 @@ __device__ __forceinline__ unsigned long long interp_part(double f, unsigned lon
     return static_cast<unsigned long long>(llrint((f * real) * e));
 }
 
+__device__ __forceinline__ unsigned long long take(unsigned long long *p) {
+    const unsigned long long v = *p;
+    *p = 0;
+    return v;
+}
+
 __global__ void k_finalize(FinalizeArgs a) {
     const bool ok = a.state->error == 0;
+    const bool multi = a.K > 1;
     for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < a.S; s += gridDim.x * blockDim.x) {
         const int atom = a.perm[s];
-        if (a.du_dx) {
-            if (ok) {
-                a.du_dx[3 * (size_t)atom + 0] += a.acc.x[s];
-                a.du_dx[3 * (size_t)atom + 1] += a.acc.y[s];
-                a.du_dx[3 * (size_t)atom + 2] += a.acc.z[s];
-            }
-            a.acc.x[s] = 0;
-            a.acc.y[s] = 0;
-            a.acc.z[s] = 0;
+        const Accum &c = a.acc;
+        const size_t B = a.acc_block;
+        const unsigned long long shared_x = take(c.x + s), shared_y = take(c.y + s), shared_z = take(c.z + s);
+        const unsigned long long shared_q = take(c.q + s), shared_sig = take(c.sig + s), shared_eps = take(c.eps + s);
+        const unsigned long long shared_u = take(c.u + s), shared_dl = take(c.dl + s);
+        unsigned long long shared_pq = 0, shared_psig = 0, shared_peps = 0;
+        if (a.split_pair_dp) {
+            shared_pq = take(c.pq + s);
+            shared_psig = take(c.psig + s);
+            shared_peps = take(c.peps + s);
         }
-        if (a.du_dp) {
-            unsigned long long v0[3] = {a.acc.q[s], a.acc.sig[s], a.acc.eps[s]};
-            unsigned long long v1[3] = {0, 0, 0};
-            a.acc.q[s] = 0;
-            a.acc.sig[s] = 0;
-            a.acc.eps[s] = 0;
-            if (a.split_pair_dp) {
-                v1[0] = a.acc.pq[s];
-                v1[1] = a.acc.psig[s];
-                v1[2] = a.acc.peps[s];
-                a.acc.pq[s] = 0;
-                a.acc.psig[s] = 0;
-                a.acc.peps[s] = 0;
+        for (int k = 0; k < a.K; k++) {
+            unsigned long long vx = shared_x, vy = shared_y, vz = shared_z;
+            unsigned long long v0[3] = {shared_q, shared_sig, shared_eps};
+            unsigned long long v1[3] = {shared_pq, shared_psig, shared_peps};
+            unsigned long long vu = shared_u, vl = shared_dl;
+            if (multi) {
+                const size_t o = B * (1 + k) + s;
+                vx += take(c.x + o);
+                vy += take(c.y + o);
+                vz += take(c.z + o);
+                v0[0] += take(c.q + o);
+                v0[1] += take(c.sig + o);
+                v0[2] += take(c.eps + o);
+                vu += take(c.u + o);
+                vl += take(c.dl + o);
+                if (a.split_pair_dp) {
+                    v1[0] += take(c.pq + o);
+                    v1[1] += take(c.psig + o);
+                    v1[2] += take(c.peps + o);
+                }
             }
-            if (ok) {
+            if (!ok) {
+                continue;
+            }
+            if (a.du_dx) {
+                unsigned long long *o = a.du_dx + a.stride_x * k + 3 * (size_t)atom;
+                o[0] += vx;
+                o[1] += vy;
+                o[2] += vz;
+            }
+            if (a.du_dp) {
                 const unsigned long long ex[3] = {FX_EXPONENT, FX_EXPONENT_SIG, FX_EXPONENT_EPS};
-                for (int c = 0; c < 3; c++) {
+                unsigned long long *o = a.du_dp + a.stride_p * k;
+                for (int d = 0; d < 3; d++) {
                     if (a.interpolated) {
-                        const double f = a.lambda;
-                        unsigned long long lo = interp_part(1 - f, v0[c], ex[c]) + interp_part(1 - f, v1[c], ex[c]);
-                        unsigned long long hi = interp_part(f, v0[c], ex[c]) + interp_part(f, v1[c], ex[c]);
-                        a.du_dp[3 * (size_t)atom + c] += lo;
-                        a.du_dp[3 * ((size_t)a.N + atom) + c] += hi;
+                        const double f = a.lambdas[k];
+                        unsigned long long lo = interp_part(1 - f, v0[d], ex[d]) + interp_part(1 - f, v1[d], ex[d]);
+                        unsigned long long hi = interp_part(f, v0[d], ex[d]) + interp_part(f, v1[d], ex[d]);
+                        o[3 * (size_t)atom + d] += lo;
+                        o[3 * ((size_t)a.N + atom) + d] += hi;
                     } else {
-                        a.du_dp[3 * (size_t)atom + c] += v0[c] + v1[c];
+                        o[3 * (size_t)atom + d] += v0[d] + v1[d];
                     }
                 }
             }
-        }
-        if (a.u) {
-            if (ok) {
-                a.u[atom] += a.acc.u[s];
+            if (a.u) {
+                a.u[a.stride_n * k + atom] += vu;
             }
-            a.acc.u[s] = 0;
-        }
-        if (a.du_dl) {
-            if (ok) {
-                a.du_dl[atom] += a.acc.dl[s];
+            if (a.du_dl) {
+                a.du_dl[a.stride_n * k + atom] += vl;
             }
-            a.acc.dl[s] = 0;
         }
     }
 }

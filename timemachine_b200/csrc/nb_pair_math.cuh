@@ -72,6 +72,22 @@ __device__ __forceinline__ unsigned long long to_fixed(double v, unsigned long l
     return static_cast<unsigned long long>(llrint(v * exponent));
 }
 
+// Fixed-point encodings of a pair term v and of its negation -v, for the two
+// atoms of the pair. llrint is odd under round-half-even, so the second is
+// -first (one conversion instead of two) -- except where the conversion
+// saturates (|v * 2^e| >= 2^63) or v is NaN, where the negated value is
+// converted on its own to keep the reference's exact result.
+__device__ __forceinline__ void to_fixed_pair(
+    float v, unsigned long long exponent, unsigned long long &pos, unsigned long long &neg) {
+    const float y = __fmul_rn(v, static_cast<float>(exponent));
+    pos = static_cast<unsigned long long>(llrintf(y));
+    if (fabsf(y) < 0x1p63f) { // strictly inside the int64 range
+        neg = 0ULL - pos;
+    } else {
+        neg = static_cast<unsigned long long>(llrintf(-y));
+    }
+}
+
 // explicit-rounding FP32 helpers
 __device__ __forceinline__ float fmul(float a, float b) { return __fmul_rn(a, b); }
 __device__ __forceinline__ float fadd(float a, float b) { return __fadd_rn(a, b); }

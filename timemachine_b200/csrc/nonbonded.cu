@@ -34,13 +34,15 @@ template <int I> struct PairKernelTable {
 
 // kernel index: bit3 U, bit2 DU_DX, bit1 DU_DL, bit0 DU_DP (+16 when interpolated),
 // the same flag order as timemachine/cpp/src/nonbonded_all_pairs.cu:374-379.
+template <int I, bool INTERP, bool MULTI> constexpr pair_kernel_t pair_kernel() {
+    return &k_pair<float, PairKernelTable<I>::U, PairKernelTable<I>::DX, PairKernelTable<I>::DL, PairKernelTable<I>::DP,
+                   INTERP, MULTI>;
+}
 template <int... Is> struct KernelList {
-    static void fill(pair_kernel_t *out, bool interp) {
-        ((out[Is] = interp ? &k_pair<float, PairKernelTable<Is>::U, PairKernelTable<Is>::DX, PairKernelTable<Is>::DL,
-                                     PairKernelTable<Is>::DP, true>
-                           : &k_pair<float, PairKernelTable<Is>::U, PairKernelTable<Is>::DX, PairKernelTable<Is>::DL,
-                                     PairKernelTable<Is>::DP, false>),
-         ...);
+    // single: one lambda window; multi: K > 1 windows sharing lambda-independent tiles
+    static void fill(pair_kernel_t *single, pair_kernel_t *multi, bool interp) {
+        ((single[Is] = interp ? pair_kernel<Is, true, false>() : pair_kernel<Is, false, false>()), ...);
+        ((multi[Is] = interp ? pair_kernel<Is, true, true>() : pair_kernel<Is, false, true>()), ...);
     }
 };
 using AllKernels = KernelList<0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 14, 15>;
@@ -134,11 +136,12 @@ class NonbondedPotential : public PotentialBase {
 
         posw_.alloc(S_);
         prm_.alloc(S_);
+        lamdep_.alloc(S_);
         if (interp_) {
             dprm_.alloc(S_);
         }
         split_pair_dp_ = interp_ && kind == Kind::Nonbonded;
-        acc_.alloc((size_t)S_ * (split_pair_dp_ ? 11 : 8));
+        acc_.alloc(acc_block_elems());
         acc_.zero();
 
         if (has_nblist_) {
@@ -165,7 +168,7 @@ class NonbondedPotential : public PotentialBase {
         DevState st{};
         st.rebuild = has_nblist_ ? 1 : 0;
         CK(cudaMemcpy(state_.p, &st, sizeof(st), cudaMemcpyHostToDevice));
-        AllKernels::fill(kernels_, interp_);
+        AllKernels::fill(kernels_, kernels_multi_, interp_);
         CK(cudaDeviceSynchronize());
     }
 
@@ -257,6 +260,23 @@ class NonbondedPotential : public PotentialBase {
     }
     void disable_hilbert() { hilbert_ = false; }
 
+    // Elements of one accumulator block (8 or 11 arrays of S slots).
+    size_t acc_block_elems() const { return (size_t)S_ * (split_pair_dp_ ? 11 : 8); }
+
+    // Staging and accumulator capacity for K windows: K staged copies of the
+    // slots and, for K > 1, the shared block plus one block per window.
+    void ensure_windows(int K) {
+        if (posw_.n < (size_t)K * S_) {
+            posw_.alloc((size_t)K * S_);
+            prm_.alloc((size_t)K * S_);
+        }
+        const size_t need = acc_block_elems() * (K > 1 ? 1 + K : 1);
+        if (acc_.n < need) {
+            acc_.alloc(need);
+            acc_.zero();
+        }
+    }
+
     void execute_device(
         int N,
         int P,
@@ -264,6 +284,25 @@ class NonbondedPotential : public PotentialBase {
         const double *d_p,
         const double *d_box,
         double lambda,
+        unsigned long long *d_du_dx,
+        unsigned long long *d_du_dp,
+        unsigned long long *d_du_dl,
+        unsigned long long *d_u,
+        cudaStream_t stream) override {
+        execute_windows_device(N, P, d_x, d_p, d_box, 1, &lambda, d_du_dx, d_du_dp, d_du_dl, d_u, stream);
+    }
+
+    // All windows in one launch sequence: one neighbour-list check/rebuild, one
+    // pair kernel in which tiles of lambda-independent atoms are evaluated once
+    // and the others once per window, one finalize writing K outputs.
+    void execute_windows_device(
+        int N,
+        int P,
+        const double *d_x,
+        const double *d_p,
+        const double *d_box,
+        int K,
+        const double *lambdas,
         unsigned long long *d_du_dx,
         unsigned long long *d_du_dp,
         unsigned long long *d_du_dl,
@@ -285,6 +324,13 @@ class NonbondedPotential : public PotentialBase {
         if (!d_x || !d_p || !d_box) {
             throw Error(TMNB_ERR_INVALID_ARGUMENT, "x, params and box must be non-null");
         }
+        if (K < 1 || K > MAX_WINDOWS || !lambdas) {
+            throw Error(
+                TMNB_ERR_INVALID_ARGUMENT,
+                "number of lambda windows must be in [1, " + std::to_string(MAX_WINDOWS) + "], got " +
+                    std::to_string(K));
+        }
+        ensure_windows(K);
 
         PrepareArgs pa;
         pa.N = N_;
@@ -292,7 +338,10 @@ class NonbondedPotential : public PotentialBase {
         pa.x = d_x;
         pa.p = d_p;
         pa.box = d_box;
-        pa.lambda = lambda;
+        pa.K = K;
+        for (int k = 0; k < MAX_WINDOWS; k++) {
+            pa.lambdas[k] = k < K ? lambdas[k] : 0.0;
+        }
         pa.cutoff = cutoff_;
         pa.padding = padding_;
         pa.plane = plane_.p;
@@ -301,6 +350,7 @@ class NonbondedPotential : public PotentialBase {
         pa.slots.posw = posw_.p;
         pa.slots.prm = prm_.p;
         pa.slots.dprm = dprm_.p;
+        pa.slots.lamdep = lamdep_.p;
 
         const int tpb = 256;
         const int sgrid = std::max(1, std::min((S_ + tpb - 1) / tpb, 8 * num_sms()));
@@ -345,6 +395,9 @@ class NonbondedPotential : public PotentialBase {
         if (kidx != 0) {
             PairArgs a;
             a.S = S_;
+            a.K = K;
+            a.lamdep = lamdep_.p;
+            a.acc_block = acc_block_elems();
             a.posw = posw_.p;
             a.prm = prm_.p;
             a.dprm = dprm_.p;
@@ -360,7 +413,7 @@ class NonbondedPotential : public PotentialBase {
             a.negated = negated_ ? 1 : 0;
             a.acc = accum();
             a.state = state_.p;
-            pair_kernel_t k = kernels_[kidx];
+            pair_kernel_t k = K > 1 ? kernels_multi_[kidx] : kernels_[kidx];
             if (timing_) {
                 CK(cudaEventRecord(ev_pair_[0], stream));
             }
@@ -376,9 +429,16 @@ class NonbondedPotential : public PotentialBase {
             fa.S = S_;
             fa.perm = perm_.p;
             fa.acc = accum();
+            fa.acc_block = acc_block_elems();
+            fa.K = K;
+            for (int w = 0; w < MAX_WINDOWS; w++) {
+                fa.lambdas[w] = pa.lambdas[w];
+            }
+            fa.stride_x = 3 * (size_t)N_;
+            fa.stride_p = (size_t)P;
+            fa.stride_n = (size_t)N_;
             fa.split_pair_dp = split_pair_dp_ ? 1 : 0;
             fa.interpolated = interp_ ? 1 : 0;
-            fa.lambda = lambda;
             fa.du_dx = d_du_dx;
             fa.du_dp = d_du_dp;
             fa.du_dl = d_du_dl;
@@ -518,6 +578,7 @@ class NonbondedPotential : public PotentialBase {
     DevBuf<double> scales_;
     DevBuf<unsigned> perm_;
     DevBuf<float4> posw_, prm_, dprm_;
+    DevBuf<unsigned char> lamdep_;
     DevBuf<unsigned long long> acc_;
     DevBuf<double> nb_x_, nb_box_;
     DevBuf<unsigned> keys_;
@@ -528,6 +589,7 @@ class NonbondedPotential : public PotentialBase {
     DevBuf<int4> items_;
     DevBuf<DevState> state_;
     pair_kernel_t kernels_[16];
+    pair_kernel_t kernels_multi_[16];
 
     // pair-kernel timing
     bool timing_ = false;
@@ -792,6 +854,58 @@ tmnb_status tmnb_potential_execute_host(
     return tmb::guarded([&] { pot->impl->execute_host(N, P, h_x, h_p, h_box, lambda, h_du_dx, h_du_dp, h_du_dl, h_u); });
 }
 
+tmnb_status tmnb_potential_execute_windows_device(
+    tmnb_potential *pot,
+    int N,
+    int P,
+    const double *d_x,
+    const double *d_p,
+    const double *d_box,
+    int K,
+    const double *lambdas,
+    unsigned long long *d_du_dx,
+    unsigned long long *d_du_dp,
+    unsigned long long *d_du_dl,
+    unsigned long long *d_u,
+    void *stream) {
+    if (tmnb_status s = check_handle(pot)) {
+        return s;
+    }
+    if (K < 1 || !lambdas) {
+        tmb::g_last_error = "K must be positive and lambdas non-null";
+        return TMNB_ERR_INVALID_ARGUMENT;
+    }
+    return tmb::guarded([&] {
+        pot->impl->execute_windows_device(
+            N, P, d_x, d_p, d_box, K, lambdas, d_du_dx, d_du_dp, d_du_dl, d_u, static_cast<cudaStream_t>(stream));
+    });
+}
+
+tmnb_status tmnb_potential_execute_windows_host(
+    tmnb_potential *pot,
+    int N,
+    int P,
+    const double *h_x,
+    const double *h_p,
+    const double *h_box,
+    int K,
+    const double *lambdas,
+    unsigned long long *h_du_dx,
+    unsigned long long *h_du_dp,
+    unsigned long long *h_du_dl,
+    unsigned long long *h_u) {
+    if (tmnb_status s = check_handle(pot)) {
+        return s;
+    }
+    if (!h_x || !h_box || (P > 0 && !h_p) || K < 1 || !lambdas) {
+        tmb::g_last_error = "null argument or K < 1";
+        return TMNB_ERR_INVALID_ARGUMENT;
+    }
+    return tmb::guarded([&] {
+        pot->impl->execute_windows_host(N, P, h_x, h_p, h_box, K, lambdas, h_du_dx, h_du_dp, h_du_dl, h_u);
+    });
+}
+
 tmnb_status tmnb_potential_execute_batch_host(
     tmnb_potential *pot,
     int coord_batches,
@@ -818,18 +932,21 @@ tmnb_status tmnb_potential_execute_batch_host(
         size_t e = 0;
         for (int c = 0; c < coord_batches; c++) {
             for (int p = 0; p < param_batches; p++) {
-                for (int l = 0; l < lambda_batches; l++, e++) {
-                    pot->impl->execute_host(
+                for (int l = 0; l < lambda_batches; l += tmb::MAX_WINDOWS) {
+                    const int K = std::min(tmb::MAX_WINDOWS, lambda_batches - l);
+                    pot->impl->execute_windows_host(
                         N,
                         P,
                         h_x + (size_t)c * N * 3,
                         h_p + (size_t)p * P,
                         h_boxes + (size_t)c * 9,
-                        h_lambdas[l],
+                        K,
+                        h_lambdas + l,
                         h_du_dx ? h_du_dx + e * N * 3 : nullptr,
                         h_du_dp ? h_du_dp + e * P : nullptr,
                         h_du_dl ? h_du_dl + e * N : nullptr,
                         h_u ? h_u + e * N : nullptr);
+                    e += K;
                 }
             }
         }

@@ -136,6 +136,27 @@ class Context:
         )
         return du_dl, xs, boxes
 
+    def multiple_steps_U(self, lamb, n_steps, lambda_windows, store_u_interval, store_x_interval):
+        """(U [F, K], xs, boxes): n_steps at lamb, the total energy at every
+        lambda window every store_u_interval steps (timemachine/cpp/src/wrap_kernels.cpp:186-219;
+        intervals <= 0 mean n_steps)."""
+        windows = np.ascontiguousarray(np.atleast_1d(lambda_windows), dtype=np.float64)
+        n_steps = int(n_steps)
+        u_int = n_steps if store_u_interval <= 0 else int(store_u_interval)
+        x_int = n_steps if store_x_interval <= 0 else int(store_x_interval)
+        F_u = n_steps // u_int if u_int > 0 else 0
+        F_x = n_steps // x_int if x_int > 0 else 0
+        u = np.zeros((F_u, windows.size))
+        xs = np.zeros((F_x, self.N, 3))
+        boxes = np.zeros((F_x, 3, 3))
+        _lib.check(
+            self._lib.tmnb_context_multiple_steps_U(
+                self._h, float(lamb), n_steps, windows.size, _p(windows), u_int, x_int, _p(u), _p(xs), _p(boxes),
+                1 if self.use_graphs else 0,
+            )
+        )
+        return u, xs, boxes
+
     def step(self, lamb):
         self.multiple_steps(np.array([lamb]))
 

@@ -18,7 +18,7 @@ import itertools
 import numpy as np
 
 from . import _lib
-from .fixed_point import FIXED_EXPONENT, fixed_to_float, du_dp_fixed_to_float, sum_fixed
+from .fixed_point import FIXED_EXPONENT, fixed_to_float, sum_fixed
 
 __all__ = [
     "CustomOpWrapper",
@@ -114,6 +114,21 @@ class Potential:
         )
         return out_dx, out_dp, out_dl, out_u
 
+    def _decode_dp(self, fixed):
+        """Fixed-point du_dp to float with this potential's per-column exponents
+        (Potential::du_dp_fixed_to_float, timemachine/cpp/src/potential.hpp:64)."""
+        fixed = np.ascontiguousarray(fixed, dtype=np.uint64)
+        flat = fixed.reshape(-1, fixed.shape[-1]) if fixed.ndim > 1 else fixed.reshape(1, -1)
+        out = np.empty(flat.shape, dtype=np.float64)
+        for r in range(flat.shape[0]):
+            row = np.ascontiguousarray(flat[r])
+            _lib.check(
+                self._lib.tmnb_potential_du_dp_fixed_to_float(
+                    self._h, self.num_atoms(), row.size, _ptr(row), _ptr(out[r])
+                )
+            )
+        return out.reshape(fixed.shape)
+
     def execute_selective(self, coords, params, box, lam, compute_du_dx, compute_du_dp, compute_du_dl, compute_u):
         """timemachine/cpp/src/wrap_kernels.cpp:552-625: tuple with None for outputs not requested."""
         params = np.asarray(params, dtype=np.float64)
@@ -121,7 +136,7 @@ class Potential:
             coords, params, box, lam, compute_du_dx, compute_du_dp, compute_du_dl, compute_u
         )
         du_dx = fixed_to_float(fdx) if compute_du_dx else None
-        du_dp = du_dp_fixed_to_float(fdp).reshape(params.shape) if compute_du_dp else None
+        du_dp = self._decode_dp(fdp).reshape(params.shape) if compute_du_dp else None
         du_dl = fixed_to_float(sum_fixed(fdl)) if compute_du_dl else None
         u = fixed_to_float(sum_fixed(fu)) if compute_u else None
         return du_dx, du_dp, du_dl, u
@@ -181,7 +196,7 @@ class Potential:
         if compute_du_dx:
             res[0] = fixed_to_float(out_dx).reshape(C, Pb, L, N, 3)
         if compute_du_dp:
-            res[1] = du_dp_fixed_to_float(out_dp).reshape((C, Pb, L) + params.shape[1:])
+            res[1] = self._decode_dp(out_dp).reshape((C, Pb, L) + params.shape[1:])
         if compute_du_dl:
             res[2] = np.array([fixed_to_float(sum_fixed(r)) for r in out_dl]).reshape(C, Pb, L)
         if compute_u:
@@ -189,7 +204,52 @@ class Potential:
         return tuple(res)
 
     def du_dp_fixed_to_float(self, N, P, du_dp):
-        return du_dp_fixed_to_float(np.asarray(du_dp, dtype=np.uint64))
+        return self._decode_dp(np.asarray(du_dp, dtype=np.uint64).reshape(-1))
+
+    def execute_windows_fixed(self, coords, params, box, lambdas, du_dx=True, du_dp=True, du_dl=True, u=True):
+        """K lambda windows of one (coords, params, box) in one multi-window
+        evaluation: raw uint64 fixed-point outputs with leading axis K (None
+        where not requested). Each window equals execute at lambdas[k] bit for bit."""
+        coords = np.ascontiguousarray(coords, dtype=np.float64)
+        params = np.ascontiguousarray(params, dtype=np.float64)
+        box = np.ascontiguousarray(box, dtype=np.float64)
+        lambdas = np.ascontiguousarray(np.atleast_1d(lambdas), dtype=np.float64)
+        if coords.ndim != 2 or coords.shape[1] != 3:
+            raise RuntimeError("coords must have shape (N, 3)")
+        if box.size != 9:
+            raise RuntimeError("box must have shape (3, 3)")
+        N, P, K = coords.shape[0], params.size, lambdas.size
+        out_dx = np.empty((K, N, 3), dtype=np.uint64) if du_dx else None
+        out_dp = np.empty((K, P), dtype=np.uint64) if du_dp else None
+        out_dl = np.empty((K, N), dtype=np.uint64) if du_dl else None
+        out_u = np.empty((K, N), dtype=np.uint64) if u else None
+        _lib.check(
+            self._lib.tmnb_potential_execute_windows_host(
+                self._h,
+                N,
+                P,
+                _ptr(coords),
+                _ptr(params),
+                _ptr(box),
+                K,
+                _ptr(lambdas),
+                _ptr(out_dx),
+                _ptr(out_dp),
+                _ptr(out_dl),
+                _ptr(out_u),
+            )
+        )
+        return out_dx, out_dp, out_dl, out_u
+
+    def execute_windows(self, coords, params, box, lambdas):
+        """(du_dx [K,N,3], du_dp [K,*params.shape], du_dl [K], u [K]) for K lambda windows."""
+        params = np.asarray(params, dtype=np.float64)
+        fdx, fdp, fdl, fu = self.execute_windows_fixed(coords, params, box, lambdas)
+        K = fdx.shape[0]
+        du_dp = self._decode_dp(fdp).reshape((K,) + params.shape)
+        du_dl = np.array([fixed_to_float(sum_fixed(r)) for r in fdl])
+        u = np.array([fixed_to_float(sum_fixed(r)) for r in fu])
+        return fixed_to_float(fdx), du_dp, du_dl, u
 
     # -- device entry point (torch tensors) -----------------------------------
     def execute_device(self, x, p, box, lam, du_dx=None, du_dp=None, du_dl=None, u=None, stream=None):
@@ -221,6 +281,41 @@ class Potential:
                 addr(p),
                 addr(box),
                 float(lam),
+                addr(du_dx),
+                addr(du_dp),
+                addr(du_dl),
+                addr(u),
+                ctypes.c_void_p(stream),
+            )
+        )
+
+    def execute_windows_device(self, x, p, box, lambdas, du_dx=None, du_dp=None, du_dl=None, u=None, stream=None):
+        """K lambda windows on device tensors; outputs [K,N,3] / [K,P] / [K,N]
+        int64 tensors that accumulate (the caller zeroes them)."""
+        import torch
+
+        def addr(t):
+            if t is None:
+                return None
+            if not t.is_contiguous():
+                raise RuntimeError("device tensors must be contiguous")
+            return ctypes.c_void_p(t.data_ptr())
+
+        lam = np.ascontiguousarray(np.atleast_1d(lambdas), dtype=np.float64)
+        if stream is None:
+            stream = torch.cuda.current_stream(x.device).cuda_stream
+        elif hasattr(stream, "cuda_stream"):
+            stream = stream.cuda_stream
+        _lib.check(
+            self._lib.tmnb_potential_execute_windows_device(
+                self._h,
+                x.shape[0],
+                p.numel(),
+                addr(x),
+                addr(p),
+                addr(box),
+                lam.size,
+                _ptr(lam),
                 addr(du_dx),
                 addr(du_dp),
                 addr(du_dl),
