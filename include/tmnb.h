@@ -364,6 +364,56 @@ tmnb_status tmnb_harmonic_angle_create(
 int tmnb_potential_num_params(const tmnb_potential *pot);
 int tmnb_potential_num_atoms(const tmnb_potential *pot);
 
+/* Largest N accepted by tmnb_pair_list_execute_static (3.16 MiB of static
+ * device scratch). */
+#define TMNB_STATIC_MAX_ATOMS 32768
+
+/*
+ * Allocation-free pair-list evaluation. NO REFERENCE COUNTERPART: it has the
+ * arguments of tmnb_pair_list_create (interpolated = 0, precision 32)
+ * followed by those of tmnb_potential_execute_device, with every array in
+ * device memory, and gives the same outputs (accumulated, +=).
+ *
+ * For callers that must not allocate device memory: processes that hand all
+ * of HBM to their own fixed arena or caching allocator up front (a raw
+ * cudaMalloc then fails or fragments it), and loops that cannot afford the
+ * device-wide synchronisation that cudaFree implies. It calls no cudaMalloc,
+ * cudaFree or allocating library routine: its slot staging, accumulators and
+ * device state live in a file-scope static device array of fixed size.
+ *
+ * Limit: 1 <= N <= TMNB_STATIC_MAX_ATOMS; larger N returns
+ * TMNB_ERR_INVALID_ARGUMENT ("N=... exceeds the static scratch capacity").
+ * The scratch must start at zero: it is zero at module load and every call
+ * leaves it at zero. The FIRST call on each device performs a one-time
+ * set-up with that device current (loads the kernels, looks up the scratch
+ * with cudaGetSymbolAddress, writes the identity slot order, synchronises
+ * the device); make that first call before any stream capture. Every call
+ * synchronises `stream` before returning, to report pair indices outside
+ * [0, N) or with src == dst (TMNB_ERR_INVALID_ARGUMENT; outputs unchanged).
+ * The scratch is shared by all calls on a device: calls that overlap in time
+ * (other host threads, or other streams still running) race on it and give
+ * wrong results; serialise them.
+ */
+tmnb_status tmnb_pair_list_execute_static(
+    int N,
+    int M,
+    const int32_t *d_pair_idxs,          /* [M,2] */
+    const double *d_scales,              /* [M,2] */
+    const int32_t *d_lambda_plane_idxs,  /* [N] */
+    const int32_t *d_lambda_offset_idxs, /* [N] */
+    double beta,
+    double cutoff,
+    int negated,
+    const double *d_x,           /* [N,3] */
+    const double *d_p,           /* [N,3] */
+    const double *d_box,         /* [3,3] */
+    double lambda,
+    unsigned long long *d_du_dx, /* [N,3] or NULL */
+    unsigned long long *d_du_dp, /* [N,3] or NULL */
+    unsigned long long *d_du_dl, /* [N] or NULL */
+    unsigned long long *d_u,     /* [N] or NULL */
+    void *stream);
+
 #ifdef __cplusplus
 }
 #endif

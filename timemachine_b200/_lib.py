@@ -25,7 +25,7 @@ NVCC_FLAGS = [
     "-shared",
 ]
 
-SOURCES = ["nonbonded.cu", "md.cu", "bonded.cu"]
+SOURCES = ["nonbonded.cu", "md.cu", "bonded.cu", "static_pairlist.cu"]
 
 
 def build(verbose: bool = False) -> str:
@@ -91,6 +91,8 @@ def _declare(lib):
     lib.tmnb_context_destroy.argtypes = [vp]
     lib.tmnb_harmonic_bond_create.argtypes = [i, i, vp, vp, vp, ctypes.POINTER(vp)]
     lib.tmnb_harmonic_angle_create.argtypes = [i, i, vp, vp, vp, ctypes.POINTER(vp)]
+    lib.tmnb_pair_list_execute_static.argtypes = [i, i, vp, vp, vp, vp, d, d, i, vp, vp, vp, d, vp, vp, vp, vp, vp]
+    lib.tmnb_pair_list_execute_static.restype = ctypes.c_int
     lib.tmnb_potential_num_params.argtypes = [vp]
     lib.tmnb_potential_num_atoms.argtypes = [vp]
     for name in [

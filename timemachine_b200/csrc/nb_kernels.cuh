@@ -18,6 +18,9 @@
 //  timemachine/cpp/src/neighborlist.cu:126-185,
 //  timemachine/cpp/src/nonbonded_pair_list.cu:95-166); the data layout,
 // spatial sort, scheduling and fusion are this file's own.
+//
+// The non-template kernels have internal linkage (static), so that several
+// translation units can include this file.
 #pragma once
 
 #include "nb_pair_math.cuh"
@@ -114,7 +117,7 @@ __device__ __forceinline__ void prepare_slot(const PrepareArgs &a, int s, int at
 // ---------------------------------------------------------------------------
 // Rebuild decision + staging.
 // ---------------------------------------------------------------------------
-__global__ void k_check_prepare(
+static __global__ void k_check_prepare(
     PrepareArgs a,
     const unsigned *__restrict__ perm, // [S] slot -> atom
     const double *__restrict__ nb_x,   // [N,3] coordinates at the last rebuild (nullptr: no neighbour list)
@@ -221,7 +224,7 @@ struct SortArgs {
 
 __device__ __forceinline__ int set_atom(const SortArgs &a, int k) { return a.set_atoms ? a.set_atoms[k] : k; }
 
-__global__ void k_bin_keys(SortArgs a, const DevState *state) {
+static __global__ void k_bin_keys(SortArgs a, const DevState *state) {
     if (!state->rebuild || state->error || !a.hilbert) {
         return;
     }
@@ -245,7 +248,7 @@ __global__ void k_bin_keys(SortArgs a, const DevState *state) {
 
 // Single-CTA exclusive scan of the cell counts (and reset of the counts and
 // of the tile-build counters).
-__global__ void k_bin_scan(SortArgs a, DevState *state) {
+static __global__ void k_bin_scan(SortArgs a, DevState *state) {
     if (!state->rebuild || state->error) {
         return;
     }
@@ -306,7 +309,7 @@ __global__ void k_bin_scan(SortArgs a, DevState *state) {
     }
 }
 
-__global__ void k_bin_scatter(
+static __global__ void k_bin_scatter(
     SortArgs sa,
     PrepareArgs pa,
     unsigned *__restrict__ perm,    // [S] slot -> atom
@@ -341,7 +344,7 @@ __global__ void k_bin_scatter(
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ float wrap_delta(float d, float L, float inv_L) { return d - L * rintf(d * inv_L); }
 
-__global__ void k_block_bounds(
+static __global__ void k_block_bounds(
     int S,
     const double *__restrict__ box,
     const float4 *__restrict__ posw,
@@ -417,7 +420,7 @@ __host__ __device__ __forceinline__ long long tile_offset(int rb, int RB) {
 
 constexpr int TB_WARPS = 4;
 
-__global__ void __launch_bounds__(TB_WARPS * 32) k_build_tiles(TileArgs a, DevState *state) {
+static __global__ void __launch_bounds__(TB_WARPS * 32) k_build_tiles(TileArgs a, DevState *state) {
     if (!state->rebuild || state->error) {
         return;
     }
@@ -586,7 +589,7 @@ __global__ void __launch_bounds__(TB_WARPS * 32) k_build_tiles(TileArgs a, DevSt
 }
 
 // Clears the rebuild flag when no neighbour list exists (pair lists only).
-__global__ void k_clear_rebuild(DevState *state) { state->rebuild = 0; }
+static __global__ void k_clear_rebuild(DevState *state) { state->rebuild = 0; }
 
 // ---------------------------------------------------------------------------
 // Pair kernel.
@@ -1139,7 +1142,7 @@ __device__ __forceinline__ unsigned long long take(unsigned long long *p) {
     return v;
 }
 
-__global__ void k_finalize(FinalizeArgs a) {
+static __global__ void k_finalize(FinalizeArgs a) {
     const bool ok = a.state->error == 0;
     const bool multi = a.K > 1;
     for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < a.S; s += gridDim.x * blockDim.x) {
