@@ -160,10 +160,32 @@ tmnb_status tmnb_potential_execute_host(
     unsigned long long *h_u);
 
 /*
+ * Replaces the NonbondedInteractionGroup constructors
+ * (timemachine/cpp/src/wrap_kernels.cpp:895-960,
+ * timemachine/cpp/src/nonbonded_interaction_group.cu:19-158): pairs (i, j)
+ * with i among the NR row atoms and j among the other N - NR atoms, no
+ * exclusions. row_atom_idxs must be non-empty, unique, < N and fewer than N
+ * ("row_atom_idxs must be nonempty", "atom indices must be unique", "number
+ * of idxs must be less than N", "indices values must be less than N").
+ * interpolated != 0: P = 2*N*3 (NonbondedInteractionGroupInterpolated).
+ */
+tmnb_status tmnb_interaction_group_create(
+    int N,
+    const int32_t *row_atom_idxs, /* [NR] */
+    int NR,
+    const int32_t *lambda_plane_idxs,  /* [N] */
+    const int32_t *lambda_offset_idxs, /* [N] */
+    double beta,
+    double cutoff,
+    int interpolated,
+    int precision,
+    tmnb_potential **out);
+
+/*
  * Multi-window device entry (no single reference counterpart: replaces the
  * loop over lambda windows that execute_selective_batch
  * (timemachine/cpp/src/wrap_kernels.cpp:381-551) and multiple_steps_U
- * (timemachine/cpp/src/context.cu:71-147) run with one execute_device per
+ * (timemachine/cpp/src/context.cu:139-234) run with one execute_device per
  * window). Evaluates K lambda windows (1 <= K <= TMNB_MAX_WINDOWS) of the same coordinates
  * and parameters in one launch sequence; window k's outputs start at
  * d_du_dx + 3*N*k, d_du_dp + P*k, d_du_dl + N*k, d_u + N*k and ACCUMULATE

@@ -187,6 +187,20 @@ def pair_list_oracle(x, params, box, lam, plane, offset, beta, cutoff, pair_idxs
     return gx.numpy(), gp.numpy(), gl, float(u.detach())
 
 
+def interaction_group_oracle(x, params, box, lam, plane, offset, beta, cutoff, row_idxs, interpolated=False):
+    """Pairs (a, b) with a among row_idxs and b among the other atoms
+    (timemachine/potentials/nonbonded.py:329-338, nonbonded_v3_interaction_groups
+    over pairs_from_interaction_groups), unscaled."""
+    x = np.asarray(x, dtype=np.float64)
+    N = x.shape[0]
+    rows = np.zeros(N, dtype=bool)
+    rows[np.asarray(row_idxs, dtype=np.int64)] = True
+    pairs = candidate_pairs(x, box, cutoff)
+    pairs = pairs[rows[pairs[:, 0]] != rows[pairs[:, 1]]]
+    ones = np.ones((len(pairs), 2))
+    return pair_list_oracle(x, params, box, lam, plane, offset, beta, cutoff, pairs, ones, interpolated)
+
+
 def force_error(ref, test):
     """max_i |F_ref - F_test|_inf / max(|F_ref,i|, 1) (tests/common.py:386-409 convention)."""
     ref = np.asarray(ref)

@@ -10,6 +10,8 @@
 // The objects built here are exactly the reference's:
 //   Nonbonded.unbound_impl  -> FanoutSummedPotential([NonbondedAllPairs, NonbondedPairList<Negated>])
 //                              (timemachine/lib/potentials.py:284-301)
+//   NonbondedInteractionGroup(_Interpolated)<float>
+//                              (timemachine/cpp/src/nonbonded_interaction_group.cu)
 //   Context + LangevinIntegrator + MonteCarloBarostat for MD throughput
 //                              (timemachine/cpp/src/context.cu, integrator.cu, barostat.cu)
 #include "bound_potential.hpp"
@@ -20,11 +22,13 @@
 #include "harmonic_bond.hpp"
 #include "integrator.hpp"
 #include "nonbonded_all_pairs.hpp"
+#include "nonbonded_interaction_group.hpp"
 #include "nonbonded_pair_list.hpp"
 
 #include <fstream>
 #include <memory>
 #include <regex>
+#include <set>
 #include <sstream>
 #include <stdexcept>
 #include <string>
@@ -160,6 +164,55 @@ int tmref_execute_device(
         r->fanout->execute_device(
             N, P, d_x, d_p, d_box, lambda, d_du_dx, d_du_dp, d_du_dl, d_u, static_cast<cudaStream_t>(stream));
     });
+}
+
+// A single reference potential (interaction group).
+struct RefPot {
+    std::shared_ptr<timemachine::Potential> pot;
+};
+
+void *tmref_group_create(
+    const char *kernel_dir,
+    int N,
+    const int *row_idxs,
+    int NR,
+    const int *plane,
+    const int *offset,
+    double beta,
+    double cutoff,
+    int interpolated) {
+    RefPot *h = nullptr;
+    int rc = guarded([&] {
+        const std::string src = jit_source(kernel_dir);
+        std::vector<int> pl(plane, plane + N), of(offset, offset + N);
+        std::set<int> rows(row_idxs, row_idxs + NR);
+        auto r = std::make_unique<RefPot>();
+        if (interpolated) {
+            r->pot = std::make_shared<timemachine::NonbondedInteractionGroup<float, true>>(rows, pl, of, beta, cutoff, src);
+        } else {
+            r->pot = std::make_shared<timemachine::NonbondedInteractionGroup<float, false>>(rows, pl, of, beta, cutoff, src);
+        }
+        h = r.release();
+    });
+    return rc == 0 ? h : nullptr;
+}
+
+void tmref_pot_destroy(void *h) { delete static_cast<RefPot *>(h); }
+
+int tmref_pot_execute_host(
+    void *h,
+    int N,
+    int P,
+    const double *h_x,
+    const double *h_p,
+    const double *h_box,
+    double lambda,
+    unsigned long long *h_du_dx,
+    unsigned long long *h_du_dp,
+    unsigned long long *h_du_dl,
+    unsigned long long *h_u) {
+    auto *r = static_cast<RefPot *>(h);
+    return guarded([&] { r->pot->execute_host(N, P, h_x, h_p, h_box, lambda, h_du_dx, h_du_dp, h_du_dl, h_u); });
 }
 
 int tmref_execute_host(

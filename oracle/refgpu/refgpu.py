@@ -47,6 +47,10 @@ def lib():
         L.tmref_disable_hilbert_sort.argtypes = [vp]
         L.tmref_execute_device.argtypes = [vp, i, i, vp, vp, vp, d, vp, vp, vp, vp, vp]
         L.tmref_execute_host.argtypes = [vp, i, i, vp, vp, vp, d, vp, vp, vp, vp]
+        L.tmref_group_create.restype = vp
+        L.tmref_group_create.argtypes = [ctypes.c_char_p, i, vp, i, vp, vp, d, d, i]
+        L.tmref_pot_destroy.argtypes = [vp]
+        L.tmref_pot_execute_host.argtypes = [vp, i, i, vp, vp, vp, d, vp, vp, vp, vp]
         L.tmref_md_create.restype = vp
         L.tmref_md_create.argtypes = [vp, i, vp, i, vp, vp, vp, d, d, vp, vp, i, d, d, vp, i, vp, i, vp, vp, i, vp]
         L.tmref_md_run.argtypes = [vp, i, d, vp, vp]
@@ -125,6 +129,38 @@ class RefNonbonded:
             np.zeros(N, np.uint64) if u else None,
         ]
         _check(lib().tmref_execute_host(self._h, N, p.size, _p(x), _p(p), _p(box), float(lam), *[_p(t) for t in o]))
+        return o
+
+
+class RefInteractionGroup:
+    """NonbondedInteractionGroup(_Interpolated)_f32 of the reference."""
+
+    def __init__(self, row_idxs, plane, offset, beta, cutoff, interpolated=False):
+        L = lib()
+        self._keep = [
+            np.ascontiguousarray(row_idxs, dtype=np.int32),
+            np.ascontiguousarray(plane, dtype=np.int32),
+            np.ascontiguousarray(offset, dtype=np.int32),
+        ]
+        r, pl, of = self._keep
+        self._h = L.tmref_group_create(
+            KERNEL_DIR.encode(), pl.size, _p(r), r.size, _p(pl), _p(of), beta, cutoff, 1 if interpolated else 0
+        )
+        if not self._h:
+            raise RuntimeError(L.tmref_last_error().decode())
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib().tmref_pot_destroy(self._h)
+            self._h = None
+
+    def execute_host_fixed(self, x, p, box, lam):
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        p = np.ascontiguousarray(p, dtype=np.float64)
+        box = np.ascontiguousarray(box, dtype=np.float64)
+        N = x.shape[0]
+        o = [np.zeros((N, 3), np.uint64), np.zeros(p.size, np.uint64), np.zeros(N, np.uint64), np.zeros(N, np.uint64)]
+        _check(lib().tmref_pot_execute_host(self._h, N, p.size, _p(x), _p(p), _p(box), float(lam), *[_p(t) for t in o]))
         return o
 
 

@@ -6,7 +6,13 @@ import pytest
 import torch
 from scipy.special import erfc
 
-from oracle.nonbonded_oracle import Oracle, candidate_pairs, exclusion_masks, pair_list_oracle
+from oracle.nonbonded_oracle import (
+    Oracle,
+    candidate_pairs,
+    exclusion_masks,
+    interaction_group_oracle,
+    pair_list_oracle,
+)
 from tests.conftest import load_golden
 from tests.helpers import f32_round, small_water_case
 
@@ -168,3 +174,26 @@ def test_exclusion_masks_lookup():
 def test_oracle_f32_rounding_convention():
     a = np.array([0.1, 1 / 3])
     assert np.all(f32_round(a) == np.float32(a).astype(np.float64))
+
+
+@pytest.mark.parametrize("interpolated", [False, True])
+def test_interaction_group_oracle_is_all_minus_both_groups(rng, interpolated):
+    """U_group = U_all - U_rows - U_cols (tests/nonbonded/test_nonbonded_interaction_group.py:188-258),
+    with every derivative, in FP64."""
+    c = small_water_case(rng, 180)
+    N = c["x"].shape[0]
+    rows = rng.choice(N, size=17, replace=False)
+    cols = np.setdiff1d(np.arange(N), rows)
+    params = c["params"]
+    if interpolated:
+        params = np.concatenate([params, params * 1.3])
+    lam = 0.3
+    g = interaction_group_oracle(c["x"], params, c["box"], lam, c["plane"], c["offset"], 2.0, 1.1, rows, interpolated)
+
+    def allp(idxs):
+        o = Oracle(c["plane"], c["offset"], 2.0, 1.1, interpolated=interpolated, atom_idxs=idxs)
+        return o(c["x"], params, c["box"], lam)
+
+    a, r, k = allp(None), allp(rows), allp(cols)
+    for n in range(4):
+        np.testing.assert_allclose(g[n], np.asarray(a[n]) - np.asarray(r[n]) - np.asarray(k[n]), rtol=1e-10, atol=1e-9)

@@ -61,6 +61,8 @@ def _declare(lib):
     lib.tmnb_version.restype = ctypes.c_char_p
     lib.tmnb_all_pairs_create.argtypes = [i, vp, vp, d, d, vp, i, i, i, ctypes.POINTER(vp)]
     lib.tmnb_pair_list_create.argtypes = [i, vp, vp, i, vp, vp, d, d, i, i, i, ctypes.POINTER(vp)]
+    lib.tmnb_interaction_group_create.argtypes = [i, vp, i, vp, vp, d, d, i, i, ctypes.POINTER(vp)]
+    lib.tmnb_interaction_group_create.restype = ctypes.c_int
     lib.tmnb_nonbonded_create.argtypes = [i, vp, vp, i, vp, vp, d, d, i, i, ctypes.POINTER(vp)]
     lib.tmnb_potential_destroy.argtypes = [vp]
     lib.tmnb_potential_execute_device.argtypes = [vp, i, i, vp, vp, vp, d, vp, vp, vp, vp, vp]

@@ -40,7 +40,7 @@ struct DevState {
     unsigned done_ctas;   // completion counter of k_build_tiles
     unsigned total_tiles; // tiles produced by the last rebuild
     int rebuilds;         // number of rebuilds performed (diagnostics)
-    int pad;
+    int n_dep;            // lambda-dependent tiles listed by k_dep_tiles (multi-window calls)
 };
 
 // Error codes written into DevState::error (mirrored in include/tmnb.h).
@@ -126,6 +126,7 @@ static __global__ void k_check_prepare(
     const int tid = blockIdx.x * blockDim.x + threadIdx.x;
     if (tid == 0) {
         state->next_item = 0;
+        state->n_dep = 0;
         if (nb_x != nullptr) {
             // Orthorhombic box whose every edge is at least twice cutoff+padding
             // (timemachine/cpp/src/nonbonded_all_pairs.cu:315-329); checked in
@@ -215,6 +216,8 @@ struct SortArgs {
     const double *x;
     const double *box;
     const int *set_atoms; // [S] atoms of the evaluated set, nullptr: identity (S == N)
+    int n_first;          // set entries [0, n_first) sort before the others (interaction
+                          // group rows before columns); S: one group
     int grid_bits;        // b: 2^b cells per axis
     int hilbert;          // 0: keep the set order
     unsigned *keys;       // [S]
@@ -240,7 +243,10 @@ static __global__ void k_bin_keys(SortArgs a, const DevState *state) {
             ci = ci < 0 ? 0 : (ci >= G ? G - 1 : ci);
             c[d] = (unsigned)ci;
         }
-        const unsigned key = hilbert_index_3d(c[0], c[1], c[2], a.grid_bits);
+        unsigned key = hilbert_index_3d(c[0], c[1], c[2], a.grid_bits);
+        if (k >= a.n_first) {
+            key += 1u << (3 * a.grid_bits);
+        }
         a.keys[k] = key;
         atomicAdd(&a.bin_count[key], 1);
     }
@@ -259,7 +265,7 @@ static __global__ void k_bin_scan(SortArgs a, DevState *state) {
     if (!a.hilbert) {
         return;
     }
-    const int NB = 1 << (3 * a.grid_bits);
+    const int NB = (1 << (3 * a.grid_bits)) * (a.n_first < a.S ? 2 : 1);
     __shared__ int warp_sums[32];
     __shared__ int carry;
     if (threadIdx.x == 0) {
@@ -402,7 +408,12 @@ static __global__ void k_block_bounds(
 // ---------------------------------------------------------------------------
 struct TileArgs {
     int S;
-    int RB;           // row blocks = column blocks = ceil(S/32)
+    int RB;           // blocks of 32 slots = ceil(S/32)
+    int group;        // 1: interaction group (rows [0, row_end) x columns [col_begin, S))
+    int row_end;      // S, or the number of row atoms
+    int col_begin;    // 0, or the number of row atoms
+    int n_row_blocks; // RB, or ceil(row_end/32)
+    int cb_first;     // group: first column block (col_begin/32)
     float radius;     // list radius (cutoff + padding + margin)
     const double *box;
     const float4 *posw;
@@ -418,7 +429,13 @@ __host__ __device__ __forceinline__ long long tile_offset(int rb, int RB) {
     return (long long)rb * RB - ((long long)rb * (rb - 1)) / 2;
 }
 
-constexpr int TB_WARPS = 4;
+// First tile of row block rb: upper triangle (RB - rb tiles per row block),
+// or for an interaction group RB - cb_first tiles per row block.
+__host__ __device__ __forceinline__ long long tile_base(const TileArgs &a, int rb) {
+    return a.group ? (long long)rb * (a.RB - a.cb_first) : tile_offset(rb, a.RB);
+}
+
+constexpr int TB_WARPS = 8;
 
 static __global__ void __launch_bounds__(TB_WARPS * 32) k_build_tiles(TileArgs a, DevState *state) {
     if (!state->rebuild || state->error) {
@@ -438,24 +455,25 @@ static __global__ void __launch_bounds__(TB_WARPS * 32) k_build_tiles(TileArgs a
     const float Lx = (float)a.box[0], Ly = (float)a.box[4], Lz = (float)a.box[8];
     const float iLx = 1.0f / Lx, iLy = 1.0f / Ly, iLz = 1.0f / Lz;
     const float r2 = a.radius * a.radius;
+    const float r2_box = (a.radius + 1e-4f) * (a.radius + 1e-4f);
 
     if (threadIdx.x < TILE) {
         const int s = rb * TILE + threadIdx.x;
-        row_pos[threadIdx.x] = s < S ? a.posw[s] : make_float4(0.f, 0.f, 0.f, 0.f);
+        row_pos[threadIdx.x] = s < a.row_end ? a.posw[s] : make_float4(0.f, 0.f, 0.f, 0.f);
     }
     if (threadIdx.x == 0) {
         tile_count = 0;
         rem_count = 0;
     }
     __syncthreads();
-    const int row_n = min(TILE, S - rb * TILE);
+    const int row_n = min(TILE, a.row_end - rb * TILE);
     const float4 rc = a.bb_ctr[rb];
     const float4 re = a.bb_ext[rb];
-    const long long base_tile = tile_offset(rb, a.RB);
+    const long long base_tile = tile_base(a, rb);
     const unsigned lane_lt = (1u << lane) - 1;
 
     int count = 0; // atoms in this warp's buffer
-    for (int cbase = rb + warp * TILE; cbase < a.RB; cbase += TB_WARPS * TILE) {
+    for (int cbase = (a.group ? a.cb_first : rb) + warp * TILE; cbase < a.RB; cbase += TB_WARPS * TILE) {
         const int cb = cbase + lane;
         bool pass = false;
         if (cb < a.RB) {
@@ -473,18 +491,31 @@ static __global__ void __launch_bounds__(TB_WARPS * 32) k_build_tiles(TileArgs a
             const int s = cb_sel * TILE + lane;
             const bool valid = s < S;
             const float4 pj = valid ? a.posw[s] : make_float4(0.f, 0.f, 0.f, 0.f);
+            // an atom farther than the radius from the row block's box is
+            // farther than the radius from every row atom (widened test,
+            // conservative under rounding): skip its per-row test
+            const float bx = fmaxf(0.f, fabsf(wrap_delta(pj.x - rc.x, Lx, iLx)) - re.x);
+            const float by = fmaxf(0.f, fabsf(wrap_delta(pj.y - rc.y, Ly, iLy)) - re.y);
+            const float bz = fmaxf(0.f, fabsf(wrap_delta(pj.z - rc.z, Lz, iLz)) - re.z);
+            const bool need = valid && s >= a.col_begin && bx * bx + by * by + bz * bz < r2_box;
             bool hit = false;
-            for (int r = 0; r < row_n; r++) {
-                const float4 pi = row_pos[r];
-                const float dx = wrap_delta(pi.x - pj.x, Lx, iLx);
-                const float dy = wrap_delta(pi.y - pj.y, Ly, iLy);
-                const float dz = wrap_delta(pi.z - pj.z, Lz, iLz);
-                hit |= dx * dx + dy * dy + dz * dz < r2;
-                if ((r & 7) == 7 && __all_sync(FULL_MASK, hit || !valid)) {
-                    break;
+            if (__any_sync(FULL_MASK, need)) {
+                // rows in groups of 8 (independent tests, then one vote)
+                for (int r0 = 0; r0 < row_n; r0 += 8) {
+#pragma unroll
+                    for (int r = r0; r < r0 + 8; r++) {
+                        const float4 pi = row_pos[r]; // rows past row_n hold zeros and are masked below
+                        const float dx = wrap_delta(pi.x - pj.x, Lx, iLx);
+                        const float dy = wrap_delta(pi.y - pj.y, Ly, iLy);
+                        const float dz = wrap_delta(pi.z - pj.z, Lz, iLz);
+                        hit |= (r < row_n) && (dx * dx + dy * dy + dz * dz < r2);
+                    }
+                    if (__all_sync(FULL_MASK, hit || !need)) {
+                        break;
+                    }
                 }
             }
-            hit = hit && valid;
+            hit = hit && need;
             const unsigned hmask = __ballot_sync(FULL_MASK, hit);
             if (hit) {
                 buf[warp][count + __popc(hmask & lane_lt)] = (unsigned)s;
@@ -533,7 +564,7 @@ static __global__ void __launch_bounds__(TB_WARPS * 32) k_build_tiles(TileArgs a
     __syncthreads();
     if (threadIdx.x == 0) {
         const unsigned prev = atomicAdd(&state->done_ctas, 1u);
-        is_last = (prev == (unsigned)a.RB - 1);
+        is_last = (prev == (unsigned)a.n_row_blocks - 1);
     }
     __syncthreads();
     if (!is_last) {
@@ -546,9 +577,9 @@ static __global__ void __launch_bounds__(TB_WARPS * 32) k_build_tiles(TileArgs a
         carry = 0;
     }
     __syncthreads();
-    for (int base = 0; base < a.RB; base += blockDim.x) {
+    for (int base = 0; base < a.n_row_blocks; base += blockDim.x) {
         const int r = base + threadIdx.x;
-        const int nt = r < a.RB ? *((volatile int *)&a.rb_ntiles[r]) : 0;
+        const int nt = r < a.n_row_blocks ? *((volatile int *)&a.rb_ntiles[r]) : 0;
         const int ni = (nt + a.chunk - 1) / a.chunk;
         int incl = ni;
         for (int o = 1; o < 32; o <<= 1) {
@@ -568,7 +599,7 @@ static __global__ void __launch_bounds__(TB_WARPS * 32) k_build_tiles(TileArgs a
         int pos = carry + wprefix + incl - ni;
         for (int c = 0; c < ni; c++) {
             const int first = c * a.chunk;
-            a.items[pos + c] = make_int4(r, (int)(tile_offset(r, a.RB) + first), min(a.chunk, nt - first), 0);
+            a.items[pos + c] = make_int4(r, (int)(tile_base(a, r) + first), min(a.chunk, nt - first), 0);
         }
         __syncthreads();
         if (threadIdx.x == 0) {
@@ -622,6 +653,7 @@ __device__ __forceinline__ Accum acc_block(const Accum &a, size_t block, int b) 
 
 struct PairArgs {
     int S;
+    int row_end;                // slots [0, row_end) act as rows (S, or the interaction group's rows)
     int K;                      // lambda windows
     const float4 *posw;         // [K][S]
     const float4 *prm;          // [K][S]
@@ -640,6 +672,7 @@ struct PairArgs {
     int negated;
     Accum acc;             // block 0
     size_t acc_block;      // elements between accumulator blocks
+    const int2 *dep_tiles; // [n_dep] (row block, tile) of the lambda-dependent tiles (multi-window)
     DevState *state;
 };
 
@@ -945,8 +978,9 @@ __device__ __forceinline__ void tile_pass(
     unsigned long long &du_dl,
     unsigned long long &energy) {
     const size_t wo = (size_t)window * a.S;
-    const bool row_ok = i < S;
+    const bool row_ok = i < (unsigned)a.row_end;
     const bool col_ok = j < S;
+    const unsigned i_eff = row_ok ? i : 0xffffffffu; // invalid rows pair with nothing
     const float4 pwi = row_ok ? a.posw[wo + i] : make_float4(0.f, 0.f, 0.f, 0.f);
     const float4 pri = row_ok ? a.prm[wo + i] : make_float4(0.f, 0.f, 0.f, 0.f);
     const float4 pwj = col_ok ? a.posw[wo + j] : make_float4(0.f, 0.f, 0.f, 0.f);
@@ -967,13 +1001,13 @@ __device__ __forceinline__ void tile_pass(
     unsigned long long gj_x = 0, gj_y = 0, gj_z = 0, g_qj = 0, g_sigj = 0, g_epsj = 0;
     if (alch) {
         sweep_tile<Real, U, DX, DL, DP, INTERP, true>(
-            lane, S, i, j, pwi.x, pwi.y, pwi.z, pwi.w, pri.x, pri.y, pri.z, pri.w, dpi.x, dpi.y, dpi.z, pwj.x, pwj.y,
+            lane, S, i_eff, j, pwi.x, pwi.y, pwi.z, pwi.w, pri.x, pri.y, pri.z, pri.w, dpi.x, dpi.y, dpi.z, pwj.x, pwj.y,
             pwj.z, pwj.w, prj.x, prj.y, prj.z, prj.w, dpj.x, dpj.y, dpj.z, box_x, box_y, box_z, inv_box_x, inv_box_y,
             inv_box_z, cutoff_squared, beta, gi_x, gi_y, gi_z, g_qi, g_sigi, g_epsi, du_dl, energy, gj_x, gj_y, gj_z,
             g_qj, g_sigj, g_epsj);
     } else {
         sweep_tile<Real, U, DX, DL, DP, INTERP, false>(
-            lane, S, i, j, pwi.x, pwi.y, pwi.z, pwi.w, pri.x, pri.y, pri.z, pri.w, dpi.x, dpi.y, dpi.z, pwj.x, pwj.y,
+            lane, S, i_eff, j, pwi.x, pwi.y, pwi.z, pwi.w, pri.x, pri.y, pri.z, pri.w, dpi.x, dpi.y, dpi.z, pwj.x, pwj.y,
             pwj.z, pwj.w, prj.x, prj.y, prj.z, prj.w, dpj.x, dpj.y, dpj.z, box_x, box_y, box_z, inv_box_x, inv_box_y,
             inv_box_z, cutoff_squared, beta, gi_x, gi_y, gi_z, g_qi, g_sigi, g_epsi, du_dl, energy, gj_x, gj_y, gj_z,
             g_qj, g_sigj, g_epsj);
@@ -1022,9 +1056,48 @@ __device__ __forceinline__ void flush_row(
     }
 }
 
-// Persistent pair kernel. MULTI: K > 1 lambda windows; tiles and scaled pairs
-// whose atoms are all lambda-independent are evaluated once into the shared
-// accumulator block, the others once per window into the window's block.
+// Multi-window calls: lists the tiles with at least one lambda-dependent row
+// or column atom (the tiles the pair kernel evaluates once per window). One
+// warp per work item, grid-stride.
+struct DepArgs {
+    int S;
+    int row_end;
+    const int4 *items;
+    const unsigned *tile_cols;
+    const unsigned char *lamdep;
+    int2 *dep_tiles;
+};
+
+static __global__ void k_dep_tiles(DepArgs a, DevState *state) {
+    if (state->error) {
+        return;
+    }
+    const int lane = threadIdx.x & 31;
+    const int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int n_warps = (gridDim.x * blockDim.x) >> 5;
+    const unsigned S = (unsigned)a.S;
+    const int n_items = state->n_items;
+    for (int w = warp; w < n_items; w += n_warps) {
+        const int4 it = a.items[w];
+        const unsigned i = (unsigned)(it.x * TILE + lane);
+        const bool row_dep = i < (unsigned)a.row_end && a.lamdep[i];
+        for (int t = 0; t < it.z; t++) {
+            const int tile = it.y + t;
+            const unsigned j = a.tile_cols[(long long)tile * TILE + lane];
+            if (__any_sync(FULL_MASK, row_dep || (j < S && a.lamdep[j])) && lane == 0) {
+                a.dep_tiles[atomicAdd(&state->n_dep, 1)] = make_int2(it.x, tile);
+            }
+        }
+    }
+}
+
+// Persistent pair kernel over dynamically scheduled work units:
+//   [0, n_items)                 tile work items (row block, first tile, count);
+//   MULTI only: [n_items, + n_dep*K)  one lambda-dependent tile at one window;
+//   then                         chunks of 32 scaled pairs (one per lane).
+// MULTI (K > 1 windows): the tile items skip lambda-dependent tiles and add
+// into the shared accumulator block; each (tile, window) unit adds into the
+// window's block; a lambda-dependent scaled pair is evaluated for every window.
 template <typename Real, bool U, bool DX, bool DL, bool DP, bool INTERP, bool MULTI>
 __global__ void __launch_bounds__(128) k_pair(PairArgs a) {
     if (a.state->error) {
@@ -1042,7 +1115,9 @@ __global__ void __launch_bounds__(128) k_pair(PairArgs a) {
     const Real beta = static_cast<Real>(a.beta);
     const unsigned S = (unsigned)a.S;
     const int n_items = a.state->n_items;
-    const int n_total = n_items + (a.M + TILE - 1) / TILE;
+    const int n_dep_units = MULTI ? a.state->n_dep * a.K : 0;
+    const int n_tiles_units = n_items + n_dep_units;
+    const int n_total = n_tiles_units + (a.M + TILE - 1) / TILE;
 
     for (;;) {
         int item = 0;
@@ -1053,8 +1128,8 @@ __global__ void __launch_bounds__(128) k_pair(PairArgs a) {
         if (item >= n_total) {
             break;
         }
-        if (item >= n_items) {
-            const int pair = (item - n_items) * TILE + lane;
+        if (item >= n_tiles_units) {
+            const int pair = (item - n_tiles_units) * TILE + lane;
             if (pair < a.M) {
                 const int atom_i = a.pair_idxs[2 * pair + 0];
                 const int atom_j = a.pair_idxs[2 * pair + 1];
@@ -1074,32 +1149,37 @@ __global__ void __launch_bounds__(128) k_pair(PairArgs a) {
             }
             continue;
         }
+        if (MULTI && item >= n_items) {
+            const int unit = item - n_items;
+            const int2 dt = a.dep_tiles[unit / a.K];
+            const int k = unit % a.K;
+            const unsigned i = (unsigned)(dt.x * TILE + lane);
+            const unsigned j = a.tile_cols[(long long)dt.y * TILE + lane];
+            const Accum wk = acc_block(a.acc, a.acc_block, 1 + k);
+            unsigned long long wx = 0, wy = 0, wz = 0, wq = 0, ws = 0, we = 0, wl = 0, wu = 0;
+            tile_pass<Real, U, DX, DL, DP, INTERP>(
+                a, lane, S, i, j, k, wk, box_x, box_y, box_z, inv_box_x, inv_box_y, inv_box_z, cutoff_squared, beta,
+                wx, wy, wz, wq, ws, we, wl, wu);
+            if (i < (unsigned)a.row_end) {
+                flush_row<U, DX, DL, DP>(wk, i, wx, wy, wz, wq, ws, we, wl, wu);
+            }
+            continue;
+        }
         const int4 it = a.items[item];
         const unsigned i = (unsigned)(it.x * TILE + lane);
-        const bool row_dep = MULTI && i < S && a.lamdep[i];
+        const bool row_dep = MULTI && i < (unsigned)a.row_end && a.lamdep[i];
         unsigned long long gi_x = 0, gi_y = 0, gi_z = 0, g_qi = 0, g_sigi = 0, g_epsi = 0, du_dl = 0, energy = 0;
         for (int t = 0; t < it.z; t++) {
             const long long tile = (long long)it.y + t;
             const unsigned j = a.tile_cols[tile * TILE + lane];
-            const bool dep = MULTI && __any_sync(FULL_MASK, row_dep || (j < S && a.lamdep[j]));
-            if (!dep) {
-                tile_pass<Real, U, DX, DL, DP, INTERP>(
-                    a, lane, S, i, j, 0, a.acc, box_x, box_y, box_z, inv_box_x, inv_box_y, inv_box_z, cutoff_squared,
-                    beta, gi_x, gi_y, gi_z, g_qi, g_sigi, g_epsi, du_dl, energy);
-            } else {
-                for (int k = 0; k < a.K; k++) {
-                    const Accum wk = acc_block(a.acc, a.acc_block, 1 + k);
-                    unsigned long long wx = 0, wy = 0, wz = 0, wq = 0, ws = 0, we = 0, wl = 0, wu = 0;
-                    tile_pass<Real, U, DX, DL, DP, INTERP>(
-                        a, lane, S, i, j, k, wk, box_x, box_y, box_z, inv_box_x, inv_box_y, inv_box_z, cutoff_squared,
-                        beta, wx, wy, wz, wq, ws, we, wl, wu);
-                    if (i < S) {
-                        flush_row<U, DX, DL, DP>(wk, i, wx, wy, wz, wq, ws, we, wl, wu);
-                    }
-                }
+            if (MULTI && __any_sync(FULL_MASK, row_dep || (j < S && a.lamdep[j]))) {
+                continue; // evaluated per window by the (tile, window) units
             }
+            tile_pass<Real, U, DX, DL, DP, INTERP>(
+                a, lane, S, i, j, 0, a.acc, box_x, box_y, box_z, inv_box_x, inv_box_y, inv_box_z, cutoff_squared,
+                beta, gi_x, gi_y, gi_z, g_qi, g_sigi, g_epsi, du_dl, energy);
         }
-        if (i < S) {
+        if (i < (unsigned)a.row_end) {
             flush_row<U, DX, DL, DP>(a.acc, i, gi_x, gi_y, gi_z, g_qi, g_sigi, g_epsi, du_dl, energy);
         }
     }
@@ -1118,7 +1198,9 @@ struct FinalizeArgs {
     int S;
     int K;
     double lambdas[MAX_WINDOWS];
-    const unsigned *perm;
+    const int *set_atoms; // [S] atoms of the evaluated set in ascending order, nullptr: 0..S-1
+    const int *slot_of;   // [N] atom -> slot, nullptr: identity
+    int take;             // 1: zero each accumulator after reading it; 0: the caller zeroes them
     Accum acc;
     size_t acc_block;
     int split_pair_dp; // 1: acc.pq/psig/peps are separate buffers
@@ -1142,71 +1224,71 @@ __device__ __forceinline__ unsigned long long take(unsigned long long *p) {
     return v;
 }
 
+// One thread per (window k, set atom), consecutive threads on consecutive
+// atoms, so the output updates are coalesced and the slot-ordered
+// accumulators are gathered through slot_of. Only the accumulators of
+// requested outputs are read (the others were never written and stay zero).
+// take = 1 zeroes each accumulator after the read (one window, identity slot
+// order); otherwise the caller zeroes the accumulator blocks after this kernel.
 static __global__ void k_finalize(FinalizeArgs a) {
     const bool ok = a.state->error == 0;
     const bool multi = a.K > 1;
-    for (int s = blockIdx.x * blockDim.x + threadIdx.x; s < a.S; s += gridDim.x * blockDim.x) {
-        const int atom = a.perm[s];
-        const Accum &c = a.acc;
-        const size_t B = a.acc_block;
-        const unsigned long long shared_x = take(c.x + s), shared_y = take(c.y + s), shared_z = take(c.z + s);
-        const unsigned long long shared_q = take(c.q + s), shared_sig = take(c.sig + s), shared_eps = take(c.eps + s);
-        const unsigned long long shared_u = take(c.u + s), shared_dl = take(c.dl + s);
-        unsigned long long shared_pq = 0, shared_psig = 0, shared_peps = 0;
-        if (a.split_pair_dp) {
-            shared_pq = take(c.pq + s);
-            shared_psig = take(c.psig + s);
-            shared_peps = take(c.peps + s);
-        }
-        for (int k = 0; k < a.K; k++) {
-            unsigned long long vx = shared_x, vy = shared_y, vz = shared_z;
-            unsigned long long v0[3] = {shared_q, shared_sig, shared_eps};
-            unsigned long long v1[3] = {shared_pq, shared_psig, shared_peps};
-            unsigned long long vu = shared_u, vl = shared_dl;
+    const size_t total = (size_t)a.S * (size_t)a.K;
+    const Accum &c = a.acc;
+    for (size_t t = blockIdx.x * (size_t)blockDim.x + threadIdx.x; t < total; t += (size_t)gridDim.x * blockDim.x) {
+        const int k = (int)(t / (size_t)a.S);
+        const int idx = (int)(t - (size_t)k * a.S);
+        const int atom = a.set_atoms ? a.set_atoms[idx] : idx;
+        const int s = a.slot_of ? a.slot_of[atom] : atom;
+        const size_t o = a.acc_block * (size_t)(1 + k) + s;
+        auto get = [&](unsigned long long *p) -> unsigned long long {
             if (multi) {
-                const size_t o = B * (1 + k) + s;
-                vx += take(c.x + o);
-                vy += take(c.y + o);
-                vz += take(c.z + o);
-                v0[0] += take(c.q + o);
-                v0[1] += take(c.sig + o);
-                v0[2] += take(c.eps + o);
-                vu += take(c.u + o);
-                vl += take(c.dl + o);
-                if (a.split_pair_dp) {
-                    v1[0] += take(c.pq + o);
-                    v1[1] += take(c.psig + o);
-                    v1[2] += take(c.peps + o);
-                }
+                return p[s] + p[o];
             }
-            if (!ok) {
-                continue;
+            return a.take ? take(p + s) : p[s];
+        };
+        if (a.du_dx) {
+            const unsigned long long vx = get(c.x), vy = get(c.y), vz = get(c.z);
+            if (ok) {
+                unsigned long long *out = a.du_dx + a.stride_x * k + 3 * (size_t)atom;
+                out[0] += vx;
+                out[1] += vy;
+                out[2] += vz;
             }
-            if (a.du_dx) {
-                unsigned long long *o = a.du_dx + a.stride_x * k + 3 * (size_t)atom;
-                o[0] += vx;
-                o[1] += vy;
-                o[2] += vz;
+        }
+        if (a.du_dp) {
+            unsigned long long v0[3] = {get(c.q), get(c.sig), get(c.eps)};
+            unsigned long long v1[3] = {0, 0, 0};
+            if (a.split_pair_dp) {
+                v1[0] = get(c.pq);
+                v1[1] = get(c.psig);
+                v1[2] = get(c.peps);
             }
-            if (a.du_dp) {
+            if (ok) {
                 const unsigned long long ex[3] = {FX_EXPONENT, FX_EXPONENT_SIG, FX_EXPONENT_EPS};
-                unsigned long long *o = a.du_dp + a.stride_p * k;
+                unsigned long long *out = a.du_dp + a.stride_p * k;
                 for (int d = 0; d < 3; d++) {
                     if (a.interpolated) {
                         const double f = a.lambdas[k];
                         unsigned long long lo = interp_part(1 - f, v0[d], ex[d]) + interp_part(1 - f, v1[d], ex[d]);
                         unsigned long long hi = interp_part(f, v0[d], ex[d]) + interp_part(f, v1[d], ex[d]);
-                        o[3 * (size_t)atom + d] += lo;
-                        o[3 * ((size_t)a.N + atom) + d] += hi;
+                        out[3 * (size_t)atom + d] += lo;
+                        out[3 * ((size_t)a.N + atom) + d] += hi;
                     } else {
-                        o[3 * (size_t)atom + d] += v0[d] + v1[d];
+                        out[3 * (size_t)atom + d] += v0[d] + v1[d];
                     }
                 }
             }
-            if (a.u) {
+        }
+        if (a.u) {
+            const unsigned long long vu = get(c.u);
+            if (ok) {
                 a.u[a.stride_n * k + atom] += vu;
             }
-            if (a.du_dl) {
+        }
+        if (a.du_dl) {
+            const unsigned long long vl = get(c.dl);
+            if (ok) {
                 a.du_dl[a.stride_n * k + atom] += vl;
             }
         }

@@ -7,6 +7,9 @@
 //   Nonbonded (timemachine/lib/potentials.py:269-301: AllPairs + negated
 //              PairList of the exclusions), evaluated as ONE pipeline whose
 //              exclusion pairs run inside the pair kernel's launch.
+//   Group     (timemachine/cpp/src/nonbonded_interaction_group.cu): pairs of
+//              one row atom and one column atom (the complement); slots hold
+//              the spatially sorted rows, then the sorted columns.
 #include "engine.hpp"
 #include "nb_kernels.cuh"
 
@@ -21,7 +24,7 @@
 
 namespace tmb {
 
-enum class Kind { AllPairs, PairList, Nonbonded };
+enum class Kind { AllPairs, PairList, Nonbonded, Group };
 
 typedef void (*pair_kernel_t)(PairArgs);
 
@@ -77,6 +80,30 @@ class NonbondedPotential : public PotentialBase {
         has_nblist_ = kind != Kind::PairList;
         S_ = N;
         std::vector<int> set_atoms;
+        if (kind == Kind::Group) {
+            // timemachine/cpp/src/nonbonded_interaction_group.cu:62-64 and
+            // timemachine/cpp/src/neighborlist.cu:215-228
+            if (atom_idxs == nullptr || K <= 0) {
+                throw Error(TMNB_ERR_INVALID_ARGUMENT, "row_atom_idxs must be nonempty");
+            }
+            std::set<int> uniq(atom_idxs, atom_idxs + K);
+            if ((int)uniq.size() != K) {
+                throw Error(TMNB_ERR_INVALID_ARGUMENT, "atom indices must be unique");
+            }
+            if (K >= N) {
+                throw Error(TMNB_ERR_INVALID_ARGUMENT, "number of idxs must be less than N");
+            }
+            if (*uniq.rbegin() >= N || *uniq.begin() < 0) {
+                throw Error(TMNB_ERR_INVALID_ARGUMENT, "indices values must be less than N");
+            }
+            set_atoms.assign(uniq.begin(), uniq.end());
+            for (int a = 0; a < N; a++) {
+                if (!uniq.count(a)) {
+                    set_atoms.push_back(a);
+                }
+            }
+            NR_ = K;
+        }
         if (kind == Kind::AllPairs && atom_idxs != nullptr) {
             std::set<int> uniq(atom_idxs, atom_idxs + K);
             if ((int)uniq.size() != K) {
@@ -126,12 +153,15 @@ class NonbondedPotential : public PotentialBase {
             perm[s] = set_atoms.empty() ? (unsigned)s : (unsigned)set_atoms[s];
         }
         perm_.upload(perm.data(), S_);
-        if (kind == Kind::Nonbonded) {
-            std::vector<int> slot(N);
+        if (has_nblist_ || kind == Kind::Nonbonded) {
+            std::vector<int> slot(N, -1);
             for (int s = 0; s < S_; s++) {
                 slot[perm[s]] = s;
             }
             slot_of_.upload(slot.data(), N);
+        }
+        if (kind == Kind::AllPairs && !set_atoms.empty()) {
+            fin_atoms_.upload(set_atoms.data(), S_); // ascending
         }
 
         posw_.alloc(S_);
@@ -146,6 +176,13 @@ class NonbondedPotential : public PotentialBase {
 
         if (has_nblist_) {
             RB_ = (S_ + TILE - 1) / TILE;
+            if (kind == Kind::Group) {
+                n_row_blocks_ = (NR_ + TILE - 1) / TILE;
+                cb_first_ = NR_ / TILE;
+            } else {
+                n_row_blocks_ = RB_;
+                cb_first_ = 0;
+            }
             nb_x_.alloc(3 * (size_t)N);
             nb_x_.zero();
             nb_box_.alloc(9);
@@ -154,13 +191,13 @@ class NonbondedPotential : public PotentialBase {
             int b = (int)std::ceil(std::log2(std::cbrt(std::max(1.0, S_ / 8.0))));
             grid_bits_ = std::min(6, std::max(2, b));
             keys_.alloc(S_);
-            bin_count_.alloc((size_t)1 << (3 * grid_bits_));
+            const size_t bins = ((size_t)1 << (3 * grid_bits_)) * (kind == Kind::Group ? 2 : 1);
+            bin_count_.alloc(bins);
             bin_count_.zero();
-            bin_cursor_.alloc((size_t)1 << (3 * grid_bits_));
+            bin_cursor_.alloc(bins);
             bb_ctr_.alloc(RB_);
             bb_ext_.alloc(RB_);
-            const long long cap_tiles = tile_offset(RB_, RB_);
-            tile_cols_.alloc((size_t)cap_tiles * TILE);
+            tile_cols_.alloc((size_t)tile_slots() * TILE);
             rb_ntiles_.alloc(RB_);
             set_chunk(4);
         }
@@ -208,11 +245,17 @@ class NonbondedPotential : public PotentialBase {
         return d;
     }
 
+    // Tile slots of row block rb, and of the whole list.
+    long long tiles_of_row_block(int rb) const { return kind_ == Kind::Group ? RB_ - cb_first_ : RB_ - rb; }
+    long long tile_slots() const {
+        return kind_ == Kind::Group ? (long long)n_row_blocks_ * (RB_ - cb_first_) : tile_offset(RB_, RB_);
+    }
+
     void set_chunk(int chunk) {
         chunk_ = std::max(1, chunk);
         long long cap = 0;
-        for (int rb = 0; rb < RB_; rb++) {
-            cap += ((RB_ - rb) + chunk_ - 1) / chunk_;
+        for (int rb = 0; rb < n_row_blocks_; rb++) {
+            cap += (tiles_of_row_block(rb) + chunk_ - 1) / chunk_;
         }
         items_.alloc((size_t)std::max(1LL, cap));
     }
@@ -247,6 +290,8 @@ class NonbondedPotential : public PotentialBase {
             return "NonbondedAllPairs";
         case Kind::PairList:
             return "NonbondedPairList";
+        case Kind::Group:
+            return "NonbondedInteractionGroup";
         default:
             return "Nonbonded";
         }
@@ -259,6 +304,8 @@ class NonbondedPotential : public PotentialBase {
         padding_ = p;
     }
     void disable_hilbert() { hilbert_ = false; }
+
+    int row_end() const { return kind_ == Kind::Group ? NR_ : S_; }
 
     // Elements of one accumulator block (8 or 11 arrays of S slots).
     size_t acc_block_elems() const { return (size_t)S_ * (split_pair_dp_ ? 11 : 8); }
@@ -274,6 +321,9 @@ class NonbondedPotential : public PotentialBase {
         if (acc_.n < need) {
             acc_.alloc(need);
             acc_.zero();
+        }
+        if (K > 1 && has_nblist_ && dep_tiles_.n == 0) {
+            dep_tiles_.alloc((size_t)std::max(1LL, tile_slots()));
         }
     }
 
@@ -365,6 +415,7 @@ class NonbondedPotential : public PotentialBase {
             sa.x = d_x;
             sa.box = d_box;
             sa.set_atoms = set_atoms_.p;
+            sa.n_first = kind_ == Kind::Group ? NR_ : S_;
             sa.grid_bits = grid_bits_;
             sa.hilbert = hilbert_ ? 1 : 0;
             sa.keys = keys_.p;
@@ -378,6 +429,11 @@ class NonbondedPotential : public PotentialBase {
             TileArgs ta;
             ta.S = S_;
             ta.RB = RB_;
+            ta.group = kind_ == Kind::Group ? 1 : 0;
+            ta.row_end = kind_ == Kind::Group ? NR_ : S_;
+            ta.col_begin = kind_ == Kind::Group ? NR_ : 0;
+            ta.n_row_blocks = n_row_blocks_;
+            ta.cb_first = cb_first_;
             ta.radius = (float)(cutoff_ + padding_ + 1e-5);
             ta.box = d_box;
             ta.posw = posw_.p;
@@ -387,14 +443,26 @@ class NonbondedPotential : public PotentialBase {
             ta.rb_ntiles = rb_ntiles_.p;
             ta.items = items_.p;
             ta.chunk = chunk_;
-            k_build_tiles<<<RB_, TB_WARPS * 32, 0, stream>>>(ta, state_.p);
+            k_build_tiles<<<n_row_blocks_, TB_WARPS * 32, 0, stream>>>(ta, state_.p);
             CK(cudaPeekAtLastError());
         }
 
         const int kidx = (d_du_dp ? 1 : 0) | (d_du_dl ? 2 : 0) | (d_du_dx ? 4 : 0) | (d_u ? 8 : 0);
+        if (kidx != 0 && K > 1 && has_nblist_) {
+            DepArgs da;
+            da.S = S_;
+            da.row_end = row_end();
+            da.items = items_.p;
+            da.tile_cols = tile_cols_.p;
+            da.lamdep = lamdep_.p;
+            da.dep_tiles = dep_tiles_.p;
+            k_dep_tiles<<<4 * num_sms(), 128, 0, stream>>>(da, state_.p);
+            CK(cudaPeekAtLastError());
+        }
         if (kidx != 0) {
             PairArgs a;
             a.S = S_;
+            a.row_end = row_end();
             a.K = K;
             a.lamdep = lamdep_.p;
             a.acc_block = acc_block_elems();
@@ -412,6 +480,7 @@ class NonbondedPotential : public PotentialBase {
             a.slot_of = slot_of_.p;
             a.negated = negated_ ? 1 : 0;
             a.acc = accum();
+            a.dep_tiles = dep_tiles_.p;
             a.state = state_.p;
             pair_kernel_t k = K > 1 ? kernels_multi_[kidx] : kernels_[kidx];
             if (timing_) {
@@ -427,7 +496,9 @@ class NonbondedPotential : public PotentialBase {
             FinalizeArgs fa;
             fa.N = N_;
             fa.S = S_;
-            fa.perm = perm_.p;
+            fa.set_atoms = fin_atoms_.p;
+            fa.slot_of = slot_of_.p;
+            fa.take = 0;
             fa.acc = accum();
             fa.acc_block = acc_block_elems();
             fa.K = K;
@@ -444,8 +515,13 @@ class NonbondedPotential : public PotentialBase {
             fa.du_dl = d_du_dl;
             fa.u = d_u;
             fa.state = state_.p;
-            k_finalize<<<sgrid, tpb, 0, stream>>>(fa);
+            const size_t fin_threads = (size_t)S_ * K;
+            const int fgrid = (int)std::max<size_t>(1, std::min<size_t>((fin_threads + tpb - 1) / tpb, 16 * (size_t)num_sms()));
+            k_finalize<<<fgrid, tpb, 0, stream>>>(fa);
             CK(cudaPeekAtLastError());
+            // zero the accumulator blocks k_finalize read (shared block + windows)
+            CK(cudaMemsetAsync(
+                acc_.p, 0, acc_block_elems() * (K > 1 ? 1 + K : 1) * sizeof(unsigned long long), stream));
         }
     }
 
@@ -525,7 +601,7 @@ class NonbondedPotential : public PotentialBase {
             *RB = RB_;
         }
         if (tile_capacity) {
-            *tile_capacity = has_nblist_ ? tile_offset(RB_, RB_) : 0;
+            *tile_capacity = has_nblist_ ? tile_slots() : 0;
         }
     }
 
@@ -568,13 +644,16 @@ class NonbondedPotential : public PotentialBase {
     bool split_pair_dp_ = false;
     int M_;
     int RB_ = 0;
+    int NR_ = 0;           // interaction group: row atoms
+    int n_row_blocks_ = 0; // blocks whose slots act as rows
+    int cb_first_ = 0;     // interaction group: first column block
     int grid_bits_ = 4;
     int chunk_ = 4;
 
     std::vector<int> h_plane_, h_offset_, h_atom_idxs_, h_pairs_;
     std::vector<double> h_scales_;
 
-    DevBuf<int> plane_, offset_, set_atoms_, pair_idxs_, slot_of_;
+    DevBuf<int> plane_, offset_, set_atoms_, pair_idxs_, slot_of_, fin_atoms_;
     DevBuf<double> scales_;
     DevBuf<unsigned> perm_;
     DevBuf<float4> posw_, prm_, dprm_;
@@ -587,6 +666,7 @@ class NonbondedPotential : public PotentialBase {
     DevBuf<unsigned> tile_cols_;
     DevBuf<int> rb_ntiles_;
     DevBuf<int4> items_;
+    DevBuf<int2> dep_tiles_;
     DevBuf<DevState> state_;
     pair_kernel_t kernels_[16];
     pair_kernel_t kernels_multi_[16];
@@ -715,6 +795,44 @@ tmnb_status tmnb_all_pairs_create(
             cutoff,
             atom_idxs,
             K,
+            nullptr,
+            nullptr,
+            0,
+            false,
+            interpolated != 0);
+        *out = h.release();
+    });
+}
+
+tmnb_status tmnb_interaction_group_create(
+    int N,
+    const int32_t *row_atom_idxs,
+    int NR,
+    const int32_t *lambda_plane_idxs,
+    const int32_t *lambda_offset_idxs,
+    double beta,
+    double cutoff,
+    int interpolated,
+    int precision,
+    tmnb_potential **out) {
+    if (tmnb_status s = check_precision(precision)) {
+        return s;
+    }
+    if (!out || !lambda_plane_idxs || !lambda_offset_idxs || NR < 0 || (NR > 0 && !row_atom_idxs)) {
+        tmb::g_last_error = "null argument";
+        return TMNB_ERR_INVALID_ARGUMENT;
+    }
+    return tmb::guarded([&] {
+        auto h = std::make_unique<tmnb_potential>();
+        h->impl = std::make_unique<tmb::NonbondedPotential>(
+            tmb::Kind::Group,
+            N,
+            lambda_plane_idxs,
+            lambda_offset_idxs,
+            beta,
+            cutoff,
+            row_atom_idxs,
+            NR,
             nullptr,
             nullptr,
             0,

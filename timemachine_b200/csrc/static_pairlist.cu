@@ -211,6 +211,7 @@ void execute_static(
     if (kidx != 0) {
         PairArgs a;
         a.S = N;
+        a.row_end = N;
         a.K = 1;
         a.posw = posw;
         a.prm = prm;
@@ -228,6 +229,7 @@ void execute_static(
         a.negated = negated ? 1 : 0;
         a.acc = c;
         a.acc_block = 8 * (size_t)SMAX;
+        a.dep_tiles = nullptr;
         a.state = state;
         g_kernels[kidx]<<<d.pair_grid[kidx], 128, 0, stream>>>(a);
         CK(cudaPeekAtLastError());
@@ -239,7 +241,9 @@ void execute_static(
         for (int k = 0; k < MAX_WINDOWS; k++) {
             fa.lambdas[k] = pa.lambdas[k];
         }
-        fa.perm = perm;
+        fa.set_atoms = nullptr;
+        fa.slot_of = nullptr;
+        fa.take = 1;
         fa.acc = c;
         fa.acc_block = 8 * (size_t)SMAX;
         fa.split_pair_dp = 0;

@@ -26,6 +26,8 @@ __all__ = [
     "NonbondedInterpolated",
     "NonbondedAllPairs",
     "NonbondedAllPairsInterpolated",
+    "NonbondedInteractionGroup",
+    "NonbondedInteractionGroupInterpolated",
     "NonbondedPairList",
     "NonbondedPairListNegated",
     "NonbondedPairListInterpolated",
@@ -335,7 +337,8 @@ class Potential:
 
     def get_nblist(self, stream=None):
         """(perm [S] slot -> atom, tiles) of the last rebuild; tiles[rb] is an
-        array of the atom indices interacting with row block rb (slots rb*32..)."""
+        array of the column SLOTS (map them to atoms through perm) listed for
+        row block rb, whose rows are slots rb*32 .. rb*32+31."""
         S, RB, cap = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_longlong()
         _lib.check(self._lib.tmnb_potential_nblist_shape(self._h, ctypes.byref(S), ctypes.byref(RB), ctypes.byref(cap)))
         perm = np.zeros(S.value, dtype=np.uint32)
@@ -346,9 +349,12 @@ class Potential:
             s = stream.cuda_stream if hasattr(stream, "cuda_stream") else stream
         _lib.check(self._lib.tmnb_potential_copy_nblist(self._h, ctypes.c_void_p(s), _ptr(perm), _ptr(nt), _ptr(cols)))
         R = RB.value
+        nr = getattr(self, "_group_rows", None)
         tiles = []
-        for rb in range(R):
-            off = rb * R - (rb * (rb - 1)) // 2
+        for rb in range(R if nr is None else (nr + 31) // 32):
+            # row block rb's first tile: upper triangle, or (interaction group)
+            # R - nr//32 tiles per row block
+            off = rb * R - (rb * (rb - 1)) // 2 if nr is None else rb * (R - nr // 32)
             c = cols[off * 32 : (off + nt[rb]) * 32]
             tiles.append(c[c < S.value])
         return perm, tiles
@@ -470,6 +476,44 @@ class NonbondedAllPairs(CustomOpWrapper):
 
 
 class NonbondedAllPairsInterpolated(NonbondedAllPairs):
+    _interpolated = True
+
+
+class NonbondedInteractionGroup(CustomOpWrapper):
+    """timemachine/lib/potentials.py:389-399: pairs of one row atom and one
+    other atom. args: (row_atom_idxs, lambda_plane_idxs, lambda_offset_idxs, beta, cutoff)."""
+
+    _interpolated = False
+
+    def unbound_impl(self, precision):
+        _check_precision(precision)
+        rows = np.ascontiguousarray(self.args[0], dtype=np.int32).reshape(-1)
+        if len(set(rows.tolist())) != rows.size:
+            # the binding's unique_idxs (timemachine/cpp/src/wrap_kernels.cpp:922)
+            raise RuntimeError("atom indices must be unique")
+        plane, offset = _plane_offset(self.args[1], self.args[2])
+        h = ctypes.c_void_p()
+        lib = _lib.lib()
+        _lib.check(
+            lib.tmnb_interaction_group_create(
+                plane.size,
+                _ptr(rows) if rows.size else None,
+                rows.size,
+                _ptr(plane),
+                _ptr(offset),
+                float(self.args[3]),
+                float(self.args[4]),
+                1 if self._interpolated else 0,
+                32,
+                ctypes.byref(h),
+            )
+        )
+        pot = Potential(h, "NonbondedInteractionGroup", self._interpolated)
+        pot._group_rows = rows.size
+        return pot
+
+
+class NonbondedInteractionGroupInterpolated(NonbondedInteractionGroup):
     _interpolated = True
 
 
