@@ -69,6 +69,12 @@ def parse():
         choices=["windows", "single"],
         help="windows: one 12-window call per step; single: one single-window call per step (cycling lambdas)",
     )
+    ap.add_argument(
+        "--forms",
+        default="batch,serve",
+        help="comma-separated extra forms measured after the plain path: batch (512 replicas), serve (request "
+        "loop); '' for none",
+    )
     return ap.parse_args()
 
 
@@ -426,6 +432,17 @@ def run_tmnb(args, world, rank, local):
         result["ns_per_day"] = result["md"]["ns_per_day"]
     except Exception as e:  # report, do not hide the evaluation numbers
         result["md"] = {"error": str(e)[:300]}
+    forms = [f for f in args.forms.split(",") if f]
+    if "batch" in forms:
+        try:
+            result["batch"] = run_batch_form()
+        except Exception as e:
+            result["batch"] = {"error": str(e)[:300]}
+    if "serve" in forms:
+        try:
+            result["serve"] = run_serve_form()
+        except Exception as e:
+            result["serve"] = {"error": str(e)[:300]}
     clk.__exit__()
     result["clocks"] = clk.summary()
     return result
@@ -526,6 +543,203 @@ def run_md_reference(steps=MD_STEPS):
         "steps": steps,
         "finite": bool(np.all(np.isfinite(xf))),
         "timing": "wall clock around Context.multiple_steps",
+    }
+
+
+BATCH_SYSTEMS = 64
+BATCH_WINDOWS = 8
+BATCH_CHUNK = 500
+BATCH_MD = dict(temperature=300.0, dt=1.5e-3, friction=1.0)
+
+
+def batch_workload(seed=SEED):
+    """64 water + ligand systems, sizes log-uniform on [1,500, 30,000] atoms at
+    1 g/cm^3, ligands of 20-60 atoms; 8 lambda windows each (512 replicas)."""
+    from timemachine_b200 import testsystems
+
+    rng = np.random.default_rng(seed)
+    sizes = np.exp(rng.uniform(np.log(1500), np.log(30000), BATCH_SYSTEMS)).astype(int)
+    systems = [testsystems.system_of_size(int(n), seed=seed + 17 * k) for k, n in enumerate(sizes)]
+    return systems, np.linspace(0.0, 1.0, BATCH_WINDOWS)
+
+
+def _mb_velocities(rng, s, temperature):
+    return rng.normal(size=(s.N, 3)) * np.sqrt(0.008314462618 * temperature / s.masses)[:, None]
+
+
+def run_batch_form():
+    """Batching form: 512 replicas (64 systems x 8 windows) through one launch
+    sequence per step, against 512 sequential plain calls (one Nonbonded +
+    HarmonicBond + HarmonicAngle execute_device per replica), and one
+    CUDA-graph-captured 500-step MD chunk of all replicas."""
+    import torch
+
+    from timemachine_b200 import potentials as P
+    from timemachine_b200.batch import ReplicaBatch
+
+    systems, lambdas = batch_workload()
+    n_rep = len(systems) * len(lambdas)
+    atoms = int(sum(s.N for s in systems) * len(lambdas))
+    b = ReplicaBatch()
+    rng = np.random.default_rng(SEED + 5)
+    for k, s in enumerate(systems):
+        for w, lam in enumerate(lambdas):
+            b.add(s, lam, v=_mb_velocities(rng, s, BATCH_MD["temperature"]), md=BATCH_MD, seed=1000 * k + w)
+    stream = torch.cuda.ExternalStream(b.stream)
+
+    def timed(fn, reps):
+        fn()  # warm-up (rebuilds, graph capture)
+        b.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        e1.synchronize()
+        return e0.elapsed_time(e1) / 1e3
+
+    tune_best, tune_table = b.autotune(
+        mode="eval",
+        steps=2,
+        repeats=1,
+        candidates=[dict(chunk=c, padding=p, grid_bits_offset=0, pair_ctas_per_sm=0) for c in (2, 4, 8) for p in (0.06, 0.1)],
+    )
+    t_eval = timed(lambda: b.evaluate(), 3)
+    batch_evals = 3 * n_rep / t_eval
+
+    # 512 sequential plain calls, device-resident inputs, CUDA events on the torch stream
+    cur = torch.cuda.current_stream()
+    plain = []
+    for s in systems:
+        pots = [
+            (P.Nonbonded(s.exclusion_idxs, s.scales, s.lambda_plane_idxs, s.lambda_offset_idxs, s.beta, s.cutoff)
+             .unbound_impl(np.float32), s.params),
+            (P.HarmonicBond(s.bond_idxs).unbound_impl(np.float32), s.bond_params),
+            (P.HarmonicAngle(s.angle_idxs).unbound_impl(np.float32), s.angle_params),
+        ]
+        dev = [(impl, torch.as_tensor(np.ascontiguousarray(p), device="cuda").reshape(-1)) for impl, p in pots]
+        dx = torch.as_tensor(s.x, device="cuda")
+        db = torch.as_tensor(s.box, device="cuda")
+        outs = [torch.zeros(sh, dtype=torch.int64, device="cuda") for sh in [(s.N, 3), (s.N * 3,), (s.N,), (s.N,)]]
+        plain.append((dev, dx, db, outs))
+
+    def plain_pass():
+        for dev, dx, db, outs in plain:
+            for lam in lambdas:
+                for o in outs:
+                    o.zero_()
+                nb_impl, nb_p = dev[0]
+                nb_impl.execute_device(dx, nb_p, db, float(lam), *outs, stream=cur)
+                for impl, p in dev[1:]:
+                    impl.execute_device(dx, p, db, float(lam), outs[0], None, None, outs[3], stream=cur)
+
+    plain_pass()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(cur)
+    plain_pass()
+    e1.record(cur)
+    e1.synchronize()
+    t_plain = e0.elapsed_time(e1) / 1e3
+    plain_evals = n_rep / t_plain
+    del plain
+
+    t_md = timed(lambda: b.md(BATCH_CHUNK, chunk=BATCH_CHUNK, use_graph=True), 1)
+    md_replica_steps = n_rep * BATCH_CHUNK / t_md
+    sample = b.ids()[:: max(1, n_rep // 16)]
+    finite = all(np.all(np.isfinite(b.get_x(r))) for r in sample)
+    return {
+        "workload": f"{len(systems)} water+ligand systems of {min(s.N for s in systems)}-{max(s.N for s in systems)} "
+        f"atoms (log-uniform on [1500, 30000]) x {len(lambdas)} lambda windows = {n_rep} replicas, "
+        f"{atoms} replica-atoms; nonbonded + harmonic bonds/angles",
+        "evals_per_s": batch_evals,
+        "plain_sequential_evals_per_s": plain_evals,
+        "speedup_vs_plain": batch_evals / plain_evals,
+        "eval_ms": t_eval / 3 * 1e3,
+        "plain_ms": t_plain * 1e3,
+        "md": {
+            "replica_steps_per_s": md_replica_steps,
+            "speedup_vs_plain_evals": md_replica_steps / plain_evals,
+            "chunk_steps": BATCH_CHUNK,
+            "chunk_ms": t_md * 1e3,
+            "dt_ps": BATCH_MD["dt"],
+            "aggregate_ns_per_day": md_replica_steps * BATCH_MD["dt"] * 86400 / 1000,
+            "finite": bool(finite),
+            "timing": "CUDA events on the batch stream around one graph-replayed 500-step chunk",
+        },
+        "autotune": {"best": tune_best, "candidates": [[c, t] for c, t in tune_table]},
+        "timing": "CUDA events (batch stream / torch stream), inputs resident on the device",
+        "device_bytes": b.bytes_in_use(),
+    }
+
+
+SERVE_RATE = 200.0  # requests/s
+SERVE_SECONDS = 3.0  # arrival window of the bounded sample
+SERVE_MD_STEPS = 1000
+
+
+def serve_workload(seed=SEED + 11, seconds=SERVE_SECONDS):
+    """Poisson arrivals at 200/s; 70 % single evaluations, 30 % 1,000-step
+    Langevin segments; sizes log-uniform on [500, 50,000] atoms; lambda U(0, 1)."""
+    from timemachine_b200 import testsystems
+    from timemachine_b200.serve import Request
+
+    rng = np.random.default_rng(seed)
+    t, reqs = 0.0, []
+    while True:
+        t += rng.exponential(1.0 / SERVE_RATE)
+        if t > seconds:
+            break
+        n = int(np.exp(rng.uniform(np.log(500), np.log(50000))))
+        s = testsystems.system_of_size(n, seed=int(rng.integers(1 << 30)))
+        kind = "md" if rng.uniform() < 0.3 else "eval"
+        reqs.append(
+            Request(
+                rid=len(reqs), system=s, lam=float(rng.uniform()), kind=kind, arrival=t,
+                n_steps=SERVE_MD_STEPS if kind == "md" else 0,
+                v0=_mb_velocities(rng, s, BATCH_MD["temperature"]) if kind == "md" else None,
+                seed=int(rng.integers(1 << 30)), md=BATCH_MD,
+            )
+        )
+    return reqs
+
+
+def run_serve_form():
+    """Serving form: the request stream through the continuous-batching loop,
+    and the same stream through sequential plain calls on the same GPU."""
+    from timemachine_b200.serve import Server, latency_stats, run_sequential
+
+    import dataclasses
+
+    reqs = serve_workload()
+    fresh = [dataclasses.replace(r) for r in reqs]  # same stream, unserved, for the sequential run
+    server = Server(hbm_budget_bytes=150e9, md_chunk=50)
+    t0 = time.perf_counter()
+    done = server.run(reqs)
+    wall = time.perf_counter() - t0
+    stats = latency_stats(done)
+    evals = [r for r in done if r.kind == "eval"]
+    mds = [r for r in done if r.kind == "md"]
+    seq = run_sequential(fresh)
+    seq_wall = max(r.finished for r in seq) - min(r.arrival for r in seq)
+    seq_stats = latency_stats(seq)
+    return {
+        "workload": f"{len(reqs)} requests over {SERVE_SECONDS:.0f} s of Poisson arrivals at {SERVE_RATE:.0f}/s "
+        f"({len(evals)} evaluations, {len(mds)} x {SERVE_MD_STEPS}-step MD segments), sizes log-uniform on "
+        "[500, 50000] atoms, lambda U(0,1), 150 GB HBM budget",
+        "latency": stats,
+        "latency_eval": latency_stats(evals) if evals else None,
+        "latency_md": latency_stats(mds) if mds else None,
+        "throughput_requests_per_s": len(done) / wall,
+        "wall_s": wall,
+        "iterations": server.iterations,
+        "peak_device_bytes": server.peak_bytes,
+        "sequential_plain": {
+            "latency": seq_stats,
+            "throughput_requests_per_s": len(seq) / seq_wall,
+            "wall_s": seq_wall,
+        },
+        "timing": "host wall clock from each request's arrival to its result on the host (D2H included)",
     }
 
 

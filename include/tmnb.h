@@ -386,6 +386,89 @@ tmnb_status tmnb_harmonic_angle_create(
 int tmnb_potential_num_params(const tmnb_potential *pot);
 int tmnb_potential_num_atoms(const tmnb_potential *pot);
 
+/*
+ * Replica batch (no single reference counterpart: it replaces the loops in
+ * which the reference evaluates or simulates replicas one at a time, one
+ * Potential::execute_device / one Context per replica and lambda). Holds any
+ * number of independent systems, each at its own lambda, with its nonbonded
+ * potential (all pairs minus the scaled exclusions), harmonic bonds and
+ * angles; one launch sequence per step serves every replica. Each replica's
+ * outputs equal a single-system evaluation of the same inputs bit for bit,
+ * whatever else is in the batch. Replicas can be added and removed between
+ * calls (each owns one device arena; tmnb_batch_footprint gives its size).
+ */
+typedef struct tmnb_batch tmnb_batch;
+
+tmnb_status tmnb_batch_create(tmnb_batch **out);
+tmnb_status tmnb_batch_destroy(tmnb_batch *b);
+
+/* Adds one replica (host arrays, copied). v, cbs, ccs may be NULL (no MD;
+ * v = 0). ca, cbs, ccs, dt: Langevin coefficients as in tmnb_context_create.
+ * id receives the replica's handle within the batch. */
+tmnb_status tmnb_batch_add(
+    tmnb_batch *b,
+    int N,
+    const double *x,      /* [N,3] */
+    const double *v,      /* [N,3] or NULL */
+    const double *box,    /* [3,3] */
+    const double *params, /* [N,3] */
+    const int32_t *lambda_plane_idxs,
+    const int32_t *lambda_offset_idxs,
+    int M,
+    const int32_t *exclusion_idxs, /* [M,2] */
+    const double *scales,          /* [M,2] */
+    int B,
+    const int32_t *bond_idxs, /* [B,2] */
+    const double *bond_params,
+    int A,
+    const int32_t *angle_idxs, /* [A,3] */
+    const double *angle_params,
+    double beta,
+    double cutoff,
+    double lambda,
+    double dt,
+    double ca,
+    const double *cbs, /* [N] or NULL */
+    const double *ccs, /* [N] or NULL */
+    unsigned long long seed,
+    int *id);
+
+tmnb_status tmnb_batch_remove(tmnb_batch *b, int id);
+
+/* Device bytes a replica of N atoms, M exclusions, B bonds, A angles holds
+ * (admission control by HBM footprint), and the bytes all replicas hold. */
+tmnb_status tmnb_batch_footprint(tmnb_batch *b, int N, int M, int B, int A, unsigned long long *bytes);
+tmnb_status tmnb_batch_bytes_in_use(tmnb_batch *b, unsigned long long *bytes);
+
+/* Schedule of the tile work: tiles per work item, neighbour-list padding (nm),
+ * Hilbert grid resolution offset (-2..2), pair-kernel CTAs per SM (0: by
+ * occupancy). Applies to every replica (re-laid out, list rebuilt). */
+tmnb_status tmnb_batch_set_tuning(tmnb_batch *b, int chunk, double padding, int grid_bits_offset, int pair_ctas_per_sm);
+
+/* One evaluation of every replica (outputs overwritten; read them with
+ * tmnb_batch_get). Asynchronous on the batch's stream. */
+tmnb_status tmnb_batch_evaluate(tmnb_batch *b, int compute_du_dx, int compute_du_dp, int compute_du_dl, int compute_u);
+
+/* n_steps Langevin steps of every replica; use_graph != 0 replays a CUDA
+ * graph of `chunk` steps. Asynchronous on the batch's stream. */
+tmnb_status tmnb_batch_md(tmnb_batch *b, int n_steps, int chunk, int use_graph);
+
+tmnb_status tmnb_batch_synchronize(tmnb_batch *b);
+
+/* Copies (synchronising) replica id's x [N,3] (which 0), v (1), box (2) as
+ * doubles, or its outputs du_dx [N,3] (3), du_dp [N,3] (4), per-atom du_dl
+ * [N] (5), per-atom u [N] (6) as int64 fixed point. */
+tmnb_status tmnb_batch_get(tmnb_batch *b, int id, int which, void *out);
+/* Overwrites replica id's x (0), v (1) or box (2). */
+tmnb_status tmnb_batch_set(tmnb_batch *b, int id, int which, const double *in);
+/* Sticky device error of replica id (TMNB_ERR_* value, 0 = none), cleared. */
+tmnb_status tmnb_batch_error(tmnb_batch *b, int id, int *code);
+tmnb_status tmnb_batch_stats(tmnb_batch *b, int id, int *tiles, int *items, int *rebuilds);
+/* The batch's CUDA stream (every batch call is ordered on it), e.g. to record
+ * events around tmnb_batch_evaluate / tmnb_batch_md. */
+tmnb_status tmnb_batch_stream(tmnb_batch *b, void **stream);
+int tmnb_batch_size(const tmnb_batch *b);
+
 /* Largest N accepted by tmnb_pair_list_execute_static (3.16 MiB of static
  * device scratch). */
 #define TMNB_STATIC_MAX_ATOMS 32768

@@ -25,7 +25,7 @@ NVCC_FLAGS = [
     "-shared",
 ]
 
-SOURCES = ["nonbonded.cu", "md.cu", "bonded.cu", "static_pairlist.cu"]
+SOURCES = ["nonbonded.cu", "md.cu", "bonded.cu", "batch.cu", "static_pairlist.cu"]
 
 
 def build(verbose: bool = False) -> str:
@@ -95,6 +95,25 @@ def _declare(lib):
     lib.tmnb_harmonic_angle_create.argtypes = [i, i, vp, vp, vp, ctypes.POINTER(vp)]
     lib.tmnb_pair_list_execute_static.argtypes = [i, i, vp, vp, vp, vp, d, d, i, vp, vp, vp, d, vp, vp, vp, vp, vp]
     lib.tmnb_pair_list_execute_static.restype = ctypes.c_int
+    ull = ctypes.c_ulonglong
+    lib.tmnb_batch_create.argtypes = [ctypes.POINTER(vp)]
+    lib.tmnb_batch_destroy.argtypes = [vp]
+    lib.tmnb_batch_add.argtypes = [vp, i, vp, vp, vp, vp, vp, vp, i, vp, vp, i, vp, vp, i, vp, vp, d, d, d, d, d, vp, vp,
+                                   ull, c_int_p]
+    lib.tmnb_batch_remove.argtypes = [vp, i]
+    lib.tmnb_batch_footprint.argtypes = [vp, i, i, i, i, ctypes.POINTER(ull)]
+    lib.tmnb_batch_bytes_in_use.argtypes = [vp, ctypes.POINTER(ull)]
+    lib.tmnb_batch_set_tuning.argtypes = [vp, i, d, i, i]
+    lib.tmnb_batch_evaluate.argtypes = [vp, i, i, i, i]
+    lib.tmnb_batch_md.argtypes = [vp, i, i, i]
+    lib.tmnb_batch_synchronize.argtypes = [vp]
+    lib.tmnb_batch_get.argtypes = [vp, i, i, vp]
+    lib.tmnb_batch_set.argtypes = [vp, i, i, vp]
+    lib.tmnb_batch_error.argtypes = [vp, i, c_int_p]
+    lib.tmnb_batch_stats.argtypes = [vp, i, c_int_p, c_int_p, c_int_p]
+    lib.tmnb_batch_stream.argtypes = [vp, ctypes.POINTER(vp)]
+    lib.tmnb_batch_size.argtypes = [vp]
+    lib.tmnb_batch_size.restype = ctypes.c_int
     lib.tmnb_potential_num_params.argtypes = [vp]
     lib.tmnb_potential_num_atoms.argtypes = [vp]
     for name in [

@@ -7,6 +7,7 @@
 // each scaled by (lambda_offset + lambda_mult * lambda); params [T, 2] = (k, r0 | a0).
 // No periodic wrapping (molecules are kept whole), as in the reference.
 #include "engine.hpp"
+#include "bonded_math.cuh"
 #include "nb_pair_math.cuh"
 
 #include <algorithm>
@@ -33,35 +34,9 @@ __global__ void k_harmonic_bond(
     if (b >= B) {
         return;
     }
-    const int i = idxs[2 * b], j = idxs[2 * b + 1];
-    Real dx[3];
-    Real d2 = 0;
-    for (int d = 0; d < 3; d++) {
-        dx[d] = (Real)x[3 * i + d] - (Real)x[3 * j + d];
-        d2 += dx[d] * dx[d];
-    }
-    const Real kb = params[2 * b], b0 = params[2 * b + 1];
-    const Real dij = sqrt(d2);
-    const Real db = dij - b0;
-    const Real pre = loff[b] + lmult[b] * (Real)lambda;
-    if (du_dx) {
-        for (int d = 0; d < 3; d++) {
-            const Real g = (b0 != 0 ? kb * db * dx[d] / dij : kb * dx[d]) * pre;
-            const unsigned long long f = to_fixed(g, FX_EXPONENT);
-            atomicAdd(du_dx + 3 * i + d, f);
-            atomicAdd(du_dx + 3 * j + d, 0ULL - f);
-        }
-    }
-    if (du_dp) {
-        atomicAdd(du_dp + 2 * b, to_fixed((Real)0.5 * db * db * pre, FX_EXPONENT));
-        atomicAdd(du_dp + 2 * b + 1, to_fixed(-kb * db * pre, FX_EXPONENT));
-    }
-    if (u) {
-        atomicAdd(u + i, to_fixed(kb / 2 * db * db * pre, FX_EXPONENT));
-    }
-    if (du_dl) {
-        atomicAdd(du_dl + i, to_fixed(lmult[b] * kb / 2 * db * db, FX_EXPONENT));
-    }
+    harmonic_bond_term(
+        x, idxs[2 * b], idxs[2 * b + 1], params[2 * b], params[2 * b + 1], lmult[b], loff[b], lambda, du_dx,
+        du_dp ? du_dp + 2 * b : nullptr, du_dl, u);
 }
 
 template <typename Real>
@@ -81,44 +56,9 @@ __global__ void k_harmonic_angle(
     if (a >= A) {
         return;
     }
-    const int i = idxs[3 * a], j = idxs[3 * a + 1], k = idxs[3 * a + 2];
-    Real rij[3], rkj[3];
-    Real nij2 = 0, nkj2 = 0, dot = 0;
-    for (int d = 0; d < 3; d++) {
-        rij[d] = (Real)x[3 * i + d] - (Real)x[3 * j + d]; // j -> i
-        rkj[d] = (Real)x[3 * k + d] - (Real)x[3 * j + d]; // j -> k
-        nij2 += rij[d] * rij[d];
-        nkj2 += rkj[d] * rkj[d];
-        dot += rij[d] * rkj[d];
-    }
-    const Real inij = (Real)1 / sqrt(nij2), inkj = (Real)1 / sqrt(nkj2);
-    const Real cos_t = dot * inij * inkj;
-    const Real ka = params[2 * a], a0 = params[2 * a + 1];
-    const Real delta = cos_t - cos(a0);
-    const Real pre = loff[a] + lmult[a] * (Real)lambda;
-    if (du_dx) {
-        const Real f = ka * delta * pre;
-        for (int d = 0; d < 3; d++) {
-            // d cos / d x_i and d x_k; x_j takes the negated sum
-            const Real gi = (rkj[d] * inij * inkj - cos_t * rij[d] * inij * inij) * f;
-            const Real gk = (rij[d] * inij * inkj - cos_t * rkj[d] * inkj * inkj) * f;
-            const unsigned long long fi = to_fixed(gi, FX_EXPONENT);
-            const unsigned long long fk = to_fixed(gk, FX_EXPONENT);
-            atomicAdd(du_dx + 3 * i + d, fi);
-            atomicAdd(du_dx + 3 * k + d, fk);
-            atomicAdd(du_dx + 3 * j + d, 0ULL - fi - fk);
-        }
-    }
-    if (du_dp) {
-        atomicAdd(du_dp + 2 * a, to_fixed(delta * delta / 2 * pre, FX_EXPONENT));
-        atomicAdd(du_dp + 2 * a + 1, to_fixed(delta * ka * sin(a0) * pre, FX_EXPONENT));
-    }
-    if (u) {
-        atomicAdd(u + i, to_fixed(ka / 2 * delta * delta * pre, FX_EXPONENT));
-    }
-    if (du_dl) {
-        atomicAdd(du_dl + i, to_fixed(lmult[a] * ka / 2 * delta * delta, FX_EXPONENT));
-    }
+    harmonic_angle_term(
+        x, idxs[3 * a], idxs[3 * a + 1], idxs[3 * a + 2], params[2 * a], params[2 * a + 1], lmult[a], loff[a], lambda,
+        du_dx, du_dp ? du_dp + 2 * a : nullptr, du_dl, u);
 }
 
 } // namespace

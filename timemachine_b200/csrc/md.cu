@@ -14,6 +14,7 @@
 // the integrator kernel, keyed by (seed, step, atom), so a step has no RNG
 // launch and a replayed graph draws fresh numbers.
 #include "engine.hpp"
+#include "md_math.cuh"
 #include "nb_pair_math.cuh"
 
 #include <algorithm>
@@ -26,35 +27,6 @@ namespace {
 
 constexpr double BOLTZ = 0.008314462618; // kJ/mol/K
 constexpr double AVOGADRO = 6.0221367e23;
-
-__device__ __forceinline__ uint4 philox4x32_10(uint4 c, uint2 k) {
-    const unsigned M0 = 0xD2511F53u, M1 = 0xCD9E8D57u, W0 = 0x9E3779B9u, W1 = 0xBB67AE85u;
-#pragma unroll
-    for (int r = 0; r < 10; r++) {
-        const unsigned hi0 = __umulhi(M0, c.x), lo0 = M0 * c.x;
-        const unsigned hi1 = __umulhi(M1, c.z), lo1 = M1 * c.z;
-        c = make_uint4(hi1 ^ c.y ^ k.x, lo1, hi0 ^ c.w ^ k.y, lo0);
-        k.x += W0;
-        k.y += W1;
-    }
-    return c;
-}
-
-// uniform double in (0, 1) from 53 random bits
-__device__ __forceinline__ double u01(unsigned a, unsigned b) {
-    const unsigned long long m = ((unsigned long long)(a >> 5) << 26) | (b >> 6);
-    return ((double)m + 0.5) * (1.0 / 9007199254740992.0);
-}
-
-// two standard normals (Box-Muller)
-__device__ __forceinline__ double2 normal2(unsigned a, unsigned b, unsigned c, unsigned d) {
-    const double u1 = u01(a, b);
-    const double u2 = u01(c, d);
-    const double r = sqrt(-2.0 * log(u1));
-    double s, co;
-    sincospi(2.0 * u2, &s, &co);
-    return make_double2(r * co, r * s);
-}
 
 struct MDState {
     unsigned long long step;  // integrator step counter (RNG counter)
@@ -91,23 +63,7 @@ __global__ void k_langevin(
     __syncthreads();
     const int i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i < N) {
-        const uint4 r0 = philox4x32_10(make_uint4((unsigned)i, (unsigned)s_step, (unsigned)(s_step >> 32), 0u), key);
-        const uint4 r1 = philox4x32_10(make_uint4((unsigned)i, (unsigned)s_step, (unsigned)(s_step >> 32), 1u), key);
-        const double2 n01 = normal2(r0.x, r0.y, r0.z, r0.w);
-        const double2 n23 = normal2(r1.x, r1.y, r1.z, r1.w);
-        const double noise[3] = {n01.x, n01.y, n23.x};
-        const double cb = cbs[i];
-        const double cc = ccs[i];
-#pragma unroll
-        for (int d = 0; d < 3; d++) {
-            const int k = 3 * i + d;
-            const double force = static_cast<double>(static_cast<long long>(du_dx[k])) / FX_EXPONENT;
-            const double v_mid = v[k] + cb * force;
-            const double v_new = ca * v_mid + cc * noise[d];
-            v[k] = v_new;
-            x[k] += 0.5 * dt * (v_mid + v_new);
-            du_dx[k] = 0; // the next step accumulates from zero
-        }
+        langevin_atom(i, s_step, key, ca, cbs[i], ccs[i], dt, x, v, du_dx);
     }
     __syncthreads();
     if (threadIdx.x == 0) {

@@ -227,12 +227,9 @@ struct SortArgs {
 
 __device__ __forceinline__ int set_atom(const SortArgs &a, int k) { return a.set_atoms ? a.set_atoms[k] : k; }
 
-static __global__ void k_bin_keys(SortArgs a, const DevState *state) {
-    if (!state->rebuild || state->error || !a.hilbert) {
-        return;
-    }
+__device__ __forceinline__ void bin_key(const SortArgs &a, int k) {
     const int G = 1 << a.grid_bits;
-    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < a.S; k += gridDim.x * blockDim.x) {
+    {
         const int atom = set_atom(a, k);
         unsigned c[3];
         for (int d = 0; d < 3; d++) {
@@ -252,12 +249,18 @@ static __global__ void k_bin_keys(SortArgs a, const DevState *state) {
     }
 }
 
-// Single-CTA exclusive scan of the cell counts (and reset of the counts and
-// of the tile-build counters).
-static __global__ void k_bin_scan(SortArgs a, DevState *state) {
-    if (!state->rebuild || state->error) {
+static __global__ void k_bin_keys(SortArgs a, const DevState *state) {
+    if (!state->rebuild || state->error || !a.hilbert) {
         return;
     }
+    for (int k = blockIdx.x * blockDim.x + threadIdx.x; k < a.S; k += gridDim.x * blockDim.x) {
+        bin_key(a, k);
+    }
+}
+
+// Single-CTA exclusive scan of the cell counts (and reset of the counts and
+// of the tile-build counters).
+__device__ __forceinline__ void bin_scan_cta(const SortArgs &a, DevState *state) {
     if (threadIdx.x == 0) {
         state->done_ctas = 0;
         state->total_tiles = 0;
@@ -315,6 +318,29 @@ static __global__ void k_bin_scan(SortArgs a, DevState *state) {
     }
 }
 
+static __global__ void k_bin_scan(SortArgs a, DevState *state) {
+    if (!state->rebuild || state->error) {
+        return;
+    }
+    bin_scan_cta(a, state);
+}
+
+// Slot of set entry k after the counting sort; records the slot order and the
+// coordinates of the rebuild.
+__device__ __forceinline__ int scatter_slot(
+    const SortArgs &sa, int k, unsigned *__restrict__ perm, int *__restrict__ slot_of, double *__restrict__ nb_x) {
+    const int atom = set_atom(sa, k);
+    const int s = sa.hilbert ? atomicAdd(&sa.bin_cursor[sa.keys[k]], 1) : k;
+    perm[s] = (unsigned)atom;
+    if (slot_of) {
+        slot_of[atom] = s;
+    }
+    nb_x[3 * (size_t)atom + 0] = sa.x[3 * (size_t)atom + 0];
+    nb_x[3 * (size_t)atom + 1] = sa.x[3 * (size_t)atom + 1];
+    nb_x[3 * (size_t)atom + 2] = sa.x[3 * (size_t)atom + 2];
+    return s;
+}
+
 static __global__ void k_bin_scatter(
     SortArgs sa,
     PrepareArgs pa,
@@ -332,14 +358,7 @@ static __global__ void k_bin_scatter(
     }
     for (int k = tid; k < sa.S; k += gridDim.x * blockDim.x) {
         const int atom = set_atom(sa, k);
-        const int s = sa.hilbert ? atomicAdd(&sa.bin_cursor[sa.keys[k]], 1) : k;
-        perm[s] = (unsigned)atom;
-        if (slot_of) {
-            slot_of[atom] = s;
-        }
-        nb_x[3 * (size_t)atom + 0] = sa.x[3 * (size_t)atom + 0];
-        nb_x[3 * (size_t)atom + 1] = sa.x[3 * (size_t)atom + 1];
-        nb_x[3 * (size_t)atom + 2] = sa.x[3 * (size_t)atom + 2];
+        const int s = scatter_slot(sa, k, perm, slot_of, nb_x);
         prepare_slot(pa, s, atom);
     }
 }
@@ -350,21 +369,18 @@ static __global__ void k_bin_scatter(
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ float wrap_delta(float d, float L, float inv_L) { return d - L * rintf(d * inv_L); }
 
-static __global__ void k_block_bounds(
+// Bounding box of the 32-slot block rb (one warp).
+__device__ __forceinline__ void block_bounds_warp(
     int S,
+    int rb,
     const double *__restrict__ box,
     const float4 *__restrict__ posw,
     float4 *__restrict__ bb_ctr,
-    float4 *__restrict__ bb_ext,
-    const DevState *state) {
-    if (!state->rebuild || state->error) {
-        return;
-    }
+    float4 *__restrict__ bb_ext) {
     const int lane = threadIdx.x & 31;
-    const int RB = (S + TILE - 1) / TILE;
     const float Lx = (float)box[0], Ly = (float)box[4], Lz = (float)box[8];
     const float iLx = 1.0f / Lx, iLy = 1.0f / Ly, iLz = 1.0f / Lz;
-    for (int rb = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; rb < RB; rb += (gridDim.x * blockDim.x) >> 5) {
+    {
         const int s = rb * TILE + lane;
         const bool valid = s < S;
         float4 p = valid ? posw[s] : make_float4(0.f, 0.f, 0.f, 0.f);
@@ -396,8 +412,24 @@ static __global__ void k_block_bounds(
     }
 }
 
+static __global__ void k_block_bounds(
+    int S,
+    const double *__restrict__ box,
+    const float4 *__restrict__ posw,
+    float4 *__restrict__ bb_ctr,
+    float4 *__restrict__ bb_ext,
+    const DevState *state) {
+    if (!state->rebuild || state->error) {
+        return;
+    }
+    const int RB = (S + TILE - 1) / TILE;
+    for (int rb = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; rb < RB; rb += (gridDim.x * blockDim.x) >> 5) {
+        block_bounds_warp(S, rb, box, posw, bb_ctr, bb_ext);
+    }
+}
+
 // ---------------------------------------------------------------------------
-// Tile list. One CTA (4 warps) per row block rb. For every column block
+// Tile list. One CTA (TB_WARPS warps) per row block rb. For every column block
 // cb >= rb (upper triangle) whose bounding box is within the list radius of
 // rb's box, each column atom is kept when any row atom lies within the list
 // radius (minimum image, 3D). Kept atoms are packed 32 to a tile; the tiles of
@@ -437,10 +469,7 @@ __host__ __device__ __forceinline__ long long tile_base(const TileArgs &a, int r
 
 constexpr int TB_WARPS = 8;
 
-static __global__ void __launch_bounds__(TB_WARPS * 32) k_build_tiles(TileArgs a, DevState *state) {
-    if (!state->rebuild || state->error) {
-        return;
-    }
+__device__ __forceinline__ void build_tiles_cta(const TileArgs &a, const int rb, DevState *state) {
     __shared__ float4 row_pos[TILE];
     __shared__ unsigned buf[TB_WARPS][2 * TILE];
     __shared__ unsigned rem[TB_WARPS * TILE];
@@ -448,7 +477,6 @@ static __global__ void __launch_bounds__(TB_WARPS * 32) k_build_tiles(TileArgs a
     __shared__ int rem_count;
     __shared__ int is_last;
 
-    const int rb = blockIdx.x;
     const int lane = threadIdx.x & 31;
     const int warp = threadIdx.x >> 5;
     const int S = a.S;
@@ -617,6 +645,13 @@ static __global__ void __launch_bounds__(TB_WARPS * 32) k_build_tiles(TileArgs a
         state->done_ctas = 0;
         state->rebuild = 0;
     }
+}
+
+static __global__ void __launch_bounds__(TB_WARPS * 32) k_build_tiles(TileArgs a, DevState *state) {
+    if (!state->rebuild || state->error) {
+        return;
+    }
+    build_tiles_cta(a, blockIdx.x, state);
 }
 
 // Clears the rebuild flag when no neighbour list exists (pair lists only).
