@@ -71,9 +71,9 @@ def parse():
     )
     ap.add_argument(
         "--forms",
-        default="batch,serve",
+        default="batch,serve,grad",
         help="comma-separated extra forms measured after the plain path: batch (512 replicas), serve (request "
-        "loop); '' for none",
+        "loop), grad (adjoint loss gradients); '' for none",
     )
     return ap.parse_args()
 
@@ -443,6 +443,11 @@ def run_tmnb(args, world, rank, local):
             result["serve"] = run_serve_form()
         except Exception as e:
             result["serve"] = {"error": str(e)[:300]}
+    if "grad" in forms:
+        try:
+            result["grad"] = run_grad_form()
+        except Exception as e:
+            result["grad"] = {"error": str(e)[:300]}
     clk.__exit__()
     result["clocks"] = clk.summary()
     return result
@@ -740,6 +745,139 @@ def run_serve_form():
             "wall_s": seq_wall,
         },
         "timing": "host wall clock from each request's arrival to its result on the host (D2H included)",
+    }
+
+
+GRAD_FRAMES = 32
+GRAD_LAMBDA = 0.5
+
+
+def run_grad_form():
+    """Differentiation form: 1,650 waters + a 50-atom ligand; 32 frames
+    (Gaussian perturbations of 0.01 nm); targets = forces with the ligand
+    parameters perturbed by 5 %; loss = mean squared force error + 0.1 du_dl^2
+    at lambda 0.5; gradients with respect to the ligand's charges, sigmas,
+    sqrt(eps) and w offsets through the adjoint kernel. Checked against the
+    FP64 double-backward oracle and FP64 central differences (step 1e-4) on
+    one frame."""
+    import torch
+
+    from oracle.nonbonded_oracle import Oracle, candidate_pairs, force_vjp_oracle
+    from timemachine_b200 import potentials as P
+    from timemachine_b200 import testsystems
+    from timemachine_b200.adjoint import nonbonded_forces
+
+    s = testsystems.build_system(1650, (1650 * testsystems.WATER_VOLUME) ** (1 / 3), seed=SEED + 3, n_ligand=50)
+    lig = np.flatnonzero(s.lambda_offset_idxs != 0)
+    rng = np.random.default_rng(SEED + 4)
+    frames = [s.x + rng.normal(scale=0.01, size=s.x.shape) for _ in range(GRAD_FRAMES)]
+    impl = P.Nonbonded(s.exclusion_idxs, s.scales, s.lambda_plane_idxs, s.lambda_offset_idxs, s.beta, s.cutoff)
+    impl = impl.unbound_impl(np.float32)
+    p_target = s.params.copy()
+    p_target[lig] *= 1 + 0.05 * rng.normal(size=(lig.size, 3))
+    box = torch.as_tensor(s.box, device="cuda")
+    xs = [torch.as_tensor(f, device="cuda") for f in frames]
+    targets = []
+    with torch.no_grad():
+        pt = torch.as_tensor(p_target, device="cuda")
+        w0 = torch.as_tensor(s.lambda_offset_idxs.astype(np.float64), device="cuda")
+        for x in xs:
+            targets.append(nonbonded_forces(impl, pt, w0, x, box, GRAD_LAMBDA)[0].clone())
+
+    def loss_and_grads():
+        params = torch.as_tensor(s.params, device="cuda").requires_grad_(True)
+        w_off = torch.as_tensor(s.lambda_offset_idxs.astype(np.float64), device="cuda").requires_grad_(True)
+        total = 0.0
+        for x, t in zip(xs, targets):
+            f, dl = nonbonded_forces(impl, params, w_off, x, box, GRAD_LAMBDA)
+            total = total + ((f - t) ** 2).mean() + 0.1 * dl**2
+        loss = total / len(xs)
+        loss.backward()
+        return loss, params.grad, w_off.grad
+
+    loss_and_grads()
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    loss, gp, gw = loss_and_grads()
+    e1.record()
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+
+    # FP64 references on frame 0 (one frame of the loss, same upstream form)
+    x0 = frames[0]
+    f0, dl0 = nonbonded_forces(impl, torch.as_tensor(s.params, device="cuda"), w0, xs[0], box, GRAD_LAMBDA)
+    o = Oracle(s.lambda_plane_idxs, s.lambda_offset_idxs, s.beta, s.cutoff, s.exclusion_idxs, s.scales)
+    fx, _, fl, _ = o(x0, s.params, s.box, GRAD_LAMBDA)
+    t0 = targets[0].cpu().numpy()
+    G = 2.0 * (fx - t0) / fx.size
+    g = 0.2 * fl
+    pairs = candidate_pairs(x0, s.box, s.cutoff)
+    off = s.lambda_offset_idxs.astype(np.float64)
+    _, rp, rw = force_vjp_oracle(
+        x0, s.params, s.box, GRAD_LAMBDA, s.lambda_plane_idxs, off, s.beta, s.cutoff, s.exclusion_idxs, s.scales, G, g,
+        pairs=pairs,
+    )
+    # the kernel's VJP with the same (FP64) upstream gradients
+    kp = torch.zeros(s.params.size, dtype=torch.float64, device="cuda")
+    kw = torch.zeros(s.N, dtype=torch.float64, device="cuda")
+    impl.adjoint_device(xs[0], torch.as_tensor(s.params, device="cuda").reshape(-1), box, GRAD_LAMBDA,
+                        torch.as_tensor(G, device="cuda"), g, kp, kw)
+    kp = kp.cpu().numpy().reshape(-1, 3)
+    kw = kw.cpu().numpy()
+
+    def rel(a, b):
+        return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+    h = 1e-4
+
+    def phi(params, offsets):
+        return force_vjp_oracle(x0, params, s.box, GRAD_LAMBDA, s.lambda_plane_idxs, offsets, s.beta, s.cutoff,
+                                s.exclusion_idxs, s.scales, G, g, pairs=pairs)[0]
+
+    def crosses_cutoff(a):
+        # a +-h offset step that carries a pair across the (discontinuous) cutoff is not a derivative test
+        mine = pairs[(pairs[:, 0] == a) | (pairs[:, 1] == a)]
+        i, j = mine[:, 0], mine[:, 1]
+        L = np.diag(s.box)
+        r = x0[i] - x0[j]
+        r -= L * np.floor(r / L + 0.5)
+        inside = []
+        for dh in (-h, h):
+            o = off.copy()
+            o[a] += dh
+            w = s.cutoff * (s.lambda_plane_idxs + o * GRAD_LAMBDA)
+            inside.append(np.sqrt((r * r).sum(1) + (w[i] - w[j]) ** 2) < s.cutoff)
+        return np.any(inside[0] != inside[1])
+
+    fd_err, n_fd = 0.0, 0
+    for a in lig[:3]:
+        for col in range(3):
+            pp, pm = s.params.copy(), s.params.copy()
+            pp[a, col] += h
+            pm[a, col] -= h
+            fd = (phi(pp, off) - phi(pm, off)) / (2 * h)
+            fd_err = max(fd_err, abs(fd - kp[a, col]) / max(abs(fd), 1.0))
+            n_fd += 1
+    for a in [a for a in lig if not crosses_cutoff(a)][:3]:
+        op, om = off.copy(), off.copy()
+        op[a] += h
+        om[a] -= h
+        fd = (phi(s.params, op) - phi(s.params, om)) / (2 * h)
+        fd_err = max(fd_err, abs(fd - kw[a]) / max(abs(fd), 1.0))
+        n_fd += 1
+    return {
+        "workload": f"{s.N} atoms (1650 waters + 50-atom ligand), {GRAD_FRAMES} frames, lambda {GRAD_LAMBDA}; "
+        "loss = mean squared force error + 0.1 du_dl^2; d/d ligand (q, sigma, sqrt eps, w offset)",
+        "loss": float(loss),
+        "ms_per_loss_gradient": ms,
+        "frames_per_s": GRAD_FRAMES / (ms / 1e3),
+        "grad_norm_ligand_params": float(gp[lig].norm()),
+        "grad_norm_ligand_offsets": float(gw[lig].norm()),
+        "vjp_relative_error_vs_fp64_double_backward": {"params": rel(kp, rp), "offsets": rel(kw, rw)},
+        "vjp_max_relative_error_vs_fp64_central_differences_step_1e-4": fd_err,
+        "central_difference_checks": n_fd,
+        "timing": "CUDA events around the 32-frame loss and its backward (forward kernels + adjoint kernel)",
     }
 
 

@@ -387,6 +387,31 @@ int tmnb_potential_num_params(const tmnb_potential *pot);
 int tmnb_potential_num_atoms(const tmnb_potential *pot);
 
 /*
+ * Adjoint (no reference counterpart: the reference differentiates its jax
+ * potential, timemachine/potentials/nonbonded.py, with jax.grad). For the
+ * potential at (x, params, lambda) and upstream gradients g_du_dx [N,3]
+ * (of du_dx, as float64) and g_du_dl (of the summed du_dl), ADDS the
+ * vector-Jacobian product to d_grad_p [P] (d/d charge, sigma/2, sqrt(eps))
+ * and d_grad_w [N] (d/d the per-atom lambda offset, treated as a continuous
+ * coefficient of w = cutoff * (plane + offset * lambda)). Pair terms are
+ * recomputed in FP64; nothing from the forward pass is stored. Non-interpolated
+ * AllPairs, PairList and Nonbonded handles (TMNB_ERR_UNSUPPORTED otherwise).
+ */
+tmnb_status tmnb_potential_adjoint_device(
+    tmnb_potential *pot,
+    int N,
+    int P,
+    const double *d_x,
+    const double *d_p,
+    const double *d_box,
+    double lambda,
+    const double *d_g_du_dx, /* [N,3] */
+    double g_du_dl,
+    double *d_grad_p, /* [P] += */
+    double *d_grad_w, /* [N] += */
+    void *stream);
+
+/*
  * Replica batch (no single reference counterpart: it replaces the loops in
  * which the reference evaluates or simulates replicas one at a time, one
  * Potential::execute_device / one Context per replica and lambda). Holds any

@@ -201,6 +201,32 @@ def interaction_group_oracle(x, params, box, lam, plane, offset, beta, cutoff, r
     return pair_list_oracle(x, params, box, lam, plane, offset, beta, cutoff, pairs, ones, interpolated)
 
 
+def force_vjp_oracle(x, params, box, lam, plane, offset, beta, cutoff, exclusion_idxs, scales, g_du_dx, g_du_dl,
+                     pairs=None):
+    """Reference for the adjoint kernel: with du_dx = dU/dx and du_dl = dU/dlambda
+    of the Nonbonded energy (offsets taken as continuous), returns
+    (Phi, dPhi/dparams [N,3], dPhi/doffsets [N]) for
+    Phi = sum(g_du_dx * du_dx) + g_du_dl * du_dl, by FP64 double backward (the
+    restatement of jax.grad applied twice to timemachine/potentials/nonbonded.py)."""
+    x = np.asarray(x, dtype=np.float64)
+    N = x.shape[0]
+    if pairs is None:
+        pairs = candidate_pairs(x, box, cutoff)
+    cm, lm = exclusion_masks(pairs, N, exclusion_idxs, scales)
+    tx = torch.tensor(x, requires_grad=True)
+    tp = torch.tensor(np.asarray(params, dtype=np.float64), requires_grad=True)
+    tl = torch.tensor(float(lam), dtype=torch.float64, requires_grad=True)
+    toff = torch.tensor(np.asarray(offset, dtype=np.float64), requires_grad=True)
+    tb = torch.tensor(np.asarray(box, dtype=np.float64))
+    u = energy(tx, tp, tb, tl, torch.tensor(np.asarray(plane, dtype=np.float64)), toff, float(beta), float(cutoff),
+               pairs, cm, lm)
+    du_dx, du_dl = torch.autograd.grad(u, [tx, tl], create_graph=True)
+    phi = (torch.as_tensor(np.asarray(g_du_dx, dtype=np.float64)) * du_dx).sum() + float(g_du_dl) * du_dl
+    gp, goff = torch.autograd.grad(phi, [tp, toff], allow_unused=True)
+    goff = torch.zeros(N, dtype=torch.float64) if goff is None else goff
+    return float(phi.detach()), gp.numpy(), goff.numpy()
+
+
 def force_error(ref, test):
     """max_i |F_ref - F_test|_inf / max(|F_ref,i|, 1) (tests/common.py:386-409 convention)."""
     ref = np.asarray(ref)

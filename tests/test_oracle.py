@@ -10,6 +10,7 @@ from oracle.nonbonded_oracle import (
     Oracle,
     candidate_pairs,
     exclusion_masks,
+    force_vjp_oracle,
     interaction_group_oracle,
     pair_list_oracle,
 )
@@ -197,3 +198,33 @@ def test_interaction_group_oracle_is_all_minus_both_groups(rng, interpolated):
     a, r, k = allp(None), allp(rows), allp(cols)
     for n in range(4):
         np.testing.assert_allclose(g[n], np.asarray(a[n]) - np.asarray(r[n]) - np.asarray(k[n]), rtol=1e-10, atol=1e-9)
+
+
+def test_force_vjp_oracle_against_finite_differences(rng):
+    """The double-backward reference of the adjoint against FP64 central
+    differences (step 1e-4) of Phi = sum(G * du_dx) + g * du_dl."""
+    c = small_water_case(rng, 90)
+    N = c["x"].shape[0]
+    G = rng.normal(size=(N, 3))
+    g = 0.7
+    lam = 0.4
+    args = (c["box"], lam, c["plane"], c["offset"].astype(np.float64), 2.0, 1.1, c["exclusion_idxs"], c["scales"])
+    pairs = candidate_pairs(c["x"], c["box"], 1.1)
+    phi, gp, goff = force_vjp_oracle(c["x"], c["params"], *args, G, g, pairs=pairs)
+    h = 1e-4
+    for a, col in [(0, 0), (3, 1), (5, 2)]:
+        pp, pm = c["params"].copy(), c["params"].copy()
+        pp[a, col] += h
+        pm[a, col] -= h
+        fd = (force_vjp_oracle(c["x"], pp, *args, G, g, pairs=pairs)[0]
+              - force_vjp_oracle(c["x"], pm, *args, G, g, pairs=pairs)[0]) / (2 * h)
+        assert abs(fd - gp[a, col]) <= 1e-5 * max(1.0, abs(fd)), (a, col, fd, gp[a, col])
+    for a in [1, 4]:
+        op, om = c["offset"].astype(np.float64), c["offset"].astype(np.float64)
+        op[a] += h
+        om[a] -= h
+        ap = (c["box"], lam, c["plane"], op, 2.0, 1.1, c["exclusion_idxs"], c["scales"])
+        am = (c["box"], lam, c["plane"], om, 2.0, 1.1, c["exclusion_idxs"], c["scales"])
+        fd = (force_vjp_oracle(c["x"], c["params"], *ap, G, g, pairs=pairs)[0]
+              - force_vjp_oracle(c["x"], c["params"], *am, G, g, pairs=pairs)[0]) / (2 * h)
+        assert abs(fd - goff[a]) <= 1e-5 * max(1.0, abs(fd)), (a, fd, goff[a])

@@ -1,0 +1,199 @@
+// Adjoint of the nonbonded forces and du/dlambda with respect to the per-atom
+// parameters (charge, sigma/2, sqrt(epsilon)) and the per-atom w offsets.
+//
+// For upstream gradients G (of du_dx, [N,3]) and g (of du_dl, scalar) it
+// accumulates the vector-Jacobian product
+//   dPhi/dtheta,  Phi = sum_i G_i . du_dx_i + g * du_dl,
+// pair by pair, recomputing each pair's terms in FP64 from the original
+// coordinates and parameters (nothing is stored by the forward pass). It walks
+// the same tile list and scaled-pair list as the forward kernels.
+//
+// Per pair (r = x_i - x_j minimum image, dw = w_i - w_j,
+// w = cutoff * (plane + offset * lambda), d^2 = r.r + dw^2 < cutoff^2) the
+// energy is U(d) = s * [cs * q_i q_j erfc(beta d)/d + ls * 4 e_i e_j ((S/d)^12 - (S/d)^6)]
+// (S = sig_i + sig_j; s = +1 for all pairs, -1 for the scaled exclusions;
+// LJ only where e_i e_j != 0), as timemachine/potentials/nonbonded.py:29-59,
+// 133-264 define it. With h = U'(d)/d the pair adds h r to du_dx_i, -h r to
+// du_dx_j and h dw cutoff (off_i - off_j) to du_dl, so
+//   Phi_pair = h * B,  B = (G_i - G_j).r + g * dw * cutoff * (off_i - off_j),
+//   dPhi/dp      = B * dh/dp                         (p: q, sig, eps of i or j)
+//   dPhi/doff_i  = B * h'(d) * dw * cutoff * lambda / d
+//                  + g * h * cutoff * (cutoff * lambda * (off_i - off_j) + dw)
+//   dPhi/doff_j  = -(the same).
+// The derivatives of erfc(beta d)/d follow from d/dd erfc(beta d) =
+// -2 beta / sqrt(pi) exp(-beta^2 d^2).
+#pragma once
+
+#include "nb_kernels.cuh"
+
+namespace tmb {
+
+struct AdjointArgs {
+    int N;
+    int S;
+    const double *x;      // [N,3]
+    const double *p;      // [N,3]
+    const double *box;    // [9]
+    const int *plane;     // [N]
+    const int *offset;    // [N]
+    double lambda, beta, cutoff;
+    const unsigned *perm; // [S] slot -> atom
+    const unsigned *tile_cols;
+    const int4 *items;
+    int M;
+    const int *pair_idxs; // [M,2] atoms
+    const double *scales; // [M,2]
+    double pair_sign;     // -1: the listed pairs are subtracted (exclusions), +1: added
+    const double *g_dx;   // [N,3]
+    double g_dl;
+    double *grad_p; // [N,3] +=
+    double *grad_w; // [N] +=
+    DevState *state;
+};
+
+// Gradient contributions of one pair: to atom i (q, sig, eps, off) and atom j.
+struct PairGrad {
+    double qi, si, ei, wi;
+    double qj, sj, ej, wj;
+};
+
+__device__ __forceinline__ PairGrad adjoint_pair(const AdjointArgs &a, int ai, int aj, double cs, double ls, double sign) {
+    PairGrad out = {0, 0, 0, 0, 0, 0, 0, 0};
+    const double *xi = a.x + 3 * (size_t)ai;
+    const double *xj = a.x + 3 * (size_t)aj;
+    double r[3];
+    double r2 = 0;
+    for (int d = 0; d < 3; d++) {
+        const double L = a.box[4 * d];
+        double v = xi[d] - xj[d];
+        v -= L * floor(v / L + 0.5);
+        r[d] = v;
+        r2 += v * v;
+    }
+    const double c = a.cutoff;
+    const double doff = (double)(a.offset[ai] - a.offset[aj]);
+    const double dw = c * ((a.plane[ai] - a.plane[aj]) + doff * a.lambda);
+    const double d2 = r2 + dw * dw;
+    if (!(d2 < c * c)) {
+        return out;
+    }
+    const double d = sqrt(d2);
+    const double inv_d = 1.0 / d;
+    const double *pi = a.p + 3 * (size_t)ai;
+    const double *pj = a.p + 3 * (size_t)aj;
+    const double qi = pi[0], si = pi[1], ei = pi[2];
+    const double qj = pj[0], sj = pj[1], ej = pj[2];
+
+    // electrostatics: E = erfc(beta d)/d
+    const double bd = a.beta * d;
+    const double g0 = erfc(bd);
+    const double g1 = -2.0 * a.beta * 0.56418958354775628695 * exp(-bd * bd); // d erfc(beta d)/dd
+    const double g2 = -2.0 * a.beta * a.beta * d * g1;                           // second derivative
+    const double E1 = g1 * inv_d - g0 * inv_d * inv_d;
+    const double E2 = g2 * inv_d - 2.0 * g1 * inv_d * inv_d + 2.0 * g0 * inv_d * inv_d * inv_d;
+    double h = cs * qi * qj * E1 * inv_d;
+    double hp = cs * qi * qj * (E2 * inv_d - E1 * inv_d * inv_d);
+    double dh_qi = cs * qj * E1 * inv_d, dh_qj = cs * qi * E1 * inv_d;
+    double dh_s = 0, dh_ei = 0, dh_ej = 0;
+    if (ei * ej != 0) {
+        const double S = si + sj;
+        const double sd = S * inv_d;
+        const double sd6 = sd * sd * sd * sd * sd * sd;
+        const double inv_d2 = inv_d * inv_d;
+        // U_lj = 4 e e (sd^12 - sd^6); h_lj = U'/d = 4 e e (-12 sd^12 + 6 sd^6) / d^2
+        const double base = (-12.0 * sd6 * sd6 + 6.0 * sd6) * inv_d2;
+        const double ee = 4.0 * ls * ei * ej;
+        h += ee * base;
+        hp += ee * (168.0 * sd6 * sd6 - 48.0 * sd6) * inv_d2 * inv_d;
+        dh_s = ee * (-144.0 * sd6 * sd6 + 36.0 * sd6) * inv_d2 / S;
+        dh_ei = 4.0 * ls * ej * base;
+        dh_ej = 4.0 * ls * ei * base;
+    }
+    h *= sign;
+    hp *= sign;
+    const double *Gi = a.g_dx + 3 * (size_t)ai;
+    const double *Gj = a.g_dx + 3 * (size_t)aj;
+    const double B = (Gi[0] - Gj[0]) * r[0] + (Gi[1] - Gj[1]) * r[1] + (Gi[2] - Gj[2]) * r[2] + a.g_dl * dw * c * doff;
+    out.qi = sign * B * dh_qi;
+    out.qj = sign * B * dh_qj;
+    out.si = sign * B * dh_s;
+    out.sj = out.si;
+    out.ei = sign * B * dh_ei;
+    out.ej = sign * B * dh_ej;
+    const double dphi_doff_i = B * hp * dw * c * a.lambda * inv_d + a.g_dl * h * c * (c * a.lambda * doff + dw);
+    out.wi = dphi_doff_i;
+    out.wj = -dphi_doff_i;
+    return out;
+}
+
+__device__ __forceinline__ void adjoint_add(const AdjointArgs &a, int atom, double q, double s, double e, double w) {
+    atomicAdd(a.grad_p + 3 * (size_t)atom + 0, q);
+    atomicAdd(a.grad_p + 3 * (size_t)atom + 1, s);
+    atomicAdd(a.grad_p + 3 * (size_t)atom + 2, e);
+    atomicAdd(a.grad_w + atom, w);
+}
+
+// One warp per tile work item (lane = row slot), then one lane per scaled
+// pair; dynamic work counter state->next_item (reset by k_check_prepare).
+static __global__ void __launch_bounds__(128) k_adjoint(AdjointArgs a) {
+    if (a.state->error) {
+        return;
+    }
+    const int lane = threadIdx.x & 31;
+    const unsigned S = (unsigned)a.S;
+    const int n_items = a.tile_cols ? a.state->n_items : 0;
+    const int n_total = n_items + (a.M + TILE - 1) / TILE;
+    for (;;) {
+        int item = 0;
+        if (lane == 0) {
+            item = atomicAdd(&a.state->next_item, 1);
+        }
+        item = __shfl_sync(FULL_MASK, item, 0);
+        if (item >= n_total) {
+            break;
+        }
+        if (item >= n_items) {
+            const int pair = (item - n_items) * TILE + lane;
+            if (pair < a.M) {
+                const int ai = a.pair_idxs[2 * pair], aj = a.pair_idxs[2 * pair + 1];
+                const PairGrad g = adjoint_pair(a, ai, aj, a.scales[2 * pair], a.scales[2 * pair + 1], a.pair_sign);
+                adjoint_add(a, ai, g.qi, g.si, g.ei, g.wi);
+                adjoint_add(a, aj, g.qj, g.sj, g.ej, g.wj);
+            }
+            continue;
+        }
+        const int4 it = a.items[item];
+        const unsigned i = (unsigned)(it.x * TILE + lane);
+        const int ai = i < S ? (int)a.perm[i] : -1;
+        double rq = 0, rs = 0, re = 0, rw = 0;
+        for (int t = 0; t < it.z; t++) {
+            const long long tile = (long long)it.y + t;
+            for (int col = 0; col < TILE; col++) {
+                const unsigned j = a.tile_cols[tile * TILE + col];
+                PairGrad g = {0, 0, 0, 0, 0, 0, 0, 0};
+                if (ai >= 0 && j < S && i < j) {
+                    g = adjoint_pair(a, ai, (int)a.perm[j], 1.0, 1.0, 1.0);
+                }
+                rq += g.qi;
+                rs += g.si;
+                re += g.ei;
+                rw += g.wi;
+                // column atom: warp sum, one atomic
+                for (int o = 16; o > 0; o >>= 1) {
+                    g.qj += __shfl_xor_sync(FULL_MASK, g.qj, o);
+                    g.sj += __shfl_xor_sync(FULL_MASK, g.sj, o);
+                    g.ej += __shfl_xor_sync(FULL_MASK, g.ej, o);
+                    g.wj += __shfl_xor_sync(FULL_MASK, g.wj, o);
+                }
+                if (lane == 0 && j < S) {
+                    adjoint_add(a, (int)a.perm[j], g.qj, g.sj, g.ej, g.wj);
+                }
+            }
+        }
+        if (ai >= 0) {
+            adjoint_add(a, ai, rq, rs, re, rw);
+        }
+    }
+}
+
+} // namespace tmb

@@ -11,6 +11,7 @@
 //              one row atom and one column atom (the complement); slots hold
 //              the spatially sorted rows, then the sorted columns.
 #include "engine.hpp"
+#include "nb_adjoint.cuh"
 #include "nb_kernels.cuh"
 
 #include <algorithm>
@@ -593,6 +594,59 @@ class NonbondedPotential : public PotentialBase {
         }
     }
 
+    // Vector-Jacobian product of (du_dx, du_dl) at (x, params, lambda) with
+    // upstream (g_du_dx [N,3], g_du_dl): adds d/dparams into grad_p [N,3] and
+    // d/d(lambda offset) into grad_w [N] (FP64, nb_adjoint.cuh). The
+    // neighbour list is brought up to date for x first.
+    void adjoint_device(
+        int N,
+        int P,
+        const double *d_x,
+        const double *d_p,
+        const double *d_box,
+        double lambda,
+        const double *d_g_dx,
+        double g_dl,
+        double *d_grad_p,
+        double *d_grad_w,
+        cudaStream_t stream) {
+        if (interp_ || kind_ == Kind::Group) {
+            throw Error(TMNB_ERR_UNSUPPORTED, "the adjoint covers non-interpolated AllPairs, PairList and Nonbonded");
+        }
+        if (!d_g_dx || !d_grad_p || !d_grad_w) {
+            throw Error(TMNB_ERR_INVALID_ARGUMENT, "upstream gradient and outputs must be non-null");
+        }
+        // check, stage and (when needed) rebuild, no pair work
+        execute_windows_device(N, P, d_x, d_p, d_box, 1, &lambda, nullptr, nullptr, nullptr, nullptr, stream);
+        AdjointArgs a;
+        a.N = N_;
+        a.S = S_;
+        a.x = d_x;
+        a.p = d_p;
+        a.box = d_box;
+        a.plane = plane_.p;
+        a.offset = offset_.p;
+        a.lambda = lambda;
+        a.beta = beta_;
+        a.cutoff = cutoff_;
+        a.perm = perm_.p;
+        a.tile_cols = has_nblist_ ? tile_cols_.p : nullptr;
+        a.items = items_.p;
+        a.M = M_;
+        a.pair_idxs = pair_idxs_.p;
+        a.scales = scales_.p;
+        a.pair_sign = negated_ ? -1.0 : 1.0;
+        a.g_dx = d_g_dx;
+        a.g_dl = g_dl;
+        a.grad_p = d_grad_p;
+        a.grad_w = d_grad_w;
+        a.state = state_.p;
+        int per_sm = 0;
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_adjoint, 128, 0));
+        k_adjoint<<<std::max(1, per_sm) * num_sms(), 128, 0, stream>>>(a);
+        CK(cudaPeekAtLastError());
+    }
+
     void nblist_shape(int *S, int *RB, long long *tile_capacity) const {
         if (S) {
             *S = S_;
@@ -1126,6 +1180,28 @@ tmnb_status tmnb_potential_copy_nblist(
     }
     return tmb::guarded(
         [&] { as_nb(pot)->copy_nblist(static_cast<cudaStream_t>(stream), perm, row_block_ntiles, tile_cols); });
+}
+
+tmnb_status tmnb_potential_adjoint_device(
+    tmnb_potential *pot,
+    int N,
+    int P,
+    const double *d_x,
+    const double *d_p,
+    const double *d_box,
+    double lambda,
+    const double *d_g_du_dx,
+    double g_du_dl,
+    double *d_grad_p,
+    double *d_grad_w,
+    void *stream) {
+    if (tmnb_status s = check_handle(pot)) {
+        return s;
+    }
+    return tmb::guarded([&] {
+        as_nb(pot)->adjoint_device(
+            N, P, d_x, d_p, d_box, lambda, d_g_du_dx, g_du_dl, d_grad_p, d_grad_w, static_cast<cudaStream_t>(stream));
+    });
 }
 
 tmnb_status tmnb_potential_enable_timing(tmnb_potential *pot, int on) {

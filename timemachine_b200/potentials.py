@@ -326,6 +326,28 @@ class Potential:
             )
         )
 
+    def adjoint_device(self, x, p, box, lam, g_du_dx, g_du_dl, grad_p, grad_w, stream=None):
+        """Adds the vector-Jacobian product of (du_dx, du_dl) with upstream
+        (g_du_dx [N,3] float64, g_du_dl float) into grad_p [P] and grad_w [N]
+        (float64 device tensors): d/d params and d/d per-atom lambda offsets."""
+        import torch
+
+        def addr(t):
+            if not t.is_contiguous():
+                raise RuntimeError("device tensors must be contiguous")
+            return ctypes.c_void_p(t.data_ptr())
+
+        if stream is None:
+            stream = torch.cuda.current_stream(x.device).cuda_stream
+        elif hasattr(stream, "cuda_stream"):
+            stream = stream.cuda_stream
+        _lib.check(
+            self._lib.tmnb_potential_adjoint_device(
+                self._h, x.shape[0], p.numel(), addr(x), addr(p), addr(box), float(lam), addr(g_du_dx),
+                float(g_du_dl), addr(grad_p), addr(grad_w), ctypes.c_void_p(stream),
+            )
+        )
+
     def check_device_error(self, stream=None):
         import torch
 

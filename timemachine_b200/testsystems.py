@@ -153,21 +153,25 @@ def build_system(
     n_side = int(np.ceil((n_waters + (n_ligand if n_ligand else 0)) ** (1.0 / 3.0) - 1e-9))
     while n_side**3 < n_waters:
         n_side += 1
-    spacing = box_edge / n_side
-    g = (np.arange(n_side) + 0.5) * spacing
-    lattice = np.stack(np.meshgrid(g, g, g, indexing="ij"), axis=-1).reshape(-1, 3)
-    if lig is not None:
-        # drop lattice sites nearest the ligand first, then random sites
-        dmin = np.min(np.linalg.norm(lattice[:, None, :] - lig[None, :, :], axis=-1), axis=1)
-        order = np.argsort(dmin)
-        near = order[dmin[order] < 0.3]
-        keep_mask = np.ones(len(lattice), dtype=bool)
-        keep_mask[near] = False
-        avail = np.flatnonzero(keep_mask)
-    else:
-        avail = np.arange(len(lattice))
-    if len(avail) < n_waters:
-        raise ValueError("box too small for the requested number of waters")
+    while True:
+        spacing = box_edge / n_side
+        g = (np.arange(n_side) + 0.5) * spacing
+        lattice = np.stack(np.meshgrid(g, g, g, indexing="ij"), axis=-1).reshape(-1, 3)
+        if lig is not None:
+            # drop lattice sites nearest the ligand first, then random sites
+            dmin = np.min(np.linalg.norm(lattice[:, None, :] - lig[None, :, :], axis=-1), axis=1)
+            order = np.argsort(dmin)
+            near = order[dmin[order] < 0.3]
+            keep_mask = np.ones(len(lattice), dtype=bool)
+            keep_mask[near] = False
+            avail = np.flatnonzero(keep_mask)
+        else:
+            avail = np.arange(len(lattice))
+        if len(avail) >= n_waters:
+            break
+        if spacing < 0.2:
+            raise ValueError("box too small for the requested number of waters")
+        n_side += 1  # the ligand displaced too many sites: a finer lattice
     chosen = np.sort(rng.choice(avail, size=n_waters, replace=False))
     O = lattice[chosen] + rng.normal(scale=jitter, size=(n_waters, 3))
     R = random_rotations(rng, n_waters)
