@@ -869,7 +869,7 @@ def run_grad_form():
     return {
         "workload": f"{s.N} atoms (1650 waters + 50-atom ligand), {GRAD_FRAMES} frames, lambda {GRAD_LAMBDA}; "
         "loss = mean squared force error + 0.1 du_dl^2; d/d ligand (q, sigma, sqrt eps, w offset)",
-        "loss": float(loss),
+        "loss": float(loss.detach()),
         "ms_per_loss_gradient": ms,
         "frames_per_s": GRAD_FRAMES / (ms / 1e3),
         "grad_norm_ligand_params": float(gp[lig].norm()),
