@@ -387,6 +387,15 @@ int tmnb_potential_num_params(const tmnb_potential *pot);
 int tmnb_potential_num_atoms(const tmnb_potential *pot);
 
 /*
+ * Tile schedule of the pair kernel (no reference counterpart): 0 (default)
+ * the rotating sweep, which evaluates a tile in 32 lane-rotation rounds; 1
+ * the compacted sweep, which tests all 32x32 slots of a tile first and then
+ * evaluates only the in-cutoff pairs, 32 at a time. The results are
+ * identical; the switch exists for measurement.
+ */
+tmnb_status tmnb_potential_set_pair_schedule(tmnb_potential *pot, int compact);
+
+/*
  * Adjoint (no reference counterpart: the reference differentiates its jax
  * potential, timemachine/potentials/nonbonded.py, with jax.grad). For the
  * potential at (x, params, lambda) and upstream gradients g_du_dx [N,3]

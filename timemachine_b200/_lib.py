@@ -95,6 +95,8 @@ def _declare(lib):
     lib.tmnb_harmonic_angle_create.argtypes = [i, i, vp, vp, vp, ctypes.POINTER(vp)]
     lib.tmnb_pair_list_execute_static.argtypes = [i, i, vp, vp, vp, vp, d, d, i, vp, vp, vp, d, vp, vp, vp, vp, vp]
     lib.tmnb_pair_list_execute_static.restype = ctypes.c_int
+    lib.tmnb_potential_set_pair_schedule.argtypes = [vp, i]
+    lib.tmnb_potential_set_pair_schedule.restype = ctypes.c_int
     lib.tmnb_potential_adjoint_device.argtypes = [vp, i, i, vp, vp, vp, d, vp, d, vp, vp, vp]
     lib.tmnb_potential_adjoint_device.restype = ctypes.c_int
     lib.tmnb_batch_create.argtypes = [ctypes.POINTER(vp)]

@@ -357,8 +357,8 @@ __global__ void __launch_bounds__(128) k_b_pair(const Rep *__restrict__ reps, in
         for (int t = 0; t < it.z; t++) {
             const long long tile = (long long)it.y + t;
             const unsigned j = r.tile_cols[tile * TILE + lane];
-            tile_pass<float, U, DX, DL, DP, false>(
-                a, lane, S, i, j, 0, a.acc, box_x, box_y, box_z, inv_box_x, inv_box_y, inv_box_z, cutoff_squared, beta,
+            tile_pass<float, U, DX, DL, DP, false, false>(
+                nullptr, a, lane, S, i, j, 0, a.acc, box_x, box_y, box_z, inv_box_x, inv_box_y, inv_box_z, cutoff_squared, beta,
                 gi_x, gi_y, gi_z, g_qi, g_sigi, g_epsi, du_dl, energy);
         }
         if (i < S) {

@@ -713,6 +713,105 @@ struct PairArgs {
 
 __device__ __forceinline__ void red_add(unsigned long long *p, unsigned long long v) { atomicAdd(p, v); }
 
+// The arithmetic of one in-range pair (row atom i, column atom j) from its
+// minimum-image deltas and 4D d2: adds the row's and the column's fixed-point
+// contributions. Every sweep calls this one function, so a pair rounds the
+// same whichever schedule evaluates it. Per-pair arithmetic and validity follow
+// timemachine/cpp/src/kernels/k_nonbonded.cuh:424-546; the column
+// contribution of du_dx is the exact negation of the row contribution
+// (llrint is odd under round-half-even), so it is converted once.
+template <typename Real, bool U, bool DX, bool DL, bool DP, bool INTERP, bool ALCH>
+__device__ __forceinline__ void pair_terms(
+    const Real delta_x,
+    const Real delta_y,
+    const Real delta_z,
+    const Real delta_w,
+    const Real d2,
+    const Real qi,
+    const Real sig_i,
+    const Real eps_i,
+    const Real dw_dl_i,
+    const Real dq_dl_i,
+    const Real dsig_dl_i,
+    const Real deps_dl_i,
+    const Real qj,
+    const Real sig_j,
+    const Real eps_j,
+    const Real dw_dl_j,
+    const Real dq_dl_j,
+    const Real dsig_dl_j,
+    const Real deps_dl_j,
+    const Real beta,
+    unsigned long long &gi_x,
+    unsigned long long &gi_y,
+    unsigned long long &gi_z,
+    unsigned long long &g_qi,
+    unsigned long long &g_sigi,
+    unsigned long long &g_epsi,
+    unsigned long long &du_dl,
+    unsigned long long &energy,
+    unsigned long long &gj_x,
+    unsigned long long &gj_y,
+    unsigned long long &gj_z,
+    unsigned long long &g_qj,
+    unsigned long long &g_sigj,
+    unsigned long long &g_epsj) {
+    Real u;
+    Real prefactor;
+    Real erfc_bd;
+    Real d;
+    Real inv_d;
+    Real inv_d2;
+    Real qij_inv;
+    Real factor;
+    electrostatics<Real, U>((Real)1, qi, qj, d2, beta, d, inv_d, inv_d2, erfc_bd, prefactor, u, qij_inv, factor);
+    Real real_du_dl = 0;
+    if (eps_i != 0 && eps_j != 0) {
+        Real sig_grad;
+        Real eps_grad;
+        lennard_jones<Real, U>(
+            (Real)1, eps_i, eps_j, sig_i, sig_j, inv_d, inv_d2, qij_inv, factor, erfc_bd, u, prefactor, sig_grad,
+            eps_grad);
+        if (DP) {
+            const unsigned long long gs = to_fixed(sig_grad, FX_EXPONENT_SIG);
+            g_sigi += gs;
+            g_sigj += gs;
+            g_epsi += to_fixed(fmul(eps_grad, eps_j), FX_EXPONENT_EPS);
+            g_epsj += to_fixed(fmul(eps_grad, eps_i), FX_EXPONENT_EPS);
+        }
+        if (DL && ALCH && INTERP) {
+            real_du_dl = ffma(sig_grad, fadd(dsig_dl_i, dsig_dl_j), real_du_dl);
+            real_du_dl = ffma(eps_grad, sum_of_products_rn(eps_j, deps_dl_i, eps_i, deps_dl_j), real_du_dl);
+        }
+    }
+    if (DX) {
+        unsigned long long fx, fy, fz, nx, ny, nz;
+        to_fixed_pair(fmul(prefactor, delta_x), FX_EXPONENT, fx, nx);
+        to_fixed_pair(fmul(prefactor, delta_y), FX_EXPONENT, fy, ny);
+        to_fixed_pair(fmul(prefactor, delta_z), FX_EXPONENT, fz, nz);
+        gi_x += fx;
+        gi_y += fy;
+        gi_z += fz;
+        gj_x += nx;
+        gj_y += ny;
+        gj_z += nz;
+    }
+    if (DP) {
+        g_qi += to_fixed(fmul(fmul(qj, inv_d), erfc_bd), FX_EXPONENT);
+        g_qj += to_fixed(fmul(fmul(qi, inv_d), erfc_bd), FX_EXPONENT);
+    }
+    if (DL && ALCH) {
+        real_du_dl = ffma(fmul(delta_w, prefactor), fsub(dw_dl_i, dw_dl_j), real_du_dl);
+        if (INTERP) {
+            real_du_dl = ffma(fmul(inv_d, erfc_bd), sum_of_products_rn(qj, dq_dl_i, qi, dq_dl_j), real_du_dl);
+        }
+        du_dl += to_fixed(real_du_dl, FX_EXPONENT);
+    }
+    if (U) {
+        energy += to_fixed(u, FX_EXPONENT);
+    }
+}
+
 // One 32x32 tile: lane owns row slot i; the column atoms rotate through the
 // lanes by one position per round (32 rounds), carrying their accumulators.
 // Per-pair arithmetic and validity follow
@@ -786,61 +885,10 @@ __device__ __forceinline__ void sweep_tile(
         }
         const bool valid = i < S && j < S && i < j;
         if (valid && d2 < cutoff_squared) {
-            Real u;
-            Real prefactor;
-            Real erfc_bd;
-            Real d;
-            Real inv_d;
-            Real inv_d2;
-            Real qij_inv;
-            Real factor;
-            electrostatics<Real, U>(
-                (Real)1, qi, qj, d2, beta, d, inv_d, inv_d2, erfc_bd, prefactor, u, qij_inv, factor);
-            Real real_du_dl = 0;
-            if (eps_i != 0 && eps_j != 0) {
-                Real sig_grad;
-                Real eps_grad;
-                lennard_jones<Real, U>(
-                    (Real)1, eps_i, eps_j, sig_i, sig_j, inv_d, inv_d2, qij_inv, factor, erfc_bd, u, prefactor,
-                    sig_grad, eps_grad);
-                if (DP) {
-                    const unsigned long long gs = to_fixed(sig_grad, FX_EXPONENT_SIG);
-                    g_sigi += gs;
-                    g_sigj += gs;
-                    g_epsi += to_fixed(fmul(eps_grad, eps_j), FX_EXPONENT_EPS);
-                    g_epsj += to_fixed(fmul(eps_grad, eps_i), FX_EXPONENT_EPS);
-                }
-                if (DL && ALCH && INTERP) {
-                    real_du_dl = ffma(sig_grad, fadd(dsig_dl_i, dsig_dl_j), real_du_dl);
-                    real_du_dl = ffma(eps_grad, sum_of_products_rn(eps_j, deps_dl_i, eps_i, deps_dl_j), real_du_dl);
-                }
-            }
-            if (DX) {
-                unsigned long long fx, fy, fz, nx, ny, nz;
-                to_fixed_pair(fmul(prefactor, delta_x), FX_EXPONENT, fx, nx);
-                to_fixed_pair(fmul(prefactor, delta_y), FX_EXPONENT, fy, ny);
-                to_fixed_pair(fmul(prefactor, delta_z), FX_EXPONENT, fz, nz);
-                gi_x += fx;
-                gi_y += fy;
-                gi_z += fz;
-                gj_x += nx;
-                gj_y += ny;
-                gj_z += nz;
-            }
-            if (DP) {
-                g_qi += to_fixed(fmul(fmul(qj, inv_d), erfc_bd), FX_EXPONENT);
-                g_qj += to_fixed(fmul(fmul(qi, inv_d), erfc_bd), FX_EXPONENT);
-            }
-            if (DL && ALCH) {
-                real_du_dl = ffma(fmul(delta_w, prefactor), fsub(dw_dl_i, dw_dl_j), real_du_dl);
-                if (INTERP) {
-                    real_du_dl = ffma(fmul(inv_d, erfc_bd), sum_of_products_rn(qj, dq_dl_i, qi, dq_dl_j), real_du_dl);
-                }
-                du_dl += to_fixed(real_du_dl, FX_EXPONENT);
-            }
-            if (U) {
-                energy += to_fixed(u, FX_EXPONENT);
-            }
+            pair_terms<Real, U, DX, DL, DP, INTERP, ALCH>(
+                delta_x, delta_y, delta_z, ALCH ? delta_w : (Real)0, d2, qi, sig_i, eps_i, dw_dl_i, dq_dl_i, dsig_dl_i,
+                deps_dl_i, qj, sig_j, eps_j, dw_dl_j, dq_dl_j, dsig_dl_j, deps_dl_j, beta, gi_x, gi_y, gi_z, g_qi,
+                g_sigi, g_epsi, du_dl, energy, gj_x, gj_y, gj_z, g_qj, g_sigj, g_epsj);
         }
         j = __shfl_sync(FULL_MASK, j, src);
         qj = __shfl_sync(FULL_MASK, qj, src);
@@ -984,11 +1032,204 @@ __device__ __forceinline__ void scaled_pair(
     }
 }
 
+// ---------------------------------------------------------------------------
+// Compacted tile sweep. Of a tile's 32x32 pair slots only about a third lie
+// within the cutoff; the rotating sweep issues the full pair arithmetic for a
+// round whenever any lane's slot is in range. Here a cheap pass first tests
+// every slot (the same 4D d2 as the pair arithmetic, so the same decisions)
+// and records each row's in-range columns as a bit mask; the in-range pairs
+// are then numbered row by row and evaluated 32 at a time, one per lane, so
+// the expensive arithmetic runs with (nearly) all lanes busy. Row
+// contributions are summed over each batch's contiguous runs of equal rows
+// (segmented warp scan) into shared memory; column contributions go to
+// shared memory with atomics. Fixed-point integer sums make the result
+// independent of this order.
+// ---------------------------------------------------------------------------
+struct TileSmem {
+    float4 rpos[TILE], rprm[TILE], rdp[TILE]; // row atoms: x, y, z, w / q, sig, eps, dw_dl / dp_dl
+    float4 cpos[TILE], cprm[TILE], cdp[TILE]; // column atoms
+    unsigned cslot[TILE];                     // column slots (S or more: empty)
+    unsigned long long racc[8][TILE];         // per row: x, y, z, q, sig, eps, du_dl, u
+    unsigned long long cacc[6][TILE];         // per column: x, y, z, q, sig, eps
+};
+
+// Bit position of the (k+1)-th set bit of m (k < popc(m)).
+__device__ __forceinline__ int nth_set_bit(unsigned m, int k) {
+    int pos = 0;
+    for (int w = 16; w > 0; w >>= 1) {
+        const int c = __popc(m & ((1u << w) - 1u));
+        if (k >= c) {
+            k -= c;
+            m >>= w;
+            pos += w;
+        }
+    }
+    return pos;
+}
+
+// Inclusive scan over lanes whose keys are equal (equal keys are contiguous);
+// take[s]: lane - 2^s has the same key.
+__device__ __forceinline__ unsigned long long seg_scan(unsigned long long v, const int lane, const bool (&take)[5]) {
+#pragma unroll
+    for (int s = 0; s < 5; s++) {
+        const unsigned long long up = __shfl_up_sync(FULL_MASK, v, 1 << s);
+        if (take[s]) {
+            v += up;
+        }
+    }
+    return v;
+}
+
+template <typename Real, bool U, bool DX, bool DL, bool DP, bool INTERP, bool ALCH>
+__device__ __forceinline__ void sweep_tile_compact(
+    TileSmem &sm,
+    const int lane,
+    const unsigned S,
+    const unsigned i,
+    const Real ci_x,
+    const Real ci_y,
+    const Real ci_z,
+    const Real ci_w,
+    const Real box_x,
+    const Real box_y,
+    const Real box_z,
+    const Real inv_box_x,
+    const Real inv_box_y,
+    const Real inv_box_z,
+    const Real cutoff_squared,
+    const Real beta) {
+    // pass 1: in-range mask of this lane's row against the 32 columns
+    unsigned mask = 0;
+#pragma unroll 4
+    for (int c = 0; c < TILE; c++) {
+        const float4 pc = sm.cpos[c];
+        const unsigned jc = sm.cslot[c];
+        Real delta_x = min_image(fsub(ci_x, pc.x), box_x, inv_box_x);
+        Real delta_y = min_image(fsub(ci_y, pc.y), box_y, inv_box_y);
+        Real delta_z = min_image(fsub(ci_z, pc.z), box_z, inv_box_z);
+        Real d2 = dist2(delta_x, delta_y, delta_z);
+        if (ALCH) {
+            d2 = add_w2(d2, fsub(ci_w, pc.w));
+        }
+        const bool valid = i < S && jc < S && i < jc;
+        mask |= (valid && d2 < cutoff_squared) ? (1u << c) : 0u;
+    }
+    // number the in-range pairs row by row
+    const int cnt = __popc(mask);
+    int incl = cnt;
+#pragma unroll
+    for (int o = 1; o < TILE; o <<= 1) {
+        const int n = __shfl_up_sync(FULL_MASK, incl, o);
+        if (lane >= o) {
+            incl += n;
+        }
+    }
+    const int excl = incl - cnt;
+    const int total = __shfl_sync(FULL_MASK, incl, TILE - 1);
+    // pass 2: 32 pairs at a time
+    for (int base = 0; base < total; base += TILE) {
+        const int g = base + lane;
+        const bool active = g < total;
+        int L = 0; // owner row: the last lane whose first pair number is <= g
+#pragma unroll
+        for (int step = 16; step > 0; step >>= 1) {
+            const int e = __shfl_sync(FULL_MASK, excl, L + step);
+            if (e <= g) {
+                L += step;
+            }
+        }
+        const int first = __shfl_sync(FULL_MASK, excl, L);
+        const unsigned mL = __shfl_sync(FULL_MASK, mask, L);
+        const int c = active ? nth_set_bit(mL, g - first) : 0;
+        unsigned long long gi_x = 0, gi_y = 0, gi_z = 0, g_qi = 0, g_sigi = 0, g_epsi = 0, du_dl = 0, energy = 0;
+        unsigned long long gj_x = 0, gj_y = 0, gj_z = 0, g_qj = 0, g_sigj = 0, g_epsj = 0;
+        if (active) {
+            const float4 pi = sm.rpos[L], ri = sm.rprm[L];
+            const float4 pj = sm.cpos[c], rj = sm.cprm[c];
+            float4 di = make_float4(0.f, 0.f, 0.f, 0.f), dj = di;
+            if (INTERP) {
+                di = sm.rdp[L];
+                dj = sm.cdp[c];
+            }
+            const Real delta_x = min_image(fsub((Real)pi.x, (Real)pj.x), box_x, inv_box_x);
+            const Real delta_y = min_image(fsub((Real)pi.y, (Real)pj.y), box_y, inv_box_y);
+            const Real delta_z = min_image(fsub((Real)pi.z, (Real)pj.z), box_z, inv_box_z);
+            Real d2 = dist2(delta_x, delta_y, delta_z);
+            Real delta_w = 0;
+            if (ALCH) {
+                delta_w = fsub((Real)pi.w, (Real)pj.w);
+                d2 = add_w2(d2, delta_w);
+            }
+            pair_terms<Real, U, DX, DL, DP, INTERP, ALCH>(
+                delta_x, delta_y, delta_z, delta_w, d2, ri.x, ri.y, ri.z, ri.w, di.x, di.y, di.z, rj.x, rj.y, rj.z,
+                rj.w, dj.x, dj.y, dj.z, beta, gi_x, gi_y, gi_z, g_qi, g_sigi, g_epsi, du_dl, energy, gj_x, gj_y, gj_z,
+                g_qj, g_sigj, g_epsj);
+        }
+        // rows: sums over runs of equal rows; the run's last lane stores
+        const int owner = active ? L : -1;
+        bool take[5];
+#pragma unroll
+        for (int s2 = 0; s2 < 5; s2++) {
+            const int o = __shfl_up_sync(FULL_MASK, owner, 1 << s2);
+            take[s2] = lane >= (1 << s2) && o == owner;
+        }
+        const int next = __shfl_down_sync(FULL_MASK, owner, 1);
+        const bool last = active && (lane == TILE - 1 || next != owner);
+        if (DX) {
+            gi_x = seg_scan(gi_x, lane, take);
+            gi_y = seg_scan(gi_y, lane, take);
+            gi_z = seg_scan(gi_z, lane, take);
+            if (last) {
+                sm.racc[0][L] += gi_x;
+                sm.racc[1][L] += gi_y;
+                sm.racc[2][L] += gi_z;
+            }
+        }
+        if (DP) {
+            g_qi = seg_scan(g_qi, lane, take);
+            g_sigi = seg_scan(g_sigi, lane, take);
+            g_epsi = seg_scan(g_epsi, lane, take);
+            if (last) {
+                sm.racc[3][L] += g_qi;
+                sm.racc[4][L] += g_sigi;
+                sm.racc[5][L] += g_epsi;
+            }
+        }
+        if (DL && ALCH) {
+            du_dl = seg_scan(du_dl, lane, take);
+            if (last) {
+                sm.racc[6][L] += du_dl;
+            }
+        }
+        if (U) {
+            energy = seg_scan(energy, lane, take);
+            if (last) {
+                sm.racc[7][L] += energy;
+            }
+        }
+        // columns: shared-memory atomics (a column can recur within a batch)
+        if (active) {
+            if (DX) {
+                atomicAdd(&sm.cacc[0][c], gj_x);
+                atomicAdd(&sm.cacc[1][c], gj_y);
+                atomicAdd(&sm.cacc[2][c], gj_z);
+            }
+            if (DP) {
+                atomicAdd(&sm.cacc[3][c], g_qj);
+                atomicAdd(&sm.cacc[4][c], g_sigj);
+                atomicAdd(&sm.cacc[5][c], g_epsj);
+            }
+        }
+        __syncwarp();
+    }
+}
+
 // One tile of row block rows (lane = row slot i) against the 32 column slots
 // j, for one window: load, sweep, column atomics. Row accumulators are
 // returned to the caller.
-template <typename Real, bool U, bool DX, bool DL, bool DP, bool INTERP>
+template <typename Real, bool U, bool DX, bool DL, bool DP, bool INTERP, bool COMPACT = false>
 __device__ __forceinline__ void tile_pass(
+    TileSmem *sm, // COMPACT: this warp's shared staging (accumulators zero on entry and on return)
     const PairArgs &a,
     const int lane,
     const unsigned S,
@@ -1033,6 +1274,75 @@ __device__ __forceinline__ void tile_pass(
     const bool row_alch = pwi.w != 0.f || (INTERP && (dpi.x != 0.f || dpi.y != 0.f || dpi.z != 0.f));
     const bool col_alch = pwj.w != 0.f || (INTERP && (dpj.x != 0.f || dpj.y != 0.f || dpj.z != 0.f));
     const bool alch = __any_sync(FULL_MASK, row_alch || col_alch);
+    if (COMPACT) {
+        sm->rpos[lane] = pwi;
+        sm->rprm[lane] = pri;
+        sm->cpos[lane] = pwj;
+        sm->cprm[lane] = prj;
+        if (INTERP) {
+            sm->rdp[lane] = dpi;
+            sm->cdp[lane] = dpj;
+        }
+        sm->cslot[lane] = col_ok ? j : 0xffffffffu;
+        __syncwarp();
+        if (alch) {
+            sweep_tile_compact<Real, U, DX, DL, DP, INTERP, true>(
+                *sm, lane, S, i_eff, pwi.x, pwi.y, pwi.z, pwi.w, box_x, box_y, box_z, inv_box_x, inv_box_y, inv_box_z,
+                cutoff_squared, beta);
+        } else {
+            sweep_tile_compact<Real, U, DX, DL, DP, INTERP, false>(
+                *sm, lane, S, i_eff, pwi.x, pwi.y, pwi.z, pwi.w, box_x, box_y, box_z, inv_box_x, inv_box_y, inv_box_z,
+                cutoff_squared, beta);
+        }
+        __syncwarp();
+        // this tile's row sums into the caller's row accumulators; column sums out
+        if (DX) {
+            gi_x += sm->racc[0][lane];
+            gi_y += sm->racc[1][lane];
+            gi_z += sm->racc[2][lane];
+            sm->racc[0][lane] = 0;
+            sm->racc[1][lane] = 0;
+            sm->racc[2][lane] = 0;
+        }
+        if (DP) {
+            g_qi += sm->racc[3][lane];
+            g_sigi += sm->racc[4][lane];
+            g_epsi += sm->racc[5][lane];
+            sm->racc[3][lane] = 0;
+            sm->racc[4][lane] = 0;
+            sm->racc[5][lane] = 0;
+        }
+        if (DL) {
+            du_dl += sm->racc[6][lane];
+            sm->racc[6][lane] = 0;
+        }
+        if (U) {
+            energy += sm->racc[7][lane];
+            sm->racc[7][lane] = 0;
+        }
+        if (DX) {
+            if (col_ok) {
+                red_add(acc_out.x + j, sm->cacc[0][lane]);
+                red_add(acc_out.y + j, sm->cacc[1][lane]);
+                red_add(acc_out.z + j, sm->cacc[2][lane]);
+            }
+            sm->cacc[0][lane] = 0;
+            sm->cacc[1][lane] = 0;
+            sm->cacc[2][lane] = 0;
+        }
+        if (DP) {
+            if (col_ok) {
+                red_add(acc_out.q + j, sm->cacc[3][lane]);
+                red_add(acc_out.sig + j, sm->cacc[4][lane]);
+                red_add(acc_out.eps + j, sm->cacc[5][lane]);
+            }
+            sm->cacc[3][lane] = 0;
+            sm->cacc[4][lane] = 0;
+            sm->cacc[5][lane] = 0;
+        }
+        __syncwarp();
+        return;
+    }
     unsigned long long gj_x = 0, gj_y = 0, gj_z = 0, g_qj = 0, g_sigj = 0, g_epsj = 0;
     if (alch) {
         sweep_tile<Real, U, DX, DL, DP, INTERP, true>(
@@ -1133,12 +1443,25 @@ static __global__ void k_dep_tiles(DepArgs a, DevState *state) {
 // MULTI (K > 1 windows): the tile items skip lambda-dependent tiles and add
 // into the shared accumulator block; each (tile, window) unit adds into the
 // window's block; a lambda-dependent scaled pair is evaluated for every window.
-template <typename Real, bool U, bool DX, bool DL, bool DP, bool INTERP, bool MULTI>
+template <typename Real, bool U, bool DX, bool DL, bool DP, bool INTERP, bool MULTI, bool COMPACT = false>
 __global__ void __launch_bounds__(128) k_pair(PairArgs a) {
     if (a.state->error) {
         return;
     }
     const int lane = threadIdx.x & 31;
+    // COMPACT: one TileSmem per warp in dynamic shared memory (4 * sizeof(TileSmem) bytes)
+    extern __shared__ __align__(16) unsigned char k_pair_smem[];
+    TileSmem *sm = nullptr;
+    if (COMPACT) {
+        sm = reinterpret_cast<TileSmem *>(k_pair_smem) + (threadIdx.x >> 5);
+        for (int f = 0; f < 8; f++) {
+            sm->racc[f][lane] = 0;
+        }
+        for (int f = 0; f < 6; f++) {
+            sm->cacc[f][lane] = 0;
+        }
+        __syncwarp();
+    }
     const Real box_x = a.box[0 * 3 + 0];
     const Real box_y = a.box[1 * 3 + 1];
     const Real box_z = a.box[2 * 3 + 2];
@@ -1192,8 +1515,8 @@ __global__ void __launch_bounds__(128) k_pair(PairArgs a) {
             const unsigned j = a.tile_cols[(long long)dt.y * TILE + lane];
             const Accum wk = acc_block(a.acc, a.acc_block, 1 + k);
             unsigned long long wx = 0, wy = 0, wz = 0, wq = 0, ws = 0, we = 0, wl = 0, wu = 0;
-            tile_pass<Real, U, DX, DL, DP, INTERP>(
-                a, lane, S, i, j, k, wk, box_x, box_y, box_z, inv_box_x, inv_box_y, inv_box_z, cutoff_squared, beta,
+            tile_pass<Real, U, DX, DL, DP, INTERP, COMPACT>(
+                sm, a, lane, S, i, j, k, wk, box_x, box_y, box_z, inv_box_x, inv_box_y, inv_box_z, cutoff_squared, beta,
                 wx, wy, wz, wq, ws, we, wl, wu);
             if (i < (unsigned)a.row_end) {
                 flush_row<U, DX, DL, DP>(wk, i, wx, wy, wz, wq, ws, we, wl, wu);
@@ -1210,8 +1533,8 @@ __global__ void __launch_bounds__(128) k_pair(PairArgs a) {
             if (MULTI && __any_sync(FULL_MASK, row_dep || (j < S && a.lamdep[j]))) {
                 continue; // evaluated per window by the (tile, window) units
             }
-            tile_pass<Real, U, DX, DL, DP, INTERP>(
-                a, lane, S, i, j, 0, a.acc, box_x, box_y, box_z, inv_box_x, inv_box_y, inv_box_z, cutoff_squared,
+            tile_pass<Real, U, DX, DL, DP, INTERP, COMPACT>(
+                sm, a, lane, S, i, j, 0, a.acc, box_x, box_y, box_z, inv_box_x, inv_box_y, inv_box_z, cutoff_squared,
                 beta, gi_x, gi_y, gi_z, g_qi, g_sigi, g_epsi, du_dl, energy);
         }
         if (i < (unsigned)a.row_end) {

@@ -38,17 +38,22 @@ template <int I> struct PairKernelTable {
 
 // kernel index: bit3 U, bit2 DU_DX, bit1 DU_DL, bit0 DU_DP (+16 when interpolated),
 // the same flag order as timemachine/cpp/src/nonbonded_all_pairs.cu:374-379.
-template <int I, bool INTERP, bool MULTI> constexpr pair_kernel_t pair_kernel() {
+template <int I, bool INTERP, bool MULTI, bool COMPACT> constexpr pair_kernel_t pair_kernel() {
     return &k_pair<float, PairKernelTable<I>::U, PairKernelTable<I>::DX, PairKernelTable<I>::DL, PairKernelTable<I>::DP,
-                   INTERP, MULTI>;
+                   INTERP, MULTI, COMPACT>;
 }
 template <int... Is> struct KernelList {
-    // single: one lambda window; multi: K > 1 windows sharing lambda-independent tiles
-    static void fill(pair_kernel_t *single, pair_kernel_t *multi, bool interp) {
-        ((single[Is] = interp ? pair_kernel<Is, true, false>() : pair_kernel<Is, false, false>()), ...);
-        ((multi[Is] = interp ? pair_kernel<Is, true, true>() : pair_kernel<Is, false, true>()), ...);
+    // [compact][kidx]; single: one lambda window; multi: K > 1 windows sharing
+    // lambda-independent tiles; compact: the compacted tile sweep
+    static void fill(pair_kernel_t (*single)[16], pair_kernel_t (*multi)[16], bool interp) {
+        ((single[0][Is] = interp ? pair_kernel<Is, true, false, false>() : pair_kernel<Is, false, false, false>()), ...);
+        ((multi[0][Is] = interp ? pair_kernel<Is, true, true, false>() : pair_kernel<Is, false, true, false>()), ...);
+        ((single[1][Is] = interp ? pair_kernel<Is, true, false, true>() : pair_kernel<Is, false, false, true>()), ...);
+        ((multi[1][Is] = interp ? pair_kernel<Is, true, true, true>() : pair_kernel<Is, false, true, true>()), ...);
     }
 };
+// dynamic shared memory of the compacted pair kernel (one TileSmem per warp)
+constexpr size_t COMPACT_SMEM = 4 * sizeof(TileSmem);
 using AllKernels = KernelList<0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 14, 15>;
 
 class NonbondedPotential : public PotentialBase {
@@ -282,6 +287,7 @@ class NonbondedPotential : public PotentialBase {
         c->padding_ = padding_;
         c->hilbert_ = hilbert_;
         c->set_chunk(chunk_);
+        c->compact_ = compact_;
         return c;
     }
 
@@ -305,6 +311,7 @@ class NonbondedPotential : public PotentialBase {
         padding_ = p;
     }
     void disable_hilbert() { hilbert_ = false; }
+    void set_compact(bool on) { compact_ = on; }
 
     int row_end() const { return kind_ == Kind::Group ? NR_ : S_; }
 
@@ -483,11 +490,13 @@ class NonbondedPotential : public PotentialBase {
             a.acc = accum();
             a.dep_tiles = dep_tiles_.p;
             a.state = state_.p;
-            pair_kernel_t k = K > 1 ? kernels_multi_[kidx] : kernels_[kidx];
+            const int ci = compact_ ? 1 : 0;
+            pair_kernel_t k = K > 1 ? kernels_multi_[ci][kidx] : kernels_[ci][kidx];
+            const size_t smem = compact_ ? COMPACT_SMEM : 0;
             if (timing_) {
                 CK(cudaEventRecord(ev_pair_[0], stream));
             }
-            k<<<pair_grid(k), 128, 0, stream>>>(a);
+            k<<<pair_grid(k, smem), 128, smem, stream>>>(a);
             CK(cudaPeekAtLastError());
             if (timing_) {
                 CK(cudaEventRecord(ev_pair_[1], stream));
@@ -550,9 +559,9 @@ class NonbondedPotential : public PotentialBase {
         return c;
     }
 
-    int pair_grid(pair_kernel_t k) {
+    int pair_grid(pair_kernel_t k, size_t smem) {
         int per_sm = 0;
-        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, 128, 0));
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, 128, smem));
         return std::max(1, per_sm) * num_sms();
     }
 
@@ -722,8 +731,9 @@ class NonbondedPotential : public PotentialBase {
     DevBuf<int4> items_;
     DevBuf<int2> dep_tiles_;
     DevBuf<DevState> state_;
-    pair_kernel_t kernels_[16];
-    pair_kernel_t kernels_multi_[16];
+    pair_kernel_t kernels_[2][16];
+    pair_kernel_t kernels_multi_[2][16];
+    bool compact_ = false; // compacted tile sweep (same results as the rotating sweep)
 
     // pair-kernel timing
     bool timing_ = false;
@@ -1149,6 +1159,13 @@ tmnb_status tmnb_potential_disable_hilbert_sort(tmnb_potential *pot) {
         return s;
     }
     return tmb::guarded([&] { as_nb(pot)->disable_hilbert(); });
+}
+
+tmnb_status tmnb_potential_set_pair_schedule(tmnb_potential *pot, int compact) {
+    if (tmnb_status s = check_handle(pot)) {
+        return s;
+    }
+    return tmb::guarded([&] { as_nb(pot)->set_compact(compact != 0); });
 }
 
 tmnb_status tmnb_potential_check_device_error(tmnb_potential *pot, void *stream) {

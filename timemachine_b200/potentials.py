@@ -78,6 +78,10 @@ class Potential:
     def disable_hilbert_sort(self):
         _lib.check(self._lib.tmnb_potential_disable_hilbert_sort(self._h))
 
+    def set_pair_schedule(self, compact=False):
+        """Rotating (default) or compacted tile sweep; identical results."""
+        _lib.check(self._lib.tmnb_potential_set_pair_schedule(self._h, 1 if compact else 0))
+
     def num_params(self):
         return self._lib.tmnb_potential_num_params(self._h)
 
