@@ -68,8 +68,9 @@ def parse():
     ap.add_argument(
         "--profile-mode",
         default="windows",
-        choices=["windows", "single"],
-        help="windows: one 12-window call per step; single: one single-window call per step (cycling lambdas)",
+        choices=["windows", "single", "md"],
+        help="windows: one 12-window call per step; single: one single-window call per step (cycling lambdas); "
+        "md: Langevin steps of the MD workload (graph-replayed)",
     )
     ap.add_argument(
         "--forms",
@@ -82,6 +83,24 @@ def parse():
 
 def run_profile(args, local):
     import torch
+
+    if args.profile_mode == "md":
+        from timemachine_b200 import md
+        from timemachine_b200 import potentials as P
+
+        s = md_system()
+        nb = P.Nonbonded(s.exclusion_idxs, s.scales, s.lambda_plane_idxs, s.lambda_offset_idxs, s.beta, s.cutoff)
+        bps = [
+            P.HarmonicBond(s.bond_idxs).bind(s.bond_params).bound_impl(np.float32),
+            P.HarmonicAngle(s.angle_idxs).bind(s.angle_params).bound_impl(np.float32),
+            nb.bind(s.params).bound_impl(np.float32),
+        ]
+        baro = md.MonteCarloBarostat(s.N, 1.0, MD_TEMPERATURE, md_groups(s), MD_BARO_INTERVAL, SEED + 1)
+        intg = md.LangevinIntegrator(MD_TEMPERATURE, MD_EQ_DT, 1.0, s.masses, SEED)
+        ctx = md.Context(s.x, md_v0(s), s.box, intg, bps, baro)
+        ctx.multiple_steps(np.full(args.profile, MD_LAMBDA))
+        print(json.dumps({"profile_md_steps": args.profile}))
+        return
 
     from timemachine_b200 import potentials as P
 
