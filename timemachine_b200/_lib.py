@@ -97,6 +97,8 @@ def _declare(lib):
     lib.tmnb_pair_list_execute_static.restype = ctypes.c_int
     lib.tmnb_potential_set_pair_schedule.argtypes = [vp, i]
     lib.tmnb_potential_set_pair_schedule.restype = ctypes.c_int
+    lib.tmnb_potential_set_rebuild_mode.argtypes = [vp, i, i]
+    lib.tmnb_potential_set_rebuild_mode.restype = ctypes.c_int
     lib.tmnb_potential_adjoint_device.argtypes = [vp, i, i, vp, vp, vp, d, vp, d, vp, vp, vp]
     lib.tmnb_potential_adjoint_device.restype = ctypes.c_int
     lib.tmnb_batch_create.argtypes = [ctypes.POINTER(vp)]

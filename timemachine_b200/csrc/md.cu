@@ -343,6 +343,15 @@ class Context {
         for (auto &kv : graphs_) {
             cudaGraphExecDestroy(kv.second);
         }
+        for (cudaStream_t s : side_) {
+            cudaStreamDestroy(s);
+        }
+        for (cudaEvent_t e : join_ev_) {
+            cudaEventDestroy(e);
+        }
+        if (fork_ev_) {
+            cudaEventDestroy(fork_ev_);
+        }
         if (stream_) {
             cudaStreamDestroy(stream_);
         }
@@ -397,11 +406,31 @@ class Context {
     }
 
     // One step: forces (+ du_dl) from every potential, then the integrator.
-    void record_step(double lambda, unsigned long long *dl_out) {
-        for (auto &b : bps_) {
-            b->pot->execute_device(
-                N_, b->P, x_.p, b->params.p, box_.p, lambda, du_dx_.p, nullptr, dl_out ? du_dl_buf_.p : nullptr,
-                nullptr, stream_);
+    // With `branch` (graph capture) each potential after the first is recorded
+    // on its own forked stream, so the captured graph runs the potentials
+    // concurrently; they all add into du_dx / du_dl with integer atomics, so
+    // the sums do not depend on the order.
+    void record_step(double lambda, unsigned long long *dl_out, bool branch = false) {
+        const size_t n = bps_.size();
+        const bool fork = branch && n > 1;
+        if (fork) {
+            ensure_branches(n - 1);
+            CK(cudaEventRecord(fork_ev_, stream_));
+        }
+        for (size_t k = 0; k < n; k++) {
+            cudaStream_t s = stream_;
+            if (fork && k > 0) {
+                s = side_[k - 1];
+                CK(cudaStreamWaitEvent(s, fork_ev_, 0));
+            }
+            BoundPot &b = *bps_[k];
+            b.pot->execute_device(
+                N_, b.P, x_.p, b.params.p, box_.p, lambda, du_dx_.p, nullptr, dl_out ? du_dl_buf_.p : nullptr,
+                nullptr, s);
+            if (fork && k > 0) {
+                CK(cudaEventRecord(join_ev_[k - 1], s));
+                CK(cudaStreamWaitEvent(stream_, join_ev_[k - 1], 0));
+            }
         }
         if (dl_out) {
             k_reduce_dl<<<1, 1024, 0, stream_>>>(N_, du_dl_buf_.p, dl_out, st_.p);
@@ -440,10 +469,13 @@ class Context {
             return it->second;
         }
         cudaGraph_t g;
+        if (kind == 0 && bps_.size() > 1) {
+            ensure_branches(bps_.size() - 1); // created outside the capture
+        }
         CK(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeRelaxed));
         try {
             if (kind == 0) {
-                record_step(lambda, dl_out);
+                record_step(lambda, dl_out, true);
             } else {
                 record_barostat(lambda);
             }
@@ -624,6 +656,21 @@ class Context {
         }
     }
 
+    // Streams and events of the forked potential branches of a captured step.
+    void ensure_branches(size_t n) {
+        if (!fork_ev_) {
+            CK(cudaEventCreateWithFlags(&fork_ev_, cudaEventDisableTiming));
+        }
+        while (side_.size() < n) {
+            cudaStream_t s;
+            CK(cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking));
+            side_.push_back(s);
+            cudaEvent_t e;
+            CK(cudaEventCreateWithFlags(&e, cudaEventDisableTiming));
+            join_ev_.push_back(e);
+        }
+    }
+
     void store_frame(int frame, double *x_out_host, double *box_out_host) {
         CK(cudaMemcpyAsync(
             x_out_host + (size_t)frame * N_ * 3, x_.p, 3 * (size_t)N_ * sizeof(double), cudaMemcpyDeviceToHost, stream_));
@@ -641,6 +688,9 @@ class Context {
     std::vector<std::unique_ptr<BoundPot>> bps_;
     cudaStream_t stream_ = nullptr;
     std::map<std::tuple<int, double, const void *>, cudaGraphExec_t> graphs_;
+    std::vector<cudaStream_t> side_;
+    std::vector<cudaEvent_t> join_ev_;
+    cudaEvent_t fork_ev_ = nullptr;
 
     bool has_baro_ = false;
     int baro_interval_ = 0;

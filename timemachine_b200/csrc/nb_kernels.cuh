@@ -41,11 +41,15 @@ struct DevState {
     unsigned total_tiles; // tiles produced by the last rebuild
     int rebuilds;         // number of rebuilds performed (diagnostics)
     int n_dep;            // lambda-dependent tiles listed by k_dep_tiles (multi-window calls)
+    unsigned prep_done;   // completion counter of k_check_prepare (graph-conditional rebuilds)
+    unsigned bar_count;   // grid barrier of k_rebuild: arrivals in the current phase
+    unsigned bar_gen;     // grid barrier of k_rebuild: completed phases
 };
 
 // Error codes written into DevState::error (mirrored in include/tmnb.h).
 constexpr int DEV_ERR_NONORTHO_BOX = 3;
 constexpr int DEV_ERR_BOX_TOO_SMALL = 4;
+constexpr int DEV_ERR_BARRIER_TIMEOUT = 6; // a grid barrier gave up waiting (bounded spin)
 
 // Up to this many lambda windows are evaluated together (one launch sequence).
 constexpr int MAX_WINDOWS = TMNB_MAX_WINDOWS;
@@ -122,11 +126,14 @@ static __global__ void k_check_prepare(
     const unsigned *__restrict__ perm, // [S] slot -> atom
     const double *__restrict__ nb_x,   // [N,3] coordinates at the last rebuild (nullptr: no neighbour list)
     const double *__restrict__ nb_box, // [9]
-    DevState *state) {
+    DevState *state,
+    const int set_cond = 0,                // 1: publish the rebuild decision to `cond`
+    const cudaGraphConditionalHandle cond = 0) {
     const int tid = blockIdx.x * blockDim.x + threadIdx.x;
     if (tid == 0) {
         state->next_item = 0;
         state->n_dep = 0;
+        state->bar_count = 0; // no k_rebuild of this state runs concurrently (stream order)
         if (nb_x != nullptr) {
             // Orthorhombic box whose every edge is at least twice cutoff+padding
             // (timemachine/cpp/src/nonbonded_all_pairs.cu:315-329); checked in
@@ -166,6 +173,24 @@ static __global__ void k_check_prepare(
             }
         }
         prepare_slot(a, s, atom);
+    }
+    if (set_cond) {
+        // The last block to finish sets the graph condition that gates the
+        // rebuild chain (keys, scan, scatter, bounds, tiles): a step that
+        // keeps its list skips those launches entirely. Every thread fences
+        // its own stores to state->rebuild before the block counts itself done.
+        __threadfence();
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            const unsigned prev = atomicAdd(&state->prep_done, 1u);
+            if (prev == gridDim.x - 1) {
+                __threadfence();
+                const int rebuild = *((volatile int *)&state->rebuild);
+                const int error = *((volatile int *)&state->error);
+                cudaGraphSetConditional(cond, (rebuild != 0 && error == 0) ? 1u : 0u);
+                state->prep_done = 0;
+            }
+        }
     }
 }
 
@@ -473,6 +498,8 @@ __device__ __forceinline__ void build_tiles_cta(const TileArgs &a, const int rb,
     __shared__ float4 row_pos[TILE];
     __shared__ unsigned buf[TB_WARPS][2 * TILE];
     __shared__ unsigned rem[TB_WARPS * TILE];
+    __shared__ int cand[TB_WARPS * 32]; // column blocks of the current window that pass the box test
+    __shared__ int warp_pass[TB_WARPS];
     __shared__ int tile_count;
     __shared__ int rem_count;
     __shared__ int is_last;
@@ -484,10 +511,22 @@ __device__ __forceinline__ void build_tiles_cta(const TileArgs &a, const int rb,
     const float iLx = 1.0f / Lx, iLy = 1.0f / Ly, iLz = 1.0f / Lz;
     const float r2 = a.radius * a.radius;
     const float r2_box = (a.radius + 1e-4f) * (a.radius + 1e-4f);
+    const float4 rc = a.bb_ctr[rb];
+    const float4 re = a.bb_ext[rb];
 
+    // Row atoms are imaged next to the row block's centre. When every box
+    // edge satisfies L/2 - extent >= radius, a column atom imaged next to the
+    // centre (once) is at its minimum image from every row atom whenever that
+    // distance is below the radius, so the per-pair test needs no wrapping.
+    const bool shifted = 0.5f * Lx - re.x >= a.radius + 1e-3f && 0.5f * Ly - re.y >= a.radius + 1e-3f &&
+                         0.5f * Lz - re.z >= a.radius + 1e-3f;
     if (threadIdx.x < TILE) {
         const int s = rb * TILE + threadIdx.x;
-        row_pos[threadIdx.x] = s < a.row_end ? a.posw[s] : make_float4(0.f, 0.f, 0.f, 0.f);
+        float4 p = s < a.row_end ? a.posw[s] : make_float4(rc.x, rc.y, rc.z, 0.f);
+        p.x = rc.x + wrap_delta(p.x - rc.x, Lx, iLx);
+        p.y = rc.y + wrap_delta(p.y - rc.y, Ly, iLy);
+        p.z = rc.z + wrap_delta(p.z - rc.z, Lz, iLz);
+        row_pos[threadIdx.x] = p;
     }
     if (threadIdx.x == 0) {
         tile_count = 0;
@@ -495,14 +534,19 @@ __device__ __forceinline__ void build_tiles_cta(const TileArgs &a, const int rb,
     }
     __syncthreads();
     const int row_n = min(TILE, a.row_end - rb * TILE);
-    const float4 rc = a.bb_ctr[rb];
-    const float4 re = a.bb_ext[rb];
     const long long base_tile = tile_base(a, rb);
     const unsigned lane_lt = (1u << lane) - 1;
 
     int count = 0; // atoms in this warp's buffer
-    for (int cbase = (a.group ? a.cb_first : rb) + warp * TILE; cbase < a.RB; cbase += TB_WARPS * TILE) {
-        const int cb = cbase + lane;
+    // Column blocks in windows of one block per thread: the box test of the
+    // window compacts the passing blocks in index order, then each warp takes
+    // an equal contiguous share of them. Passing blocks cluster at nearby
+    // indices, so a fixed split of the window by index would leave most warps
+    // idle; contiguous shares keep each warp's tiles spatially compact (the
+    // slot order is a space-filling curve), which the pair kernel's
+    // divergence depends on.
+    for (int wbase = a.group ? a.cb_first : rb; wbase < a.RB; wbase += TB_WARPS * 32) {
+        const int cb = wbase + (int)threadIdx.x;
         bool pass = false;
         if (cb < a.RB) {
             const float4 cc = a.bb_ctr[cb];
@@ -512,34 +556,68 @@ __device__ __forceinline__ void build_tiles_cta(const TileArgs &a, const int rb,
             float dz = fmaxf(0.f, fabsf(wrap_delta(rc.z - cc.z, Lz, iLz)) - re.z - ce.z);
             pass = dx * dx + dy * dy + dz * dz < r2;
         }
-        unsigned blocks = __ballot_sync(FULL_MASK, pass);
-        while (blocks) {
-            const int cb_sel = cbase + __ffs(blocks) - 1;
-            blocks &= blocks - 1;
+        const unsigned m = __ballot_sync(FULL_MASK, pass);
+        if (lane == 0) {
+            warp_pass[warp] = __popc(m);
+        }
+        __syncthreads();
+        int base = 0, nc = 0;
+        for (int w = 0; w < TB_WARPS; w++) {
+            const int c = warp_pass[w];
+            base += w < warp ? c : 0;
+            nc += c;
+        }
+        if (pass) {
+            cand[base + __popc(m & lane_lt)] = cb;
+        }
+        __syncthreads();
+        const int k_end = ((warp + 1) * nc) / TB_WARPS;
+        for (int k = (warp * nc) / TB_WARPS; k < k_end; k++) {
+            const int cb_sel = cand[k];
             const int s = cb_sel * TILE + lane;
             const bool valid = s < S;
             const float4 pj = valid ? a.posw[s] : make_float4(0.f, 0.f, 0.f, 0.f);
             // an atom farther than the radius from the row block's box is
             // farther than the radius from every row atom (widened test,
             // conservative under rounding): skip its per-row test
-            const float bx = fmaxf(0.f, fabsf(wrap_delta(pj.x - rc.x, Lx, iLx)) - re.x);
-            const float by = fmaxf(0.f, fabsf(wrap_delta(pj.y - rc.y, Ly, iLy)) - re.y);
-            const float bz = fmaxf(0.f, fabsf(wrap_delta(pj.z - rc.z, Lz, iLz)) - re.z);
+            const float wx = wrap_delta(pj.x - rc.x, Lx, iLx);
+            const float wy = wrap_delta(pj.y - rc.y, Ly, iLy);
+            const float wz = wrap_delta(pj.z - rc.z, Lz, iLz);
+            const float bx = fmaxf(0.f, fabsf(wx) - re.x);
+            const float by = fmaxf(0.f, fabsf(wy) - re.y);
+            const float bz = fmaxf(0.f, fabsf(wz) - re.z);
             const bool need = valid && s >= a.col_begin && bx * bx + by * by + bz * bz < r2_box;
             bool hit = false;
             if (__any_sync(FULL_MASK, need)) {
-                // rows in groups of 8 (independent tests, then one vote)
-                for (int r0 = 0; r0 < row_n; r0 += 8) {
+                if (shifted) {
+                    const float qx = rc.x + wx, qy = rc.y + wy, qz = rc.z + wz;
+                    for (int r0 = 0; r0 < row_n; r0 += 8) {
 #pragma unroll
-                    for (int r = r0; r < r0 + 8; r++) {
-                        const float4 pi = row_pos[r]; // rows past row_n hold zeros and are masked below
-                        const float dx = wrap_delta(pi.x - pj.x, Lx, iLx);
-                        const float dy = wrap_delta(pi.y - pj.y, Ly, iLy);
-                        const float dz = wrap_delta(pi.z - pj.z, Lz, iLz);
-                        hit |= (r < row_n) && (dx * dx + dy * dy + dz * dz < r2);
+                        for (int r = r0; r < r0 + 8; r++) {
+                            const float4 pi = row_pos[r]; // rows past row_n sit at the centre and are masked below
+                            const float dx = pi.x - qx;
+                            const float dy = pi.y - qy;
+                            const float dz = pi.z - qz;
+                            hit |= (r < row_n) && (dx * dx + dy * dy + dz * dz < r2);
+                        }
+                        if (__all_sync(FULL_MASK, hit || !need)) {
+                            break;
+                        }
                     }
-                    if (__all_sync(FULL_MASK, hit || !need)) {
-                        break;
+                } else {
+                    // rows in groups of 8 (independent tests, then one vote)
+                    for (int r0 = 0; r0 < row_n; r0 += 8) {
+#pragma unroll
+                        for (int r = r0; r < r0 + 8; r++) {
+                            const float4 pi = row_pos[r];
+                            const float dx = wrap_delta(pi.x - pj.x, Lx, iLx);
+                            const float dy = wrap_delta(pi.y - pj.y, Ly, iLy);
+                            const float dz = wrap_delta(pi.z - pj.z, Lz, iLz);
+                            hit |= (r < row_n) && (dx * dx + dy * dy + dz * dz < r2);
+                        }
+                        if (__all_sync(FULL_MASK, hit || !need)) {
+                            break;
+                        }
                     }
                 }
             }
@@ -563,8 +641,9 @@ __device__ __forceinline__ void build_tiles_cta(const TileArgs &a, const int rb,
                 count -= TILE;
             }
         }
+        __syncthreads(); // cand / warp_pass are rewritten by the next window
     }
-    // merge the partial buffers of the four warps
+    // merge the partial buffers of the warps
     int off = 0;
     if (lane == 0) {
         off = atomicAdd(&rem_count, count);
@@ -656,6 +735,100 @@ static __global__ void __launch_bounds__(TB_WARPS * 32) k_build_tiles(TileArgs a
 
 // Clears the rebuild flag when no neighbour list exists (pair lists only).
 static __global__ void k_clear_rebuild(DevState *state) { state->rebuild = 0; }
+
+// ---------------------------------------------------------------------------
+// The whole rebuild (sort keys, cell scan, scatter + restaging, block bounds,
+// tile build) as one cooperative launch with grid barriers between the
+// phases. A step that keeps its list pays one launch that returns at once
+// instead of five.
+// ---------------------------------------------------------------------------
+constexpr unsigned BARRIER_SPIN_LIMIT = 1u << 22; // x >= 64 ns sleeps: well above any phase
+
+// Grid-wide barrier for a cooperative launch (all blocks co-resident). The
+// wait is bounded: on timeout it records DEV_ERR_BARRIER_TIMEOUT and every
+// block leaves at its next barrier. Returns false once an error is recorded.
+__device__ __forceinline__ bool grid_barrier(DevState *st) {
+    __threadfence();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const unsigned gen = *((volatile unsigned *)&st->bar_gen);
+        __threadfence();
+        if (atomicAdd(&st->bar_count, 1u) == gridDim.x - 1) {
+            atomicExch(&st->bar_count, 0u);
+            __threadfence();
+            atomicAdd(&st->bar_gen, 1u);
+        } else {
+            unsigned it = 0;
+            while (*((volatile unsigned *)&st->bar_gen) == gen) {
+                if (++it > BARRIER_SPIN_LIMIT) {
+                    atomicExch(&st->error, DEV_ERR_BARRIER_TIMEOUT);
+                    break;
+                }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+    return *((volatile int *)&st->error) == 0;
+}
+
+struct RebuildArgs {
+    SortArgs sa;
+    PrepareArgs pa;
+    unsigned *perm;   // [S] slot -> atom
+    int *slot_of;     // [N] atom -> slot (nullptr: not needed)
+    double *nb_x;     // [N,3] coordinates of the rebuild
+    double *nb_box;   // [9]
+    TileArgs ta;      // ta.posw / ta.bb_ctr / ta.bb_ext are the block-bounds buffers too
+};
+
+static __global__ void __launch_bounds__(TB_WARPS * 32) k_rebuild(RebuildArgs r, DevState *state) {
+    if (!state->rebuild || state->error) {
+        return;
+    }
+    const int S = r.sa.S;
+    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
+    const int nth = gridDim.x * blockDim.x;
+    if (r.sa.hilbert) {
+        for (int k = tid; k < S; k += nth) {
+            bin_key(r.sa, k);
+        }
+    }
+    if (!grid_barrier(state)) {
+        return;
+    }
+    if (blockIdx.x == 0) {
+        bin_scan_cta(r.sa, state);
+    }
+    if (!grid_barrier(state)) {
+        return;
+    }
+    if (tid < 9) {
+        r.nb_box[tid] = r.sa.box[tid];
+    }
+    for (int k = tid; k < S; k += nth) {
+        const int atom = set_atom(r.sa, k);
+        const int s = scatter_slot(r.sa, k, r.perm, r.slot_of, r.nb_x);
+        prepare_slot(r.pa, s, atom);
+    }
+    if (!grid_barrier(state)) {
+        return;
+    }
+    {
+        const int warp = tid >> 5;
+        const int n_warps = nth >> 5;
+        for (int rb = warp; rb < r.ta.RB; rb += n_warps) {
+            block_bounds_warp(S, rb, r.sa.box, r.ta.posw, const_cast<float4 *>(r.ta.bb_ctr), const_cast<float4 *>(r.ta.bb_ext));
+        }
+    }
+    if (!grid_barrier(state)) {
+        return;
+    }
+    for (int rb = blockIdx.x; rb < r.ta.n_row_blocks; rb += gridDim.x) {
+        build_tiles_cta(r.ta, rb, state);
+    }
+}
 
 // ---------------------------------------------------------------------------
 // Pair kernel.
@@ -1586,8 +1759,11 @@ __device__ __forceinline__ unsigned long long take(unsigned long long *p) {
 // atoms, so the output updates are coalesced and the slot-ordered
 // accumulators are gathered through slot_of. Only the accumulators of
 // requested outputs are read (the others were never written and stay zero).
-// take = 1 zeroes each accumulator after the read (one window, identity slot
-// order); otherwise the caller zeroes the accumulator blocks after this kernel.
+// take = 1 zeroes each accumulator after the read (one window: every slot is
+// read by exactly one thread); otherwise the caller zeroes the accumulator
+// blocks after this kernel. Outputs are added with integer atomics, so other
+// potentials may accumulate into the same buffers concurrently (the sums are
+// order-independent).
 static __global__ void k_finalize(FinalizeArgs a) {
     const bool ok = a.state->error == 0;
     const bool multi = a.K > 1;
@@ -1609,9 +1785,9 @@ static __global__ void k_finalize(FinalizeArgs a) {
             const unsigned long long vx = get(c.x), vy = get(c.y), vz = get(c.z);
             if (ok) {
                 unsigned long long *out = a.du_dx + a.stride_x * k + 3 * (size_t)atom;
-                out[0] += vx;
-                out[1] += vy;
-                out[2] += vz;
+                atomicAdd(out + 0, vx);
+                atomicAdd(out + 1, vy);
+                atomicAdd(out + 2, vz);
             }
         }
         if (a.du_dp) {
@@ -1630,10 +1806,10 @@ static __global__ void k_finalize(FinalizeArgs a) {
                         const double f = a.lambdas[k];
                         unsigned long long lo = interp_part(1 - f, v0[d], ex[d]) + interp_part(1 - f, v1[d], ex[d]);
                         unsigned long long hi = interp_part(f, v0[d], ex[d]) + interp_part(f, v1[d], ex[d]);
-                        out[3 * (size_t)atom + d] += lo;
-                        out[3 * ((size_t)a.N + atom) + d] += hi;
+                        atomicAdd(out + 3 * (size_t)atom + d, lo);
+                        atomicAdd(out + 3 * ((size_t)a.N + atom) + d, hi);
                     } else {
-                        out[3 * (size_t)atom + d] += v0[d] + v1[d];
+                        atomicAdd(out + 3 * (size_t)atom + d, v0[d] + v1[d]);
                     }
                 }
             }
@@ -1641,13 +1817,13 @@ static __global__ void k_finalize(FinalizeArgs a) {
         if (a.u) {
             const unsigned long long vu = get(c.u);
             if (ok) {
-                a.u[a.stride_n * k + atom] += vu;
+                atomicAdd(a.u + a.stride_n * k + atom, vu);
             }
         }
         if (a.du_dl) {
             const unsigned long long vl = get(c.dl);
             if (ok) {
-                a.du_dl[a.stride_n * k + atom] += vl;
+                atomicAdd(a.du_dl + a.stride_n * k + atom, vl);
             }
         }
     }

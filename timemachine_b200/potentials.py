@@ -82,6 +82,12 @@ class Potential:
         """Rotating (default) or compacted tile sweep; identical results."""
         _lib.check(self._lib.tmnb_potential_set_pair_schedule(self._h, 1 if compact else 0))
 
+    def set_rebuild_mode(self, fused=False, conditional=False):
+        """Neighbour-list rebuild as five kernels (default) or one cooperative
+        launch (fused); under stream capture as plain nodes (default) or a
+        conditional graph node. Identical results in every mode."""
+        _lib.check(self._lib.tmnb_potential_set_rebuild_mode(self._h, 1 if fused else 0, 1 if conditional else 0))
+
     def num_params(self):
         return self._lib.tmnb_potential_num_params(self._h)
 
