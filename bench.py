@@ -68,9 +68,10 @@ def parse():
     ap.add_argument(
         "--profile-mode",
         default="windows",
-        choices=["windows", "single", "md"],
+        choices=["windows", "single", "md", "batch", "grad"],
         help="windows: one 12-window call per step; single: one single-window call per step (cycling lambdas); "
-        "md: Langevin steps of the MD workload (graph-replayed)",
+        "md: Langevin steps of the MD workload (graph-replayed); batch: evaluations of 64 replicas (the first 8 "
+        "systems of the batching mix x 8 windows); grad: loss gradients of the differentiation workload on 4 frames",
     )
     ap.add_argument(
         "--forms",
@@ -100,6 +101,26 @@ def run_profile(args, local):
         ctx = md.Context(s.x, md_v0(s), s.box, intg, bps, baro)
         ctx.multiple_steps(np.full(args.profile, MD_LAMBDA))
         print(json.dumps({"profile_md_steps": args.profile}))
+        return
+    if args.profile_mode == "batch":
+        from timemachine_b200.batch import ReplicaBatch
+
+        systems, lambdas = batch_workload()
+        b = ReplicaBatch()
+        for k, s in enumerate(systems[:8]):
+            for w, lam in enumerate(lambdas):
+                b.add(s, lam, seed=1000 * k + w)
+        for _ in range(args.profile):
+            b.evaluate()
+        b.synchronize()
+        print(json.dumps({"profile_batch_evaluations": args.profile, "replicas": len(b)}))
+        return
+    if args.profile_mode == "grad":
+        loss_and_grads = grad_workload(n_frames=4)[0]
+        for _ in range(args.profile):
+            loss_and_grads()
+        torch.cuda.synchronize()
+        print(json.dumps({"profile_loss_gradients": args.profile, "frames": 4}))
         return
 
     from timemachine_b200 import potentials as P
@@ -774,17 +795,14 @@ GRAD_FRAMES = 32
 GRAD_LAMBDA = 0.5
 
 
-def run_grad_form():
-    """Differentiation form: 1,650 waters + a 50-atom ligand; 32 frames
-    (Gaussian perturbations of 0.01 nm); targets = forces with the ligand
-    parameters perturbed by 5 %; loss = mean squared force error + 0.1 du_dl^2
-    at lambda 0.5; gradients with respect to the ligand's charges, sigmas,
-    sqrt(eps) and w offsets through the adjoint kernel. Checked against the
-    FP64 double-backward oracle and FP64 central differences (step 1e-4) on
-    one frame."""
+def grad_workload(n_frames=GRAD_FRAMES):
+    """The differentiation workload: (loss_and_grads, parts). loss_and_grads()
+    runs the forward kernels and the adjoint kernel over all frames and returns
+    (loss, d/dparams, d/doffsets); parts holds the system, the potential, the
+    frames (host and device), the ligand atoms, the box, the target forces and
+    the base w offsets."""
     import torch
 
-    from oracle.nonbonded_oracle import Oracle, candidate_pairs, force_vjp_oracle
     from timemachine_b200 import potentials as P
     from timemachine_b200 import testsystems
     from timemachine_b200.adjoint import nonbonded_forces
@@ -792,7 +810,7 @@ def run_grad_form():
     s = testsystems.build_system(1650, (1650 * testsystems.WATER_VOLUME) ** (1 / 3), seed=SEED + 3, n_ligand=50)
     lig = np.flatnonzero(s.lambda_offset_idxs != 0)
     rng = np.random.default_rng(SEED + 4)
-    frames = [s.x + rng.normal(scale=0.01, size=s.x.shape) for _ in range(GRAD_FRAMES)]
+    frames = [s.x + rng.normal(scale=0.01, size=s.x.shape) for _ in range(n_frames)]
     impl = P.Nonbonded(s.exclusion_idxs, s.scales, s.lambda_plane_idxs, s.lambda_offset_idxs, s.beta, s.cutoff)
     impl = impl.unbound_impl(np.float32)
     p_target = s.params.copy()
@@ -817,6 +835,25 @@ def run_grad_form():
         loss.backward()
         return loss, params.grad, w_off.grad
 
+    return loss_and_grads, dict(s=s, impl=impl, frames=frames, lig=lig, xs=xs, box=box, targets=targets, w0=w0)
+
+
+def run_grad_form():
+    """Differentiation form: 1,650 waters + a 50-atom ligand; 32 frames
+    (Gaussian perturbations of 0.01 nm); targets = forces with the ligand
+    parameters perturbed by 5 %; loss = mean squared force error + 0.1 du_dl^2
+    at lambda 0.5; gradients with respect to the ligand's charges, sigmas,
+    sqrt(eps) and w offsets through the adjoint kernel. Checked against the
+    FP64 double-backward oracle and FP64 central differences (step 1e-4) on
+    one frame."""
+    import torch
+
+    from oracle.nonbonded_oracle import Oracle, candidate_pairs, force_vjp_oracle
+    from timemachine_b200.adjoint import nonbonded_forces
+
+    loss_and_grads, parts = grad_workload()
+    s, impl, frames, lig = parts["s"], parts["impl"], parts["frames"], parts["lig"]
+    xs, box, targets, w0 = parts["xs"], parts["box"], parts["targets"], parts["w0"]
     loss_and_grads()
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)

@@ -40,6 +40,7 @@ struct AdjointArgs {
     const unsigned *perm; // [S] slot -> atom
     const unsigned *tile_cols;
     const int4 *items;
+    int chunk;            // tiles per work item (item.z <= chunk)
     int M;
     const int *pair_idxs; // [M,2] atoms
     const double *scales; // [M,2]
@@ -51,38 +52,57 @@ struct AdjointArgs {
     DevState *state;
 };
 
+// What the pair terms need of one atom: coordinates, parameters (q, sigma/2,
+// sqrt eps), the upstream gradient of its du_dx, and its lambda plane/offset.
+struct AdjAtom {
+    double x[3];
+    double p[3];
+    double g[3];
+    int plane;
+    int offset;
+};
+
+__device__ __forceinline__ AdjAtom load_adj_atom(const AdjointArgs &a, int atom) {
+    AdjAtom t;
+    for (int d = 0; d < 3; d++) {
+        t.x[d] = a.x[3 * (size_t)atom + d];
+        t.p[d] = a.p[3 * (size_t)atom + d];
+        t.g[d] = a.g_dx[3 * (size_t)atom + d];
+    }
+    t.plane = a.plane[atom];
+    t.offset = a.offset[atom];
+    return t;
+}
+
 // Gradient contributions of one pair: to atom i (q, sig, eps, off) and atom j.
 struct PairGrad {
     double qi, si, ei, wi;
     double qj, sj, ej, wj;
 };
 
-__device__ __forceinline__ PairGrad adjoint_pair(const AdjointArgs &a, int ai, int aj, double cs, double ls, double sign) {
+__device__ __forceinline__ PairGrad
+adjoint_pair(const AdjointArgs &a, const AdjAtom &I, const AdjAtom &J, double cs, double ls, double sign) {
     PairGrad out = {0, 0, 0, 0, 0, 0, 0, 0};
-    const double *xi = a.x + 3 * (size_t)ai;
-    const double *xj = a.x + 3 * (size_t)aj;
     double r[3];
     double r2 = 0;
     for (int d = 0; d < 3; d++) {
         const double L = a.box[4 * d];
-        double v = xi[d] - xj[d];
+        double v = I.x[d] - J.x[d];
         v -= L * floor(v / L + 0.5);
         r[d] = v;
         r2 += v * v;
     }
     const double c = a.cutoff;
-    const double doff = (double)(a.offset[ai] - a.offset[aj]);
-    const double dw = c * ((a.plane[ai] - a.plane[aj]) + doff * a.lambda);
+    const double doff = (double)(I.offset - J.offset);
+    const double dw = c * ((I.plane - J.plane) + doff * a.lambda);
     const double d2 = r2 + dw * dw;
     if (!(d2 < c * c)) {
         return out;
     }
     const double d = sqrt(d2);
     const double inv_d = 1.0 / d;
-    const double *pi = a.p + 3 * (size_t)ai;
-    const double *pj = a.p + 3 * (size_t)aj;
-    const double qi = pi[0], si = pi[1], ei = pi[2];
-    const double qj = pj[0], sj = pj[1], ej = pj[2];
+    const double qi = I.p[0], si = I.p[1], ei = I.p[2];
+    const double qj = J.p[0], sj = J.p[1], ej = J.p[2];
 
     // electrostatics: E = erfc(beta d)/d
     const double bd = a.beta * d;
@@ -111,9 +131,8 @@ __device__ __forceinline__ PairGrad adjoint_pair(const AdjointArgs &a, int ai, i
     }
     h *= sign;
     hp *= sign;
-    const double *Gi = a.g_dx + 3 * (size_t)ai;
-    const double *Gj = a.g_dx + 3 * (size_t)aj;
-    const double B = (Gi[0] - Gj[0]) * r[0] + (Gi[1] - Gj[1]) * r[1] + (Gi[2] - Gj[2]) * r[2] + a.g_dl * dw * c * doff;
+    const double B = (I.g[0] - J.g[0]) * r[0] + (I.g[1] - J.g[1]) * r[1] + (I.g[2] - J.g[2]) * r[2] +
+                     a.g_dl * dw * c * doff;
     out.qi = sign * B * dh_qi;
     out.qj = sign * B * dh_qj;
     out.si = sign * B * dh_s;
@@ -133,66 +152,122 @@ __device__ __forceinline__ void adjoint_add(const AdjointArgs &a, int atom, doub
     atomicAdd(a.grad_w + atom, w);
 }
 
-// One warp per tile work item (lane = row slot), then one lane per scaled
-// pair; dynamic work counter state->next_item (reset by k_check_prepare).
-static __global__ void __launch_bounds__(128) k_adjoint(AdjointArgs a) {
+constexpr int ADJ_WARPS = 4;
+
+// A tile's 32 column atoms, structure-of-arrays in shared memory (one per
+// warp), and their gradient accumulators.
+struct AdjTileSmem {
+    double x[3][TILE];
+    double p[3][TILE];
+    double g[3][TILE];
+    int plane[TILE];
+    int offset[TILE];
+    unsigned slot[TILE];
+    int atom[TILE];
+    double acc[4][TILE];
+};
+
+// One warp per tile (lane = row slot). The tile's column atoms are staged in
+// shared memory; in round r lane l pairs its row atom with column (l + r) mod
+// 32, so the 32 lanes of a round touch 32 distinct columns and add into their
+// shared-memory accumulators without conflicts. Each tile ends with one FP64
+// atomic per (atom, output) for its rows and its columns. The scaled pairs
+// follow as one lane per pair. Dynamic work counter state->next_item (reset
+// by k_check_prepare).
+static __global__ void __launch_bounds__(ADJ_WARPS * 32) k_adjoint(AdjointArgs a) {
+    __shared__ AdjTileSmem smem[ADJ_WARPS];
     if (a.state->error) {
         return;
     }
+    AdjTileSmem &sm = smem[threadIdx.x >> 5];
     const int lane = threadIdx.x & 31;
     const unsigned S = (unsigned)a.S;
-    const int n_items = a.tile_cols ? a.state->n_items : 0;
-    const int n_total = n_items + (a.M + TILE - 1) / TILE;
+    const int n_tile_units = a.tile_cols ? a.state->n_items * a.chunk : 0;
+    const int n_total = n_tile_units + (a.M + TILE - 1) / TILE;
     for (;;) {
-        int item = 0;
+        int unit = 0;
         if (lane == 0) {
-            item = atomicAdd(&a.state->next_item, 1);
+            unit = atomicAdd(&a.state->next_item, 1);
         }
-        item = __shfl_sync(FULL_MASK, item, 0);
-        if (item >= n_total) {
+        unit = __shfl_sync(FULL_MASK, unit, 0);
+        if (unit >= n_total) {
             break;
         }
-        if (item >= n_items) {
-            const int pair = (item - n_items) * TILE + lane;
+        if (unit >= n_tile_units) {
+            const int pair = (unit - n_tile_units) * TILE + lane;
             if (pair < a.M) {
                 const int ai = a.pair_idxs[2 * pair], aj = a.pair_idxs[2 * pair + 1];
-                const PairGrad g = adjoint_pair(a, ai, aj, a.scales[2 * pair], a.scales[2 * pair + 1], a.pair_sign);
+                const PairGrad g = adjoint_pair(
+                    a, load_adj_atom(a, ai), load_adj_atom(a, aj), a.scales[2 * pair], a.scales[2 * pair + 1],
+                    a.pair_sign);
                 adjoint_add(a, ai, g.qi, g.si, g.ei, g.wi);
                 adjoint_add(a, aj, g.qj, g.sj, g.ej, g.wj);
             }
             continue;
         }
-        const int4 it = a.items[item];
+        const int4 it = a.items[unit / a.chunk];
+        const int t = unit - (unit / a.chunk) * a.chunk;
+        if (t >= it.z) {
+            continue; // warp-uniform
+        }
+        const long long tile = (long long)it.y + t;
         const unsigned i = (unsigned)(it.x * TILE + lane);
         const int ai = i < S ? (int)a.perm[i] : -1;
-        double rq = 0, rs = 0, re = 0, rw = 0;
-        for (int t = 0; t < it.z; t++) {
-            const long long tile = (long long)it.y + t;
-            for (int col = 0; col < TILE; col++) {
-                const unsigned j = a.tile_cols[tile * TILE + col];
-                PairGrad g = {0, 0, 0, 0, 0, 0, 0, 0};
-                if (ai >= 0 && j < S && i < j) {
-                    g = adjoint_pair(a, ai, (int)a.perm[j], 1.0, 1.0, 1.0);
+        AdjAtom I = {};
+        if (ai >= 0) {
+            I = load_adj_atom(a, ai);
+        }
+        {
+            const unsigned j = a.tile_cols[tile * TILE + lane];
+            const int aj = j < S ? (int)a.perm[j] : -1;
+            sm.slot[lane] = j;
+            sm.atom[lane] = aj;
+            if (aj >= 0) {
+                const AdjAtom J = load_adj_atom(a, aj);
+                for (int d = 0; d < 3; d++) {
+                    sm.x[d][lane] = J.x[d];
+                    sm.p[d][lane] = J.p[d];
+                    sm.g[d][lane] = J.g[d];
                 }
+                sm.plane[lane] = J.plane;
+                sm.offset[lane] = J.offset;
+            }
+            for (int k = 0; k < 4; k++) {
+                sm.acc[k][lane] = 0.0;
+            }
+        }
+        __syncwarp();
+        double rq = 0, rs = 0, re = 0, rw = 0;
+        for (int r = 0; r < TILE; r++) {
+            const int c = (lane + r) & (TILE - 1);
+            if (ai >= 0 && sm.atom[c] >= 0 && i < sm.slot[c]) {
+                AdjAtom J;
+                for (int d = 0; d < 3; d++) {
+                    J.x[d] = sm.x[d][c];
+                    J.p[d] = sm.p[d][c];
+                    J.g[d] = sm.g[d][c];
+                }
+                J.plane = sm.plane[c];
+                J.offset = sm.offset[c];
+                const PairGrad g = adjoint_pair(a, I, J, 1.0, 1.0, 1.0);
                 rq += g.qi;
                 rs += g.si;
                 re += g.ei;
                 rw += g.wi;
-                // column atom: warp sum, one atomic
-                for (int o = 16; o > 0; o >>= 1) {
-                    g.qj += __shfl_xor_sync(FULL_MASK, g.qj, o);
-                    g.sj += __shfl_xor_sync(FULL_MASK, g.sj, o);
-                    g.ej += __shfl_xor_sync(FULL_MASK, g.ej, o);
-                    g.wj += __shfl_xor_sync(FULL_MASK, g.wj, o);
-                }
-                if (lane == 0 && j < S) {
-                    adjoint_add(a, (int)a.perm[j], g.qj, g.sj, g.ej, g.wj);
-                }
+                sm.acc[0][c] += g.qj;
+                sm.acc[1][c] += g.sj;
+                sm.acc[2][c] += g.ej;
+                sm.acc[3][c] += g.wj;
             }
+            __syncwarp();
         }
         if (ai >= 0) {
             adjoint_add(a, ai, rq, rs, re, rw);
         }
+        if (sm.atom[lane] >= 0) {
+            adjoint_add(a, sm.atom[lane], sm.acc[0][lane], sm.acc[1][lane], sm.acc[2][lane], sm.acc[3][lane]);
+        }
+        __syncwarp();
     }
 }
 

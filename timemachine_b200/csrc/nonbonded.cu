@@ -739,6 +739,7 @@ class NonbondedPotential : public PotentialBase {
         a.perm = perm_.p;
         a.tile_cols = has_nblist_ ? tile_cols_.p : nullptr;
         a.items = items_.p;
+        a.chunk = chunk_;
         a.M = M_;
         a.pair_idxs = pair_idxs_.p;
         a.scales = scales_.p;
@@ -749,8 +750,8 @@ class NonbondedPotential : public PotentialBase {
         a.grad_w = d_grad_w;
         a.state = state_.p;
         int per_sm = 0;
-        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_adjoint, 128, 0));
-        k_adjoint<<<std::max(1, per_sm) * num_sms(), 128, 0, stream>>>(a);
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_adjoint, ADJ_WARPS * 32, 0));
+        k_adjoint<<<std::max(1, per_sm) * num_sms(), ADJ_WARPS * 32, 0, stream>>>(a);
         CK(cudaPeekAtLastError());
     }
 
