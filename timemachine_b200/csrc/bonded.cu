@@ -30,6 +30,7 @@ __global__ void k_harmonic_bond(
     unsigned long long *__restrict__ du_dp,
     unsigned long long *__restrict__ du_dl,
     unsigned long long *__restrict__ u) {
+    grid_dependency_wait();
     const int b = blockIdx.x * blockDim.x + threadIdx.x;
     if (b >= B) {
         return;
@@ -52,6 +53,7 @@ __global__ void k_harmonic_angle(
     unsigned long long *__restrict__ du_dp,
     unsigned long long *__restrict__ du_dl,
     unsigned long long *__restrict__ u) {
+    grid_dependency_wait();
     const int a = blockIdx.x * blockDim.x + threadIdx.x;
     if (a >= A) {
         return;
@@ -113,11 +115,13 @@ class BondedPotential : public PotentialBase {
         const int tpb = 128;
         const int blocks = (T_ + tpb - 1) / tpb;
         if (arity_ == 2) {
-            k_harmonic_bond<float><<<blocks, tpb, 0, stream>>>(
-                T_, d_x, d_p, lambda, mult_.p, off_.p, idxs_.p, d_du_dx, d_du_dp, d_du_dl, d_u);
+            launch_dependent(
+                k_harmonic_bond<float>, dim3(blocks), dim3(tpb), 0, stream, T_, d_x, d_p, lambda, mult_.p, off_.p, idxs_.p,
+                d_du_dx, d_du_dp, d_du_dl, d_u);
         } else {
-            k_harmonic_angle<float><<<blocks, tpb, 0, stream>>>(
-                T_, d_x, d_p, lambda, mult_.p, off_.p, idxs_.p, d_du_dx, d_du_dp, d_du_dl, d_u);
+            launch_dependent(
+                k_harmonic_angle<float>, dim3(blocks), dim3(tpb), 0, stream, T_, d_x, d_p, lambda, mult_.p, off_.p,
+                idxs_.p, d_du_dx, d_du_dp, d_du_dl, d_u);
         }
         CK(cudaPeekAtLastError());
     }

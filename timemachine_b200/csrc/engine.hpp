@@ -9,6 +9,7 @@
 #include <memory>
 #include <stdexcept>
 #include <string>
+#include <utility>
 
 namespace tmb {
 
@@ -25,6 +26,26 @@ inline void cuda_check(cudaError_t e, const char *what) {
     }
 }
 #define CK(call) ::tmb::cuda_check((call), #call)
+
+// Launch with programmatic stream serialization: the kernel's launch may
+// overlap the drain of the previous kernel in the stream, so the kernel must
+// execute griddepcontrol.wait (grid_dependency_wait()) before it reads or
+// writes anything the previous kernel touches.
+template <typename... KArgs, typename... Args>
+inline void launch_dependent(
+    void (*kernel)(KArgs...), dim3 grid, dim3 block, size_t smem, cudaStream_t stream, Args &&...args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = smem;
+    cfg.stream = stream;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = 1;
+    CK(cudaLaunchKernelEx(&cfg, kernel, std::forward<Args>(args)...));
+}
 
 template <typename T> struct DevBuf {
     T *p = nullptr;

@@ -56,6 +56,7 @@ __global__ void k_langevin(
     unsigned long long *__restrict__ du_dx,
     uint2 key,
     MDState *st) {
+    grid_dependency_wait();
     __shared__ unsigned long long s_step;
     if (threadIdx.x == 0) {
         s_step = st->step;
@@ -436,8 +437,9 @@ class Context {
             k_reduce_dl<<<1, 1024, 0, stream_>>>(N_, du_dl_buf_.p, dl_out, st_.p);
         }
         const int tpb = 128;
-        k_langevin<<<(N_ + tpb - 1) / tpb, tpb, 0, stream_>>>(
-            N_, ca_, cbs_.p, ccs_.p, dt_, x_.p, v_.p, du_dx_.p, key_, st_.p);
+        launch_dependent(
+            k_langevin, dim3((N_ + tpb - 1) / tpb), dim3(tpb), 0, stream_, N_, ca_, (const double *)cbs_.p,
+            (const double *)ccs_.p, dt_, x_.p, v_.p, du_dx_.p, key_, st_.p);
         CK(cudaPeekAtLastError());
     }
 

@@ -129,6 +129,7 @@ static __global__ void k_check_prepare(
     DevState *state,
     const int set_cond = 0,                // 1: publish the rebuild decision to `cond`
     const cudaGraphConditionalHandle cond = 0) {
+    grid_dependency_wait();
     const int tid = blockIdx.x * blockDim.x + threadIdx.x;
     if (tid == 0) {
         state->next_item = 0;
@@ -275,6 +276,7 @@ __device__ __forceinline__ void bin_key(const SortArgs &a, int k) {
 }
 
 static __global__ void k_bin_keys(SortArgs a, const DevState *state) {
+    grid_dependency_wait();
     if (!state->rebuild || state->error || !a.hilbert) {
         return;
     }
@@ -344,6 +346,7 @@ __device__ __forceinline__ void bin_scan_cta(const SortArgs &a, DevState *state)
 }
 
 static __global__ void k_bin_scan(SortArgs a, DevState *state) {
+    grid_dependency_wait();
     if (!state->rebuild || state->error) {
         return;
     }
@@ -374,6 +377,7 @@ static __global__ void k_bin_scatter(
     double *__restrict__ nb_x,      // [N,3]
     double *__restrict__ nb_box,    // [9]
     const DevState *state) {
+    grid_dependency_wait();
     if (!state->rebuild || state->error) {
         return;
     }
@@ -444,6 +448,7 @@ static __global__ void k_block_bounds(
     float4 *__restrict__ bb_ctr,
     float4 *__restrict__ bb_ext,
     const DevState *state) {
+    grid_dependency_wait();
     if (!state->rebuild || state->error) {
         return;
     }
@@ -727,6 +732,7 @@ __device__ __forceinline__ void build_tiles_cta(const TileArgs &a, const int rb,
 }
 
 static __global__ void __launch_bounds__(TB_WARPS * 32) k_build_tiles(TileArgs a, DevState *state) {
+    grid_dependency_wait();
     if (!state->rebuild || state->error) {
         return;
     }
@@ -958,16 +964,27 @@ __device__ __forceinline__ void pair_terms(
         }
     }
     if (DX) {
-        unsigned long long fx, fy, fz, nx, ny, nz;
-        to_fixed_pair(fmul(prefactor, delta_x), FX_EXPONENT, fx, nx);
-        to_fixed_pair(fmul(prefactor, delta_y), FX_EXPONENT, fy, ny);
-        to_fixed_pair(fmul(prefactor, delta_z), FX_EXPONENT, fz, nz);
+        // The column's term llrint(-y) equals -llrint(y) (round-half-even is
+        // odd) except where the conversion saturates (|y| >= 2^63) or y is NaN;
+        // those lanes add the difference afterwards.
+        const float ex = static_cast<float>(FX_EXPONENT);
+        const float yx = fmul(fmul(prefactor, delta_x), ex);
+        const float yy = fmul(fmul(prefactor, delta_y), ex);
+        const float yz = fmul(fmul(prefactor, delta_z), ex);
+        const unsigned long long fx = static_cast<unsigned long long>(llrintf(yx));
+        const unsigned long long fy = static_cast<unsigned long long>(llrintf(yy));
+        const unsigned long long fz = static_cast<unsigned long long>(llrintf(yz));
         gi_x += fx;
         gi_y += fy;
         gi_z += fz;
-        gj_x += nx;
-        gj_y += ny;
-        gj_z += nz;
+        gj_x -= fx;
+        gj_y -= fy;
+        gj_z -= fz;
+        if (!(fabsf(yx) < 0x1p63f) || !(fabsf(yy) < 0x1p63f) || !(fabsf(yz) < 0x1p63f)) {
+            gj_x += static_cast<unsigned long long>(llrintf(-yx)) + fx;
+            gj_y += static_cast<unsigned long long>(llrintf(-yy)) + fy;
+            gj_z += static_cast<unsigned long long>(llrintf(-yz)) + fz;
+        }
     }
     if (DP) {
         g_qi += to_fixed(fmul(fmul(qj, inv_d), erfc_bd), FX_EXPONENT);
@@ -991,7 +1008,7 @@ __device__ __forceinline__ void pair_terms(
 // timemachine/cpp/src/kernels/k_nonbonded.cuh:424-546; the column
 // contribution of du_dx is the exact negation of the row contribution
 // (llrint is odd under round-half-even), so it is converted once.
-template <typename Real, bool U, bool DX, bool DL, bool DP, bool INTERP, bool ALCH>
+template <typename Real, bool U, bool DX, bool DL, bool DP, bool INTERP, bool ALCH, bool CHECK>
 __device__ __forceinline__ void sweep_tile(
     const int lane,
     const unsigned S,
@@ -1056,14 +1073,20 @@ __device__ __forceinline__ void sweep_tile(
             delta_w = fsub(ci_w, cj_w);
             d2 = add_w2(d2, delta_w);
         }
-        const bool valid = i < S && j < S && i < j;
+        // CHECK: the tile holds atoms of the row block itself, so i < j decides
+        // which lane evaluates each pair. Otherwise every column slot exceeds
+        // every row slot, and padding rows/columns carry NaN coordinates,
+        // which fail the cutoff test.
+        const bool valid = !CHECK || (i < S && j < S && i < j);
         if (valid && d2 < cutoff_squared) {
             pair_terms<Real, U, DX, DL, DP, INTERP, ALCH>(
                 delta_x, delta_y, delta_z, ALCH ? delta_w : (Real)0, d2, qi, sig_i, eps_i, dw_dl_i, dq_dl_i, dsig_dl_i,
                 deps_dl_i, qj, sig_j, eps_j, dw_dl_j, dq_dl_j, dsig_dl_j, deps_dl_j, beta, gi_x, gi_y, gi_z, g_qi,
                 g_sigi, g_epsi, du_dl, energy, gj_x, gj_y, gj_z, g_qj, g_sigj, g_epsj);
         }
-        j = __shfl_sync(FULL_MASK, j, src);
+        if (CHECK) {
+            j = __shfl_sync(FULL_MASK, j, src);
+        }
         qj = __shfl_sync(FULL_MASK, qj, src);
         eps_j = __shfl_sync(FULL_MASK, eps_j, src);
         sig_j = __shfl_sync(FULL_MASK, sig_j, src);
@@ -1430,9 +1453,11 @@ __device__ __forceinline__ void tile_pass(
     const bool row_ok = i < (unsigned)a.row_end;
     const bool col_ok = j < S;
     const unsigned i_eff = row_ok ? i : 0xffffffffu; // invalid rows pair with nothing
-    const float4 pwi = row_ok ? a.posw[wo + i] : make_float4(0.f, 0.f, 0.f, 0.f);
+    // padding rows and columns: NaN coordinates (no pair passes the cutoff test), w = 0
+    const float nan = __int_as_float(0x7fffffff);
+    const float4 pwi = row_ok ? a.posw[wo + i] : make_float4(nan, nan, nan, 0.f);
     const float4 pri = row_ok ? a.prm[wo + i] : make_float4(0.f, 0.f, 0.f, 0.f);
-    const float4 pwj = col_ok ? a.posw[wo + j] : make_float4(0.f, 0.f, 0.f, 0.f);
+    const float4 pwj = col_ok ? a.posw[wo + j] : make_float4(nan, nan, nan, 0.f);
     const float4 prj = col_ok ? a.prm[wo + j] : make_float4(0.f, 0.f, 0.f, 0.f);
     float4 dpi = make_float4(0.f, 0.f, 0.f, 0.f);
     float4 dpj = dpi;
@@ -1517,19 +1542,32 @@ __device__ __forceinline__ void tile_pass(
         return;
     }
     unsigned long long gj_x = 0, gj_y = 0, gj_z = 0, g_qj = 0, g_sigj = 0, g_epsj = 0;
+    // Only a tile holding atoms of the row block itself (the diagonal block)
+    // needs the per-pair i < j test. The diagonal block is the first
+    // candidate of the list builder's first warp, so a full one fills a tile
+    // of its own; the flag is computed per tile either way.
+    const unsigned row_first = i & ~(unsigned)(TILE - 1);
+    const bool check = __any_sync(FULL_MASK, col_ok && j < row_first + TILE);
+#define TMB_SWEEP(ALCH_, CHECK_)                                                                                      \
+    sweep_tile<Real, U, DX, DL, DP, INTERP, ALCH_, CHECK_>(                                                           \
+        lane, S, i_eff, j, pwi.x, pwi.y, pwi.z, pwi.w, pri.x, pri.y, pri.z, pri.w, dpi.x, dpi.y, dpi.z, pwj.x, pwj.y,   \
+        pwj.z, pwj.w, prj.x, prj.y, prj.z, prj.w, dpj.x, dpj.y, dpj.z, box_x, box_y, box_z, inv_box_x, inv_box_y,       \
+        inv_box_z, cutoff_squared, beta, gi_x, gi_y, gi_z, g_qi, g_sigi, g_epsi, du_dl, energy, gj_x, gj_y, gj_z, g_qj, \
+        g_sigj, g_epsj)
     if (alch) {
-        sweep_tile<Real, U, DX, DL, DP, INTERP, true>(
-            lane, S, i_eff, j, pwi.x, pwi.y, pwi.z, pwi.w, pri.x, pri.y, pri.z, pri.w, dpi.x, dpi.y, dpi.z, pwj.x, pwj.y,
-            pwj.z, pwj.w, prj.x, prj.y, prj.z, prj.w, dpj.x, dpj.y, dpj.z, box_x, box_y, box_z, inv_box_x, inv_box_y,
-            inv_box_z, cutoff_squared, beta, gi_x, gi_y, gi_z, g_qi, g_sigi, g_epsi, du_dl, energy, gj_x, gj_y, gj_z,
-            g_qj, g_sigj, g_epsj);
+        if (check) {
+            TMB_SWEEP(true, true);
+        } else {
+            TMB_SWEEP(true, false);
+        }
     } else {
-        sweep_tile<Real, U, DX, DL, DP, INTERP, false>(
-            lane, S, i_eff, j, pwi.x, pwi.y, pwi.z, pwi.w, pri.x, pri.y, pri.z, pri.w, dpi.x, dpi.y, dpi.z, pwj.x, pwj.y,
-            pwj.z, pwj.w, prj.x, prj.y, prj.z, prj.w, dpj.x, dpj.y, dpj.z, box_x, box_y, box_z, inv_box_x, inv_box_y,
-            inv_box_z, cutoff_squared, beta, gi_x, gi_y, gi_z, g_qi, g_sigi, g_epsi, du_dl, energy, gj_x, gj_y, gj_z,
-            g_qj, g_sigj, g_epsj);
+        if (check) {
+            TMB_SWEEP(false, true);
+        } else {
+            TMB_SWEEP(false, false);
+        }
     }
+#undef TMB_SWEEP
     if (col_ok) {
         if (DX) {
             red_add(acc_out.x + j, gj_x);
@@ -1587,6 +1625,7 @@ struct DepArgs {
 };
 
 static __global__ void k_dep_tiles(DepArgs a, DevState *state) {
+    grid_dependency_wait();
     if (state->error) {
         return;
     }
@@ -1618,6 +1657,7 @@ static __global__ void k_dep_tiles(DepArgs a, DevState *state) {
 // window's block; a lambda-dependent scaled pair is evaluated for every window.
 template <typename Real, bool U, bool DX, bool DL, bool DP, bool INTERP, bool MULTI, bool COMPACT = false>
 __global__ void __launch_bounds__(128) k_pair(PairArgs a) {
+    grid_dependency_wait();
     if (a.state->error) {
         return;
     }
@@ -1765,6 +1805,7 @@ __device__ __forceinline__ unsigned long long take(unsigned long long *p) {
 // potentials may accumulate into the same buffers concurrently (the sums are
 // order-independent).
 static __global__ void k_finalize(FinalizeArgs a) {
+    grid_dependency_wait();
     const bool ok = a.state->error == 0;
     const bool multi = a.K > 1;
     const size_t total = (size_t)a.S * (size_t)a.K;

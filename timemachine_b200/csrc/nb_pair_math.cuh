@@ -60,6 +60,11 @@
 
 namespace tmb {
 
+// Waits until the previous kernel in the stream has completed and its memory
+// is visible (a no-op unless this kernel was launched with programmatic
+// stream serialization).
+__device__ __forceinline__ void grid_dependency_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
+
 // Fixed-point exponents of the accumulators.
 constexpr unsigned long long FX_EXPONENT = 0x1000000000ULL;     // 2^36: du_dx, u, du_dl, du_dq
 constexpr unsigned long long FX_EXPONENT_SIG = 0x2000000000ULL; // 2^37: du_dsig

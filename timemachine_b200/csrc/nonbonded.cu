@@ -441,8 +441,10 @@ class NonbondedPotential : public PotentialBase {
         if (conditional) {
             CK(cudaGraphConditionalHandleCreate(&cond, cap_graph, 1, cudaGraphCondAssignDefault));
         }
-        k_check_prepare<<<sgrid, tpb, 0, stream>>>(
-            pa, perm_.p, has_nblist_ ? nb_x_.p : nullptr, nb_box_.p, state_.p, conditional ? 1 : 0, cond);
+        launch_dependent(
+            k_check_prepare, dim3(sgrid), dim3(tpb), 0, stream, pa, (const unsigned *)perm_.p,
+            (const double *)(has_nblist_ ? nb_x_.p : nullptr), (const double *)nb_box_.p, state_.p, conditional ? 1 : 0,
+            cond);
         CK(cudaPeekAtLastError());
 
         if (has_nblist_) {
@@ -487,7 +489,7 @@ class NonbondedPotential : public PotentialBase {
             da.tile_cols = tile_cols_.p;
             da.lamdep = lamdep_.p;
             da.dep_tiles = dep_tiles_.p;
-            k_dep_tiles<<<4 * num_sms(), 128, 0, stream>>>(da, state_.p);
+            launch_dependent(k_dep_tiles, dim3(4 * num_sms()), dim3(128), 0, stream, da, state_.p);
             CK(cudaPeekAtLastError());
         }
         if (kidx != 0) {
@@ -519,7 +521,7 @@ class NonbondedPotential : public PotentialBase {
             if (timing_) {
                 CK(cudaEventRecord(ev_pair_[0], stream));
             }
-            k<<<pair_grid(k, smem), 128, smem, stream>>>(a);
+            launch_dependent(k, dim3(pair_grid(k, smem)), dim3(128), smem, stream, a);
             CK(cudaPeekAtLastError());
             if (timing_) {
                 CK(cudaEventRecord(ev_pair_[1], stream));
@@ -550,7 +552,7 @@ class NonbondedPotential : public PotentialBase {
             fa.state = state_.p;
             const size_t fin_threads = (size_t)S_ * K;
             const int fgrid = (int)std::max<size_t>(1, std::min<size_t>((fin_threads + tpb - 1) / tpb, 16 * (size_t)num_sms()));
-            k_finalize<<<fgrid, tpb, 0, stream>>>(fa);
+            launch_dependent(k_finalize, dim3(fgrid), dim3(tpb), 0, stream, fa);
             CK(cudaPeekAtLastError());
             // One window: k_finalize zeroed every accumulator it read (each
             // slot is read by exactly one thread). Several windows share the
@@ -608,12 +610,16 @@ class NonbondedPotential : public PotentialBase {
             CK(cudaLaunchCooperativeKernel(
                 (const void *)k_rebuild, dim3(rebuild_grid()), dim3(TB_WARPS * 32), args, 0, stream));
         } else {
-            k_bin_keys<<<sgrid, tpb, 0, stream>>>(sa, state_.p);
-            k_bin_scan<<<1, 1024, 0, stream>>>(sa, state_.p);
-            k_bin_scatter<<<sgrid, tpb, 0, stream>>>(sa, pa, perm_.p, slot_of_.p, nb_x_.p, nb_box_.p, state_.p);
+            const DevState *cst = state_.p;
+            launch_dependent(k_bin_keys, dim3(sgrid), dim3(tpb), 0, stream, sa, cst);
+            launch_dependent(k_bin_scan, dim3(1), dim3(1024), 0, stream, sa, state_.p);
+            launch_dependent(
+                k_bin_scatter, dim3(sgrid), dim3(tpb), 0, stream, sa, pa, perm_.p, slot_of_.p, nb_x_.p, nb_box_.p, cst);
             const int bb_grid = std::max(1, (RB_ * 32 + tpb - 1) / tpb);
-            k_block_bounds<<<bb_grid, tpb, 0, stream>>>(S_, d_box, posw_.p, bb_ctr_.p, bb_ext_.p, state_.p);
-            k_build_tiles<<<n_row_blocks_, TB_WARPS * 32, 0, stream>>>(ta, state_.p);
+            launch_dependent(
+                k_block_bounds, dim3(bb_grid), dim3(tpb), 0, stream, S_, d_box, (const float4 *)posw_.p, bb_ctr_.p,
+                bb_ext_.p, cst);
+            launch_dependent(k_build_tiles, dim3(n_row_blocks_), dim3(TB_WARPS * 32), 0, stream, ta, state_.p);
         }
         CK(cudaPeekAtLastError());
     }
