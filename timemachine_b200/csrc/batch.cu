@@ -203,6 +203,7 @@ __global__ void __launch_bounds__(TB_WARPS * 32) k_b_tiles(const Rep *__restrict
     ta.radius = (float)(r.cutoff + r.padding + 1e-5);
     ta.box = r.box;
     ta.posw = r.posw;
+    ta.prm = nullptr;
     ta.bb_ctr = r.bb_ctr;
     ta.bb_ext = r.bb_ext;
     ta.tile_cols = r.tile_cols;

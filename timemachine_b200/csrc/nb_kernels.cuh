@@ -398,6 +398,64 @@ static __global__ void k_bin_scatter(
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ float wrap_delta(float d, float L, float inv_L) { return d - L * rintf(d * inv_L); }
 
+// Lennard-Jones atoms first within the 32-slot block rb (one warp): the pair
+// kernel's LJ branch is taken in a rotation round only when some lane pairs
+// two LJ atoms, and with LJ rows and LJ columns both leading the tile those
+// pairs fall in fewer rounds. Blocks that straddle the interaction group's
+// row/column boundary keep their order. Restages the moved atoms' slots.
+__device__ __forceinline__ void lj_first_warp(
+    const PrepareArgs &pa, int S, int n_first, int rb, unsigned *__restrict__ perm, int *__restrict__ slot_of) {
+    const int lane = threadIdx.x & 31;
+    const int lo = rb * TILE;
+    const int hi = min(S, lo + TILE);
+    if (lo < n_first && hi > n_first) {
+        return;
+    }
+    const int s = lo + lane;
+    const bool valid = s < S;
+    const unsigned atom = valid ? perm[s] : 0u;
+    bool lj = false;
+    if (valid) {
+        lj = pa.p[3 * (size_t)atom + 2] != 0.0;
+        if (pa.interpolated) {
+            lj = lj || pa.p[3 * ((size_t)pa.N + atom) + 2] != 0.0;
+        }
+    }
+    const unsigned m = __ballot_sync(FULL_MASK, lj);
+    const unsigned vm = __ballot_sync(FULL_MASK, valid);
+    if (m == 0u || m == vm) {
+        return;
+    }
+    const unsigned lt = (1u << lane) - 1u;
+    const int pos = lj ? __popc(m & lt) : __popc(m) + __popc(vm & ~m & lt);
+    __syncwarp();
+    if (valid && lo + pos != s) {
+        const int ns = lo + pos;
+        perm[ns] = atom;
+        if (slot_of) {
+            slot_of[atom] = ns;
+        }
+        prepare_slot(pa, ns, (int)atom);
+    }
+    __syncwarp();
+}
+
+// Writes one tile's 32 column slots with the LJ atoms first (prm: staged
+// parameters, eps in .z; nullptr keeps the order).
+__device__ __forceinline__ void store_tile_lj_first(
+    unsigned *__restrict__ dst, unsigned s, unsigned S, const float4 *__restrict__ prm) {
+    const int lane = threadIdx.x & 31;
+    if (prm == nullptr) {
+        dst[lane] = s;
+        return;
+    }
+    const bool lj = s < S && prm[s].z != 0.f;
+    const unsigned m = __ballot_sync(FULL_MASK, lj);
+    const unsigned lt = (1u << lane) - 1u;
+    const int pos = lj ? __popc(m & lt) : __popc(m) + __popc(~m & lt);
+    dst[pos] = s;
+}
+
 // Bounding box of the 32-slot block rb (one warp).
 __device__ __forceinline__ void block_bounds_warp(
     int S,
@@ -447,13 +505,18 @@ static __global__ void k_block_bounds(
     const float4 *__restrict__ posw,
     float4 *__restrict__ bb_ctr,
     float4 *__restrict__ bb_ext,
-    const DevState *state) {
+    const DevState *state,
+    PrepareArgs pa,
+    int n_first,
+    unsigned *__restrict__ perm,
+    int *__restrict__ slot_of) {
     grid_dependency_wait();
     if (!state->rebuild || state->error) {
         return;
     }
     const int RB = (S + TILE - 1) / TILE;
     for (int rb = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; rb < RB; rb += (gridDim.x * blockDim.x) >> 5) {
+        lj_first_warp(pa, S, n_first, rb, perm, slot_of);
         block_bounds_warp(S, rb, box, posw, bb_ctr, bb_ext);
     }
 }
@@ -479,6 +542,7 @@ struct TileArgs {
     float radius;     // list radius (cutoff + padding + margin)
     const double *box;
     const float4 *posw;
+    const float4 *prm;     // staged parameters (eps in .z) to put LJ atoms first in a tile; nullptr: keep order
     const float4 *bb_ctr;
     const float4 *bb_ext;
     unsigned *tile_cols;   // [capacity*32] slot of each column atom (S = empty)
@@ -639,7 +703,7 @@ __device__ __forceinline__ void build_tiles_cta(const TileArgs &a, const int rb,
                     t = atomicAdd(&tile_count, 1);
                 }
                 t = __shfl_sync(FULL_MASK, t, 0);
-                a.tile_cols[(base_tile + t) * TILE + lane] = buf[warp][lane];
+                store_tile_lj_first(a.tile_cols + (base_tile + t) * TILE, buf[warp][lane], (unsigned)S, a.prm);
                 __syncwarp();
                 buf[warp][lane] = buf[warp][TILE + lane];
                 __syncwarp();
@@ -662,7 +726,8 @@ __device__ __forceinline__ void build_tiles_cta(const TileArgs &a, const int rb,
         const int n = rem_count;
         for (int b = 0; b < n; b += TILE) {
             const int t = tile_count + b / TILE;
-            a.tile_cols[(base_tile + t) * TILE + lane] = b + lane < n ? rem[b + lane] : (unsigned)S;
+            store_tile_lj_first(a.tile_cols + (base_tile + t) * TILE, b + lane < n ? rem[b + lane] : (unsigned)S,
+                                (unsigned)S, a.prm);
         }
         __syncwarp();
         if (lane == 0) {
@@ -825,6 +890,7 @@ static __global__ void __launch_bounds__(TB_WARPS * 32) k_rebuild(RebuildArgs r,
         const int warp = tid >> 5;
         const int n_warps = nth >> 5;
         for (int rb = warp; rb < r.ta.RB; rb += n_warps) {
+            lj_first_warp(r.pa, S, r.sa.n_first, rb, r.perm, r.slot_of);
             block_bounds_warp(S, rb, r.sa.box, r.ta.posw, const_cast<float4 *>(r.ta.bb_ctr), const_cast<float4 *>(r.ta.bb_ext));
         }
     }

@@ -590,6 +590,7 @@ class NonbondedPotential : public PotentialBase {
         ta.radius = (float)(cutoff_ + padding_ + 1e-5);
         ta.box = d_box;
         ta.posw = posw_.p;
+        ta.prm = prm_.p;
         ta.bb_ctr = bb_ctr_.p;
         ta.bb_ext = bb_ext_.p;
         ta.tile_cols = tile_cols_.p;
@@ -618,7 +619,7 @@ class NonbondedPotential : public PotentialBase {
             const int bb_grid = std::max(1, (RB_ * 32 + tpb - 1) / tpb);
             launch_dependent(
                 k_block_bounds, dim3(bb_grid), dim3(tpb), 0, stream, S_, d_box, (const float4 *)posw_.p, bb_ctr_.p,
-                bb_ext_.p, cst);
+                bb_ext_.p, cst, pa, sa.n_first, perm_.p, slot_of_.p);
             launch_dependent(k_build_tiles, dim3(n_row_blocks_), dim3(TB_WARPS * 32), 0, stream, ta, state_.p);
         }
         CK(cudaPeekAtLastError());
