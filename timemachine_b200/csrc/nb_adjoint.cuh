@@ -40,7 +40,6 @@ struct AdjointArgs {
     const unsigned *perm; // [S] slot -> atom
     const unsigned *tile_cols;
     const int4 *items;
-    int chunk;            // tiles per work item (item.z <= chunk)
     int M;
     const int *pair_idxs; // [M,2] atoms
     const double *scales; // [M,2]
@@ -182,7 +181,8 @@ static __global__ void __launch_bounds__(ADJ_WARPS * 32) k_adjoint(AdjointArgs a
     AdjTileSmem &sm = smem[threadIdx.x >> 5];
     const int lane = threadIdx.x & 31;
     const unsigned S = (unsigned)a.S;
-    const int n_tile_units = a.tile_cols ? a.state->n_items * a.chunk : 0;
+    const int chunk = max(1, a.state->items_chunk); // the list's, whichever call built it
+    const int n_tile_units = a.tile_cols ? a.state->n_items * chunk : 0;
     const int n_total = n_tile_units + (a.M + TILE - 1) / TILE;
     for (;;) {
         int unit = 0;
@@ -205,8 +205,8 @@ static __global__ void __launch_bounds__(ADJ_WARPS * 32) k_adjoint(AdjointArgs a
             }
             continue;
         }
-        const int4 it = a.items[unit / a.chunk];
-        const int t = unit - (unit / a.chunk) * a.chunk;
+        const int4 it = a.items[unit / chunk];
+        const int t = unit - (unit / chunk) * chunk;
         if (t >= it.z) {
             continue; // warp-uniform
         }

@@ -42,6 +42,7 @@ struct DevState {
     int rebuilds;         // number of rebuilds performed (diagnostics)
     int n_dep;            // lambda-dependent tiles listed by k_dep_tiles (multi-window calls)
     unsigned prep_done;   // completion counter of k_check_prepare (graph-conditional rebuilds)
+    int items_chunk;      // tiles per work item in the list of the last rebuild
     unsigned bar_count;   // grid barrier of k_rebuild: arrivals in the current phase
     unsigned bar_gen;     // grid barrier of k_rebuild: completed phases
 };
@@ -790,6 +791,7 @@ __device__ __forceinline__ void build_tiles_cta(const TileArgs &a, const int rb,
     }
     if (threadIdx.x == 0) {
         state->n_items = carry;
+        state->items_chunk = a.chunk;
         state->rebuilds += 1;
         state->done_ctas = 0;
         state->rebuild = 0;
