@@ -650,7 +650,7 @@ def run_batch_form():
         mode="eval",
         steps=2,
         repeats=1,
-        candidates=[dict(chunk=c, padding=p, grid_bits_offset=0, pair_ctas_per_sm=0) for c in (2, 4, 8) for p in (0.06, 0.1)],
+        candidates=[dict(chunk=c, padding=p, grid_bits_offset=0, pair_ctas_per_sm=0) for c in (1, 2, 4, 8) for p in (0.06, 0.1)],
     )
     t_eval = timed(lambda: b.evaluate(), 3)
     batch_evals = 3 * n_rep / t_eval

@@ -207,12 +207,12 @@ class ReplicaBatch:
         the fastest. mode "md": `steps` Langevin steps (rebuild cadence
         included; the replicas' states advance); "eval": `steps` evaluations.
         Candidates: dicts of set_tuning keywords (default: tiles per item
-        {2, 4, 8} x padding {0.06, 0.1, 0.14} x Hilbert grid offset {0, 1}).
+        {1, 2, 4, 8} x padding {0.06, 0.1, 0.14} x Hilbert grid offset {0, 1}).
         Returns (best, [(config, seconds), ...])."""
         if candidates is None:
             candidates = [
                 {"chunk": c, "padding": p, "grid_bits_offset": g, "pair_ctas_per_sm": 0}
-                for c, p, g in itertools.product([2, 4, 8], [0.06, 0.1, 0.14], [0, 1])
+                for c, p, g in itertools.product([1, 2, 4, 8], [0.06, 0.1, 0.14], [0, 1])
             ]
 
         def run():
