@@ -692,6 +692,13 @@ def run_batch_form():
     plain_evals = n_rep / t_plain
     del plain
 
+    # the MD step computes forces only: its best schedule can differ from the evaluation's
+    md_tune_best, md_tune_table = b.autotune(
+        mode="md",
+        steps=20,
+        repeats=1,
+        candidates=[dict(chunk=c, padding=p, grid_bits_offset=0, pair_ctas_per_sm=0) for c in (1, 2, 4, 8) for p in (0.06, 0.1)],
+    )
     t_md = timed(lambda: b.md(BATCH_CHUNK, chunk=BATCH_CHUNK, use_graph=True), 1)
     md_replica_steps = n_rep * BATCH_CHUNK / t_md
     sample = b.ids()[:: max(1, n_rep // 16)]
@@ -716,6 +723,7 @@ def run_batch_form():
             "timing": "CUDA events on the batch stream around one graph-replayed 500-step chunk",
         },
         "autotune": {"best": tune_best, "candidates": [[c, t] for c, t in tune_table]},
+        "autotune_md": {"best": md_tune_best, "candidates": [[c, t] for c, t in md_tune_table]},
         "timing": "CUDA events (batch stream / torch stream), inputs resident on the device",
         "device_bytes": b.bytes_in_use(),
     }
