@@ -47,6 +47,9 @@ SEED = 2024
 # where both atoms carry epsilon.
 FLOPS_PER_PAIR = 67
 FLOPS_PER_LJ_PAIR = 26
+# DRAM bytes (read + write) of one 12-window pair-kernel launch on this
+# workload, from an ncu capture of the same command (14.4 MB read, 0 written)
+PAIR_LAUNCH_DRAM_BYTES = 14.4e6
 
 
 def parse():
@@ -455,7 +458,11 @@ def run_tmnb(args, world, rank, local):
             "peak": peak.value,
             "unit": "TFLOP/s",
             "frac": achieved / peak.value,
-            "traffic": None,
+            # dram__bytes_read.sum + dram__bytes_write.sum of one launch of this kernel on
+            # this workload (ncu --set full capture, k_pair_12windows_water_ligand_22840.md
+            # under profiles/): the working set stays in L2, DRAM is not the bound
+            "traffic": PAIR_LAUNCH_DRAM_BYTES,
+            "traffic_unit": "bytes per launch",
             "kernel": "k_pair (full variant, 12 windows in one launch)",
             "pair_kernel_ms": float(np.mean(pair_ms)),
             "flops_per_launch": float(flops_launch),
