@@ -65,6 +65,29 @@ def test_vjp_matches_double_backward_oracle(lam):
     assert _rel(gp2, gp) < 1e-10
 
 
+def test_vjp_on_a_list_built_by_a_multi_window_call():
+    """A multi-window call builds its neighbour list with several tiles per work
+    item, a single-window call with one; an adjoint that reuses a list built by
+    either (no rebuild in between) walks it correctly."""
+    s = _system()
+    lam = 0.5
+    impl = P.Nonbonded(s.exclusion_idxs, s.scales, s.lambda_plane_idxs, s.lambda_offset_idxs, s.beta, s.cutoff)
+    impl = impl.unbound_impl(np.float32)
+    rng = np.random.default_rng(6)
+    G = rng.normal(size=(s.N, 3))
+    g = 0.25
+    impl.execute_windows_fixed(s.x, s.params, s.box, np.linspace(0.0, 1.0, 12))
+    rebuilds = impl.nblist_stats()[2]
+    gp, gw = _adjoint(impl, s, lam, G, g)
+    assert impl.nblist_stats()[2] == rebuilds  # the adjoint reused the multi-window list
+    _, rp, rw = force_vjp_oracle(
+        s.x, s.params, s.box, lam, s.lambda_plane_idxs, s.lambda_offset_idxs.astype(np.float64), s.beta, s.cutoff,
+        s.exclusion_idxs, s.scales, G, g,
+    )
+    assert _rel(gp, rp) < TOL_VJP
+    assert _rel(gw, rw) < TOL_VJP
+
+
 def test_vjp_matches_finite_differences():
     """FP64 central differences (step 1e-4) of Phi = sum(G * du_dx) + g * du_dl
     of the oracle, for ligand charges, sigmas, sqrt(eps) and offsets."""
