@@ -173,6 +173,32 @@ __global__ void k_b_scatter(const Rep *__restrict__ reps, const int2 *__restrict
     }
 }
 
+// Lennard-Jones atoms first within the replica's 32-slot block rb (one warp),
+// as lj_first_warp does for a single system; restages the moved slots.
+__device__ __forceinline__ void lj_first_rep(const Rep &r, int rb) {
+    const int lane = threadIdx.x & 31;
+    const int lo = rb * TILE;
+    const int s = lo + lane;
+    const bool valid = s < r.N;
+    const unsigned atom = valid ? r.perm[s] : 0u;
+    const bool lj = valid && r.p[3 * (size_t)atom + 2] != 0.0;
+    const unsigned m = __ballot_sync(FULL_MASK, lj);
+    const unsigned vm = __ballot_sync(FULL_MASK, valid);
+    if (m == 0u || m == vm) {
+        return;
+    }
+    const unsigned lt = (1u << lane) - 1u;
+    const int pos = lj ? __popc(m & lt) : __popc(m) + __popc(vm & ~m & lt);
+    __syncwarp();
+    if (valid && lo + pos != s) {
+        const int ns = lo + pos;
+        r.perm[ns] = atom;
+        r.slot_of[atom] = ns;
+        stage_slot(r, ns, (int)atom);
+    }
+    __syncwarp();
+}
+
 __global__ void k_b_bounds(const Rep *__restrict__ reps, const int2 *__restrict__ rbmap, int n_rb) {
     const int g = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     if (g >= n_rb) {
@@ -183,6 +209,7 @@ __global__ void k_b_bounds(const Rep *__restrict__ reps, const int2 *__restrict_
     if (!r.state->rebuild || r.state->error) {
         return;
     }
+    lj_first_rep(r, m.y);
     block_bounds_warp(r.N, m.y, r.box, r.posw, r.bb_ctr, r.bb_ext);
 }
 
@@ -203,7 +230,7 @@ __global__ void __launch_bounds__(TB_WARPS * 32) k_b_tiles(const Rep *__restrict
     ta.radius = (float)(r.cutoff + r.padding + 1e-5);
     ta.box = r.box;
     ta.posw = r.posw;
-    ta.prm = nullptr;
+    ta.prm = r.prm;
     ta.bb_ctr = r.bb_ctr;
     ta.bb_ext = r.bb_ext;
     ta.tile_cols = r.tile_cols;
