@@ -275,6 +275,21 @@ tmnb_status tmnb_potential_nblist_stats(
  * block [RB] and the column slots of all tiles [tile_capacity*32]; row block
  * rb owns the tiles starting at rb*RB - rb*(rb-1)/2. Any pointer may be NULL. */
 tmnb_status tmnb_potential_nblist_shape(tmnb_potential *pot, int *S, int *RB, long long *tile_capacity);
+
+/*
+ * Rows per tile of the neighbour list (no reference counterpart; the
+ * reference's tiles are 32 rows x 32 columns): 16 (default), 32 or 8 slots per
+ * row group. A tile is always 32 column atoms; smaller row groups occupy
+ * smaller regions and list fewer out-of-range pairs, at more tiles. The
+ * results are identical; the next call rebuilds the list. nblist_rows reports
+ * the row-group size and the number of 32-slot column blocks, with which row
+ * group g owns the tiles from
+ *   m * (b*CB - b*(b-1)/2) + (g - b*m) * (CB - b),  m = 32/rows, b = g/m
+ * (interaction groups: g * (CB - NR/32)); nblist_shape's RB is then the number
+ * of row groups and copy_nblist's row_block_ntiles has one entry per group.
+ */
+tmnb_status tmnb_potential_set_tile_rows(tmnb_potential *pot, int rows);
+tmnb_status tmnb_potential_nblist_rows(tmnb_potential *pot, int *rows, int *column_blocks);
 tmnb_status tmnb_potential_copy_nblist(
     tmnb_potential *pot, void *stream, unsigned *perm, int *row_block_ntiles, unsigned *tile_cols);
 
@@ -391,7 +406,9 @@ int tmnb_potential_num_atoms(const tmnb_potential *pot);
  * the rotating sweep, which evaluates a tile in 32 lane-rotation rounds; 1
  * the compacted sweep, which tests all 32x32 slots of a tile first and then
  * evaluates only the in-cutoff pairs, 32 at a time. The results are
- * identical; the switch exists for measurement.
+ * identical; the switch exists for measurement. The compacted sweep runs on
+ * 32-row tiles: selecting it sets the tile rows to 32, and setting other tile
+ * rows (tmnb_potential_set_tile_rows) returns to the rotating sweep.
  */
 tmnb_status tmnb_potential_set_pair_schedule(tmnb_potential *pot, int compact);
 

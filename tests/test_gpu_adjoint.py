@@ -44,11 +44,12 @@ def _adjoint(impl, s, lam, G, g):
     return gp.cpu().numpy().reshape(-1, 3), gw.cpu().numpy()
 
 
-@pytest.mark.parametrize("lam", [0.0, 0.5])
-def test_vjp_matches_double_backward_oracle(lam):
+@pytest.mark.parametrize("lam,rows", [(0.0, 32), (0.5, 32), (0.5, 16), (0.5, 8)])
+def test_vjp_matches_double_backward_oracle(lam, rows):
     s = _system()
     impl = P.Nonbonded(s.exclusion_idxs, s.scales, s.lambda_plane_idxs, s.lambda_offset_idxs, s.beta, s.cutoff)
     impl = impl.unbound_impl(np.float32)
+    impl.set_tile_rows(rows)
     rng = np.random.default_rng(3)
     G = rng.normal(size=(s.N, 3))
     g = 0.37
@@ -57,7 +58,7 @@ def test_vjp_matches_double_backward_oracle(lam):
         s.x, s.params, s.box, lam, s.lambda_plane_idxs, s.lambda_offset_idxs.astype(np.float64), s.beta, s.cutoff,
         s.exclusion_idxs, s.scales, G, g,
     )
-    print(f"[lambda={lam}] relative error params {_rel(gp, rp):.2e} offsets {_rel(gw, rw):.2e}")
+    print(f"[lambda={lam}, rows={rows}] relative error params {_rel(gp, rp):.2e} offsets {_rel(gw, rw):.2e}")
     assert _rel(gp, rp) < TOL_VJP
     assert _rel(gw, rw) < TOL_VJP or np.linalg.norm(rw) == 0
     # a second call gives the same gradient up to the order of the FP64 atomic sums

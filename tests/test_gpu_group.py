@@ -116,13 +116,13 @@ def test_neighbour_list_covers_every_row_column_pair():
     rows = np.flatnonzero(s.lambda_offset_idxs != 0).astype(np.int32)
     g = _group(rows, s.lambda_plane_idxs, s.lambda_offset_idxs, s.beta, s.cutoff)
     g.execute(s.x, s.params, s.box, 0.0)
-    perm, tiles = g.get_nblist()
+    perm, tiles, R = g.get_nblist()
     NR = rows.size
     assert sorted(perm[:NR].tolist()) == sorted(rows.tolist())
     listed = set()
     for rb, cols in enumerate(tiles):
         assert np.all(cols >= NR)
-        for r in range(rb * 32, min(NR, rb * 32 + 32)):
+        for r in range(rb * R, min(NR, rb * R + R)):
             for cs in cols:
                 listed.add((int(perm[r]), int(perm[cs])))
     o = Oracle(s.lambda_plane_idxs, s.lambda_offset_idxs, s.beta, s.cutoff)

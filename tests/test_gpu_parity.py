@@ -154,19 +154,22 @@ def test_tolerance_vs_fp64_oracle(name):
         assert edl <= TOL_RANDOM
 
 
+@pytest.mark.parametrize("rows", [32, 16, 8])
 @pytest.mark.parametrize("name", ["water23k_lam0.5", "golden_repro"])
-def test_nblist_covers_every_pair_within_cutoff(name):
+def test_nblist_covers_every_pair_within_cutoff(name, rows):
     """Every pair within the list radius (cutoff + the 0.1 nm padding) sits in
-    the tile list of the lower slot's row block (tests/test_nblist.py:70-94
-    against brute force): pairs that start just outside the cutoff can come
-    within it before the next rebuild."""
+    the tile list of the lower slot's row group (tests/test_nblist.py:70-94
+    against brute force), for row groups of 32, 16 and 8 slots: pairs that
+    start just outside the cutoff can come within it before the next rebuild."""
     from scipy.spatial import cKDTree
 
     c = CASES[name]()
     x, p, box = _inputs(c)
     impl = _nonbonded(c).unbound_impl(np.float32)
+    impl.set_tile_rows(rows)
     impl.execute(x, p, box, c["lam"])
-    perm, tiles = impl.get_nblist()
+    perm, tiles, got_rows = impl.get_nblist()
+    assert got_rows == rows
     assert np.array_equal(np.sort(perm), np.arange(perm.size))
     inv = np.empty_like(perm)
     inv[perm] = np.arange(perm.size, dtype=perm.dtype)
@@ -177,7 +180,7 @@ def test_nblist_covers_every_pair_within_cutoff(name):
     si, sj = inv[pairs[:, 0]], inv[pairs[:, 1]]
     lo, hi = np.minimum(si, sj), np.maximum(si, sj)
     sets = [set(t.tolist()) for t in tiles]
-    missing = sum(1 for a, b in zip(lo.tolist(), hi.tolist()) if b not in sets[a // 32])
+    missing = sum(1 for a, b in zip(lo.tolist(), hi.tolist()) if b not in sets[a // rows])
     assert missing == 0
     for t in tiles:
         assert len(t) == len(set(t.tolist()))
@@ -211,6 +214,38 @@ def test_hilbert_sort_on_off_bitwise_golden_repro():
     b = b_impl.execute(x, p, box, c["lam"])
     for k in range(4):
         np.testing.assert_array_equal(a[k], b[k])
+
+
+@pytest.mark.parametrize("rows", [16, 8])
+@pytest.mark.parametrize("name", ["water23k_lam0.5", "random1050", "golden_repro"])
+def test_tile_rows_bitwise_equal(name, rows):
+    """Neighbour-list tiles of 16 (the default) or 8 rows give the fixed-point
+    outputs of 32-row tiles bit for bit (one window and several windows): du_dx and du_dp
+    per atom; u and du_dl as sums, since a pair's u and du_dl go to the atom
+    in the lower slot, and the slot order within a row group differs."""
+    c = CASES[name]()
+    x, p, box = _inputs(c)
+    a_impl = _nonbonded(c).unbound_impl(np.float32)
+    a_impl.set_tile_rows(32)
+    b_impl = _nonbonded(c).unbound_impl(np.float32)
+    b_impl.set_tile_rows(rows)
+
+    def same(a, b, per_atom):
+        if per_atom:
+            np.testing.assert_array_equal(a, b)
+        else:
+            assert int(np.sum(a, dtype=np.uint64)) == int(np.sum(b, dtype=np.uint64))
+
+    fa = a_impl._execute_fixed(x, p, box, c["lam"], True, True, True, True)
+    fb = b_impl._execute_fixed(x, p, box, c["lam"], True, True, True, True)
+    for k in range(4):
+        same(fa[k], fb[k], k < 2)
+    lams = np.linspace(0.0, 1.0, 5)
+    wa = a_impl.execute_windows_fixed(x, p, box, lams)
+    wb = b_impl.execute_windows_fixed(x, p, box, lams)
+    for k in range(4):
+        for w in range(lams.size):
+            same(wa[k][w], wb[k][w], k < 2)
 
 
 def test_golden_bad_test_547_du_dl_exactly_zero():

@@ -222,6 +222,7 @@ __global__ void __launch_bounds__(TB_WARPS * 32) k_b_tiles(const Rep *__restrict
     TileArgs ta;
     ta.S = r.N;
     ta.RB = r.RB;
+    ta.rows = TILE;
     ta.group = 0;
     ta.row_end = r.N;
     ta.col_begin = 0;

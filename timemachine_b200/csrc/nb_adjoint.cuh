@@ -40,6 +40,7 @@ struct AdjointArgs {
     const unsigned *perm; // [S] slot -> atom
     const unsigned *tile_cols;
     const int4 *items;
+    int rows;             // slots per row group of the tile list
     int M;
     const int *pair_idxs; // [M,2] atoms
     const double *scales; // [M,2]
@@ -166,13 +167,15 @@ struct AdjTileSmem {
     double acc[4][TILE];
 };
 
-// One warp per tile (lane = row slot). The tile's column atoms are staged in
-// shared memory; in round r lane l pairs its row atom with column (l + r) mod
-// 32, so the 32 lanes of a round touch 32 distinct columns and add into their
+// One warp per tile. The tile's 32 column atoms are staged in shared memory.
+// With 32-slot row groups lane l holds row l and in round r pairs it with
+// column (l + r) mod 32; with smaller groups of R rows, lane l holds row
+// l mod R and its lane group sweeps its own R columns in R rounds. Either way
+// the lanes of a round touch distinct columns and add into their
 // shared-memory accumulators without conflicts. Each tile ends with one FP64
-// atomic per (atom, output) for its rows and its columns. The scaled pairs
-// follow as one lane per pair. Dynamic work counter state->next_item (reset
-// by k_check_prepare).
+// atomic per (lane, output) for its row and one per (column, output). The
+// scaled pairs follow as one lane per pair. Dynamic work counter
+// state->next_item (reset by k_check_prepare).
 static __global__ void __launch_bounds__(ADJ_WARPS * 32) k_adjoint(AdjointArgs a) {
     __shared__ AdjTileSmem smem[ADJ_WARPS];
     if (a.state->error) {
@@ -211,7 +214,10 @@ static __global__ void __launch_bounds__(ADJ_WARPS * 32) k_adjoint(AdjointArgs a
             continue; // warp-uniform
         }
         const long long tile = (long long)it.y + t;
-        const unsigned i = (unsigned)(it.x * TILE + lane);
+        // row groups of `rows` slots: lane l holds row l mod rows and sweeps
+        // the `rows` columns of its lane group (all 32 when rows = 32)
+        const int rows = a.rows;
+        const unsigned i = (unsigned)(it.x * rows + (lane & (rows - 1)));
         const int ai = i < S ? (int)a.perm[i] : -1;
         AdjAtom I = {};
         if (ai >= 0) {
@@ -238,8 +244,8 @@ static __global__ void __launch_bounds__(ADJ_WARPS * 32) k_adjoint(AdjointArgs a
         }
         __syncwarp();
         double rq = 0, rs = 0, re = 0, rw = 0;
-        for (int r = 0; r < TILE; r++) {
-            const int c = (lane + r) & (TILE - 1);
+        for (int r = 0; r < rows; r++) {
+            const int c = (lane & ~(rows - 1)) | (((lane & (rows - 1)) + r) & (rows - 1));
             if (ai >= 0 && sm.atom[c] >= 0 && i < sm.slot[c]) {
                 AdjAtom J;
                 for (int d = 0; d < 3; d++) {

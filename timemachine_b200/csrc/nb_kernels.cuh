@@ -399,13 +399,16 @@ static __global__ void k_bin_scatter(
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ float wrap_delta(float d, float L, float inv_L) { return d - L * rintf(d * inv_L); }
 
-// Lennard-Jones atoms first within the 32-slot block rb (one warp): the pair
-// kernel's LJ branch is taken in a rotation round only when some lane pairs
-// two LJ atoms, and with LJ rows and LJ columns both leading the tile those
-// pairs fall in fewer rounds. Blocks that straddle the interaction group's
-// row/column boundary keep their order. Restages the moved atoms' slots.
+// Lennard-Jones atoms first within each row group (`rows` slots) of the
+// 32-slot block rb (one warp): the pair kernel's LJ branch is taken in a
+// rotation round only when some lane pairs two LJ atoms, and with LJ rows and
+// LJ columns both leading the tile those pairs fall in fewer rounds. Sorting
+// within row groups, not across them, keeps each group spatially compact.
+// Blocks that straddle the interaction group's row/column boundary keep their
+// order. Restages the moved atoms' slots.
 __device__ __forceinline__ void lj_first_warp(
-    const PrepareArgs &pa, int S, int n_first, int rb, unsigned *__restrict__ perm, int *__restrict__ slot_of) {
+    const PrepareArgs &pa, int S, int n_first, int rb, unsigned *__restrict__ perm, int *__restrict__ slot_of,
+    int rows = TILE) {
     const int lane = threadIdx.x & 31;
     const int lo = rb * TILE;
     const int hi = min(S, lo + TILE);
@@ -428,7 +431,10 @@ __device__ __forceinline__ void lj_first_warp(
         return;
     }
     const unsigned lt = (1u << lane) - 1u;
-    const int pos = lj ? __popc(m & lt) : __popc(m) + __popc(vm & ~m & lt);
+    const int seg = lane / rows;
+    const unsigned segm = (rows == TILE ? FULL_MASK : ((1u << rows) - 1u)) << (seg * rows);
+    const int pos = seg * rows +
+                    (lj ? __popc(m & lt & segm) : __popc(m & segm) + __popc(vm & ~m & lt & segm));
     __syncwarp();
     if (valid && lo + pos != s) {
         const int ns = lo + pos;
@@ -510,35 +516,41 @@ static __global__ void k_block_bounds(
     PrepareArgs pa,
     int n_first,
     unsigned *__restrict__ perm,
-    int *__restrict__ slot_of) {
+    int *__restrict__ slot_of,
+    int rows) {
     grid_dependency_wait();
     if (!state->rebuild || state->error) {
         return;
     }
     const int RB = (S + TILE - 1) / TILE;
     for (int rb = (blockIdx.x * blockDim.x + threadIdx.x) >> 5; rb < RB; rb += (gridDim.x * blockDim.x) >> 5) {
-        lj_first_warp(pa, S, n_first, rb, perm, slot_of);
+        lj_first_warp(pa, S, n_first, rb, perm, slot_of, rows);
         block_bounds_warp(S, rb, box, posw, bb_ctr, bb_ext);
     }
 }
 
 // ---------------------------------------------------------------------------
-// Tile list. One CTA (TB_WARPS warps) per row block rb. For every column block
-// cb >= rb (upper triangle) whose bounding box is within the list radius of
-// rb's box, each column atom is kept when any row atom lies within the list
-// radius (minimum image, 3D). Kept atoms are packed 32 to a tile; the tiles of
-// row block rb occupy the fixed range tile_offset(rb) .. + (CB - rb), which
-// bounds their number. The last CTA to finish turns the per-row-block tile
-// counts into work items of at most `chunk` tiles.
-// (Same selection rule as timemachine/cpp/src/kernels/k_neighborlist.cuh:168-427.)
+// Tile list. Rows come in groups of `rows` (32, 16 or 8) consecutive slots;
+// one CTA (TB_WARPS warps) per row group g. For every 32-slot column block from
+// the one holding the group's first slot on (upper triangle) whose bounding
+// box is within the list radius of the group's box, each column atom at or
+// after the group's first slot is kept when any row atom lies within the list
+// radius (minimum image, 3D). Kept atoms are packed 32 to a tile, so a tile is
+// rows x 32 pairs; smaller row groups sit in smaller regions and list fewer
+// out-of-range column atoms. The tiles of row group g occupy a fixed range
+// (tile_base) sized by the column blocks it can reach. The last CTA to finish
+// turns the per-group tile counts into work items of at most `chunk` tiles.
+// (Same selection rule as timemachine/cpp/src/kernels/k_neighborlist.cuh:168-427,
+// which uses 32-atom row blocks.)
 // ---------------------------------------------------------------------------
 struct TileArgs {
     int S;
-    int RB;           // blocks of 32 slots = ceil(S/32)
+    int RB;           // blocks of 32 slots = ceil(S/32) (column blocks)
+    int rows;         // slots per row group: 32, 16 or 8
     int group;        // 1: interaction group (rows [0, row_end) x columns [col_begin, S))
     int row_end;      // S, or the number of row atoms
     int col_begin;    // 0, or the number of row atoms
-    int n_row_blocks; // RB, or ceil(row_end/32)
+    int n_row_blocks; // row groups: ceil(row_end/rows)
     int cb_first;     // group: first column block (col_begin/32)
     float radius;     // list radius (cutoff + padding + margin)
     const double *box;
@@ -547,8 +559,8 @@ struct TileArgs {
     const float4 *bb_ctr;
     const float4 *bb_ext;
     unsigned *tile_cols;   // [capacity*32] slot of each column atom (S = empty)
-    int *rb_ntiles;        // [RB]
-    int4 *items;           // [item_capacity] (rb, first tile, tile count, 0)
+    int *rb_ntiles;        // [n_row_blocks] tiles of each row group
+    int4 *items;           // [item_capacity] (row group, first tile, tile count, 0)
     int chunk;             // tiles per work item
 };
 
@@ -556,16 +568,28 @@ __host__ __device__ __forceinline__ long long tile_offset(int rb, int RB) {
     return (long long)rb * RB - ((long long)rb * (rb - 1)) / 2;
 }
 
-// First tile of row block rb: upper triangle (RB - rb tiles per row block),
-// or for an interaction group RB - cb_first tiles per row block.
-__host__ __device__ __forceinline__ long long tile_base(const TileArgs &a, int rb) {
-    return a.group ? (long long)rb * (a.RB - a.cb_first) : tile_offset(rb, a.RB);
+// First tile of row group g. Upper triangle: the group reaches the RB - b
+// column blocks from its own block b = g*rows/32 on, one tile per block at
+// most; with m = 32/rows groups per block that sums to
+// m * tile_offset(b, RB) + (g mod m) * (RB - b). Interaction group:
+// RB - cb_first tiles per row group.
+__host__ __device__ __forceinline__ long long tile_base_rows(int g, int rows, int RB, int group, int cb_first) {
+    if (group) {
+        return (long long)g * (RB - cb_first);
+    }
+    const int m = TILE / rows;
+    const int b = g / m;
+    return (long long)m * tile_offset(b, RB) + (long long)(g - b * m) * (RB - b);
+}
+__host__ __device__ __forceinline__ long long tile_base(const TileArgs &a, int g) {
+    return tile_base_rows(g, a.rows, a.RB, a.group, a.cb_first);
 }
 
 constexpr int TB_WARPS = 8;
 
 __device__ __forceinline__ void build_tiles_cta(const TileArgs &a, const int rb, DevState *state) {
     __shared__ float4 row_pos[TILE];
+    __shared__ float4 row_box[2]; // the row group's box: centre, half-extent
     __shared__ unsigned buf[TB_WARPS][2 * TILE];
     __shared__ unsigned rem[TB_WARPS * TILE];
     __shared__ int cand[TB_WARPS * 32]; // column blocks of the current window that pass the box test
@@ -581,8 +605,39 @@ __device__ __forceinline__ void build_tiles_cta(const TileArgs &a, const int rb,
     const float iLx = 1.0f / Lx, iLy = 1.0f / Ly, iLz = 1.0f / Lz;
     const float r2 = a.radius * a.radius;
     const float r2_box = (a.radius + 1e-4f) * (a.radius + 1e-4f);
-    const float4 rc = a.bb_ctr[rb];
-    const float4 re = a.bb_ext[rb];
+    const int rows = a.rows;
+    const int row_first = rb * rows;
+    const int row_n = min(rows, a.row_end - row_first);
+    if (warp == 0) {
+        // the row group's box, as block_bounds_warp computes a 32-slot block's
+        const bool valid = lane < row_n;
+        const float4 p = valid ? a.posw[row_first + lane] : make_float4(0.f, 0.f, 0.f, 0.f);
+        const float rx = __shfl_sync(FULL_MASK, p.x, 0);
+        const float ry = __shfl_sync(FULL_MASK, p.y, 0);
+        const float rz = __shfl_sync(FULL_MASK, p.z, 0);
+        const float dx = wrap_delta(p.x - rx, Lx, iLx);
+        const float dy = wrap_delta(p.y - ry, Ly, iLy);
+        const float dz = wrap_delta(p.z - rz, Lz, iLz);
+        float mnx = valid ? dx : 3.0e38f, mny = valid ? dy : 3.0e38f, mnz = valid ? dz : 3.0e38f;
+        float mxx = valid ? dx : -3.0e38f, mxy = valid ? dy : -3.0e38f, mxz = valid ? dz : -3.0e38f;
+        for (int o = 16; o > 0; o >>= 1) {
+            mnx = fminf(mnx, __shfl_xor_sync(FULL_MASK, mnx, o));
+            mny = fminf(mny, __shfl_xor_sync(FULL_MASK, mny, o));
+            mnz = fminf(mnz, __shfl_xor_sync(FULL_MASK, mnz, o));
+            mxx = fmaxf(mxx, __shfl_xor_sync(FULL_MASK, mxx, o));
+            mxy = fmaxf(mxy, __shfl_xor_sync(FULL_MASK, mxy, o));
+            mxz = fmaxf(mxz, __shfl_xor_sync(FULL_MASK, mxz, o));
+        }
+        if (lane == 0) {
+            row_box[0] = make_float4(rx + 0.5f * (mnx + mxx), ry + 0.5f * (mny + mxy), rz + 0.5f * (mnz + mxz), 0.f);
+            row_box[1] = make_float4(
+                0.5f * (mxx - mnx) * 1.000001f + 1e-6f, 0.5f * (mxy - mny) * 1.000001f + 1e-6f,
+                0.5f * (mxz - mnz) * 1.000001f + 1e-6f, 0.f);
+        }
+    }
+    __syncthreads();
+    const float4 rc = row_box[0];
+    const float4 re = row_box[1];
 
     // Row atoms are imaged next to the row block's centre. When every box
     // edge satisfies L/2 - extent >= radius, a column atom imaged next to the
@@ -590,8 +645,8 @@ __device__ __forceinline__ void build_tiles_cta(const TileArgs &a, const int rb,
     // distance is below the radius, so the per-pair test needs no wrapping.
     const bool shifted = 0.5f * Lx - re.x >= a.radius + 1e-3f && 0.5f * Ly - re.y >= a.radius + 1e-3f &&
                          0.5f * Lz - re.z >= a.radius + 1e-3f;
-    if (threadIdx.x < TILE) {
-        const int s = rb * TILE + threadIdx.x;
+    if (threadIdx.x < rows) {
+        const int s = row_first + threadIdx.x;
         float4 p = s < a.row_end ? a.posw[s] : make_float4(rc.x, rc.y, rc.z, 0.f);
         p.x = rc.x + wrap_delta(p.x - rc.x, Lx, iLx);
         p.y = rc.y + wrap_delta(p.y - rc.y, Ly, iLy);
@@ -603,7 +658,7 @@ __device__ __forceinline__ void build_tiles_cta(const TileArgs &a, const int rb,
         rem_count = 0;
     }
     __syncthreads();
-    const int row_n = min(TILE, a.row_end - rb * TILE);
+    const int col_lo = a.group ? a.col_begin : row_first; // first column slot of the group's pairs
     const long long base_tile = tile_base(a, rb);
     const unsigned lane_lt = (1u << lane) - 1;
 
@@ -615,7 +670,7 @@ __device__ __forceinline__ void build_tiles_cta(const TileArgs &a, const int rb,
     // idle; contiguous shares keep each warp's tiles spatially compact (the
     // slot order is a space-filling curve), which the pair kernel's
     // divergence depends on.
-    for (int wbase = a.group ? a.cb_first : rb; wbase < a.RB; wbase += TB_WARPS * 32) {
+    for (int wbase = a.group ? a.cb_first : row_first / TILE; wbase < a.RB; wbase += TB_WARPS * 32) {
         const int cb = wbase + (int)threadIdx.x;
         bool pass = false;
         if (cb < a.RB) {
@@ -656,7 +711,7 @@ __device__ __forceinline__ void build_tiles_cta(const TileArgs &a, const int rb,
             const float bx = fmaxf(0.f, fabsf(wx) - re.x);
             const float by = fmaxf(0.f, fabsf(wy) - re.y);
             const float bz = fmaxf(0.f, fabsf(wz) - re.z);
-            const bool need = valid && s >= a.col_begin && bx * bx + by * by + bz * bz < r2_box;
+            const bool need = valid && s >= col_lo && bx * bx + by * by + bz * bz < r2_box;
             bool hit = false;
             if (__any_sync(FULL_MASK, need)) {
                 if (shifted) {
@@ -892,7 +947,7 @@ static __global__ void __launch_bounds__(TB_WARPS * 32) k_rebuild(RebuildArgs r,
         const int warp = tid >> 5;
         const int n_warps = nth >> 5;
         for (int rb = warp; rb < r.ta.RB; rb += n_warps) {
-            lj_first_warp(r.pa, S, r.sa.n_first, rb, r.perm, r.slot_of);
+            lj_first_warp(r.pa, S, r.sa.n_first, rb, r.perm, r.slot_of, r.ta.rows);
             block_bounds_warp(S, rb, r.sa.box, r.ta.posw, const_cast<float4 *>(r.ta.bb_ctr), const_cast<float4 *>(r.ta.bb_ext));
         }
     }
@@ -1076,7 +1131,7 @@ __device__ __forceinline__ void pair_terms(
 // timemachine/cpp/src/kernels/k_nonbonded.cuh:424-546; the column
 // contribution of du_dx is the exact negation of the row contribution
 // (llrint is odd under round-half-even), so it is converted once.
-template <typename Real, bool U, bool DX, bool DL, bool DP, bool INTERP, bool ALCH, bool CHECK>
+template <typename Real, bool U, bool DX, bool DL, bool DP, bool INTERP, bool ALCH, bool CHECK, int RG = TILE>
 __device__ __forceinline__ void sweep_tile(
     const int lane,
     const unsigned S,
@@ -1126,12 +1181,15 @@ __device__ __forceinline__ void sweep_tile(
     unsigned long long &g_qj,
     unsigned long long &g_sigj,
     unsigned long long &g_epsj) {
-    const int src = (lane + 1) & 31;
+    // rows of RG < 32 slots: the warp is 32/RG lane groups, each sweeping RG
+    // of the tile's columns against the RG rows (lane l holds row l mod RG), so
+    // the columns rotate inside their lane group and a tile takes RG rounds
+    const int src = (lane & ~(RG - 1)) | ((lane + 1) & (RG - 1));
     // measured on B200: 4 rounds per iteration for the force-only variant,
     // no unrolling for the variants with more outputs (register pressure)
     constexpr int UNROLL = (DX && !U && !DL && !DP) ? 4 : 1;
 #pragma unroll UNROLL
-    for (int round = 0; round < TILE; round++) {
+    for (int round = 0; round < RG; round++) {
         Real delta_x = fsub(ci_x, cj_x);
         Real delta_y = fsub(ci_y, cj_y);
         Real delta_z = fsub(ci_z, cj_z);
@@ -1494,7 +1552,7 @@ __device__ __forceinline__ void sweep_tile_compact(
 // One tile of row block rows (lane = row slot i) against the 32 column slots
 // j, for one window: load, sweep, column atomics. Row accumulators are
 // returned to the caller.
-template <typename Real, bool U, bool DX, bool DL, bool DP, bool INTERP, bool COMPACT = false>
+template <typename Real, bool U, bool DX, bool DL, bool DP, bool INTERP, bool COMPACT = false, int RG = TILE>
 __device__ __forceinline__ void tile_pass(
     TileSmem *sm, // COMPACT: this warp's shared staging (accumulators zero on entry and on return)
     const PairArgs &a,
@@ -1543,7 +1601,7 @@ __device__ __forceinline__ void tile_pass(
     const bool row_alch = pwi.w != 0.f || (INTERP && (dpi.x != 0.f || dpi.y != 0.f || dpi.z != 0.f));
     const bool col_alch = pwj.w != 0.f || (INTERP && (dpj.x != 0.f || dpj.y != 0.f || dpj.z != 0.f));
     const bool alch = __any_sync(FULL_MASK, row_alch || col_alch);
-    if (COMPACT) {
+    if (COMPACT && RG == TILE) {
         sm->rpos[lane] = pwi;
         sm->rprm[lane] = pri;
         sm->cpos[lane] = pwj;
@@ -1617,10 +1675,10 @@ __device__ __forceinline__ void tile_pass(
     // needs the per-pair i < j test. The diagonal block is the first
     // candidate of the list builder's first warp, so a full one fills a tile
     // of its own; the flag is computed per tile either way.
-    const unsigned row_first = i & ~(unsigned)(TILE - 1);
-    const bool check = __any_sync(FULL_MASK, col_ok && j < row_first + TILE);
+    const unsigned row_first = i & ~(unsigned)(RG - 1);
+    const bool check = __any_sync(FULL_MASK, col_ok && j < row_first + RG);
 #define TMB_SWEEP(ALCH_, CHECK_)                                                                                      \
-    sweep_tile<Real, U, DX, DL, DP, INTERP, ALCH_, CHECK_>(                                                           \
+    sweep_tile<Real, U, DX, DL, DP, INTERP, ALCH_, CHECK_, RG>(                                                       \
         lane, S, i_eff, j, pwi.x, pwi.y, pwi.z, pwi.w, pri.x, pri.y, pri.z, pri.w, dpi.x, dpi.y, dpi.z, pwj.x, pwj.y,   \
         pwj.z, pwj.w, prj.x, prj.y, prj.z, prj.w, dpj.x, dpj.y, dpj.z, box_x, box_y, box_z, inv_box_x, inv_box_y,       \
         inv_box_z, cutoff_squared, beta, gi_x, gi_y, gi_z, g_qi, g_sigi, g_epsi, du_dl, energy, gj_x, gj_y, gj_z, g_qj, \
@@ -1683,11 +1741,56 @@ __device__ __forceinline__ void flush_row(
     }
 }
 
+// Row sums of a tile sweep with RG-slot row groups: the 32/RG lanes holding
+// one row combine their partial sums, and the first of them flushes.
+template <int RG, bool U, bool DX, bool DL, bool DP>
+__device__ __forceinline__ void flush_row_rg(
+    const Accum &acc_out,
+    unsigned i,
+    bool row_ok,
+    unsigned long long gi_x,
+    unsigned long long gi_y,
+    unsigned long long gi_z,
+    unsigned long long g_qi,
+    unsigned long long g_sigi,
+    unsigned long long g_epsi,
+    unsigned long long du_dl,
+    unsigned long long energy) {
+    if (RG < TILE) {
+#pragma unroll
+        for (int o = RG; o < TILE; o <<= 1) {
+            if (DX) {
+                gi_x += __shfl_xor_sync(FULL_MASK, gi_x, o);
+                gi_y += __shfl_xor_sync(FULL_MASK, gi_y, o);
+                gi_z += __shfl_xor_sync(FULL_MASK, gi_z, o);
+            }
+            if (DP) {
+                g_qi += __shfl_xor_sync(FULL_MASK, g_qi, o);
+                g_sigi += __shfl_xor_sync(FULL_MASK, g_sigi, o);
+                g_epsi += __shfl_xor_sync(FULL_MASK, g_epsi, o);
+            }
+            if (DL) {
+                du_dl += __shfl_xor_sync(FULL_MASK, du_dl, o);
+            }
+            if (U) {
+                energy += __shfl_xor_sync(FULL_MASK, energy, o);
+            }
+        }
+        if ((threadIdx.x & (TILE - 1)) >= RG) {
+            return;
+        }
+    }
+    if (row_ok) {
+        flush_row<U, DX, DL, DP>(acc_out, i, gi_x, gi_y, gi_z, g_qi, g_sigi, g_epsi, du_dl, energy);
+    }
+}
+
 // Multi-window calls: lists the tiles with at least one lambda-dependent row
 // or column atom (the tiles the pair kernel evaluates once per window). One
 // warp per work item, grid-stride.
 struct DepArgs {
     int S;
+    int rows; // slots per row group
     int row_end;
     const int4 *items;
     const unsigned *tile_cols;
@@ -1707,7 +1810,7 @@ static __global__ void k_dep_tiles(DepArgs a, DevState *state) {
     const int n_items = state->n_items;
     for (int w = warp; w < n_items; w += n_warps) {
         const int4 it = a.items[w];
-        const unsigned i = (unsigned)(it.x * TILE + lane);
+        const unsigned i = (unsigned)(it.x * a.rows + (lane & (a.rows - 1)));
         const bool row_dep = i < (unsigned)a.row_end && a.lamdep[i];
         for (int t = 0; t < it.z; t++) {
             const int tile = it.y + t;
@@ -1726,7 +1829,7 @@ static __global__ void k_dep_tiles(DepArgs a, DevState *state) {
 // MULTI (K > 1 windows): the tile items skip lambda-dependent tiles and add
 // into the shared accumulator block; each (tile, window) unit adds into the
 // window's block; a lambda-dependent scaled pair is evaluated for every window.
-template <typename Real, bool U, bool DX, bool DL, bool DP, bool INTERP, bool MULTI, bool COMPACT = false>
+template <typename Real, bool U, bool DX, bool DL, bool DP, bool INTERP, bool MULTI, bool COMPACT = false, int RG = TILE>
 __global__ void __launch_bounds__(128) k_pair(PairArgs a) {
     grid_dependency_wait();
     if (a.state->error) {
@@ -1795,20 +1898,18 @@ __global__ void __launch_bounds__(128) k_pair(PairArgs a) {
             const int unit = item - n_items;
             const int2 dt = a.dep_tiles[unit / a.K];
             const int k = unit % a.K;
-            const unsigned i = (unsigned)(dt.x * TILE + lane);
+            const unsigned i = (unsigned)(dt.x * RG + (lane & (RG - 1)));
             const unsigned j = a.tile_cols[(long long)dt.y * TILE + lane];
             const Accum wk = acc_block(a.acc, a.acc_block, 1 + k);
             unsigned long long wx = 0, wy = 0, wz = 0, wq = 0, ws = 0, we = 0, wl = 0, wu = 0;
-            tile_pass<Real, U, DX, DL, DP, INTERP, COMPACT>(
+            tile_pass<Real, U, DX, DL, DP, INTERP, COMPACT, RG>(
                 sm, a, lane, S, i, j, k, wk, box_x, box_y, box_z, inv_box_x, inv_box_y, inv_box_z, cutoff_squared, beta,
                 wx, wy, wz, wq, ws, we, wl, wu);
-            if (i < (unsigned)a.row_end) {
-                flush_row<U, DX, DL, DP>(wk, i, wx, wy, wz, wq, ws, we, wl, wu);
-            }
+            flush_row_rg<RG, U, DX, DL, DP>(wk, i, i < (unsigned)a.row_end, wx, wy, wz, wq, ws, we, wl, wu);
             continue;
         }
         const int4 it = a.items[item];
-        const unsigned i = (unsigned)(it.x * TILE + lane);
+        const unsigned i = (unsigned)(it.x * RG + (lane & (RG - 1)));
         const bool row_dep = MULTI && i < (unsigned)a.row_end && a.lamdep[i];
         unsigned long long gi_x = 0, gi_y = 0, gi_z = 0, g_qi = 0, g_sigi = 0, g_epsi = 0, du_dl = 0, energy = 0;
         for (int t = 0; t < it.z; t++) {
@@ -1817,13 +1918,12 @@ __global__ void __launch_bounds__(128) k_pair(PairArgs a) {
             if (MULTI && __any_sync(FULL_MASK, row_dep || (j < S && a.lamdep[j]))) {
                 continue; // evaluated per window by the (tile, window) units
             }
-            tile_pass<Real, U, DX, DL, DP, INTERP, COMPACT>(
+            tile_pass<Real, U, DX, DL, DP, INTERP, COMPACT, RG>(
                 sm, a, lane, S, i, j, 0, a.acc, box_x, box_y, box_z, inv_box_x, inv_box_y, inv_box_z, cutoff_squared,
                 beta, gi_x, gi_y, gi_z, g_qi, g_sigi, g_epsi, du_dl, energy);
         }
-        if (i < (unsigned)a.row_end) {
-            flush_row<U, DX, DL, DP>(a.acc, i, gi_x, gi_y, gi_z, g_qi, g_sigi, g_epsi, du_dl, energy);
-        }
+        flush_row_rg<RG, U, DX, DL, DP>(
+            a.acc, i, i < (unsigned)a.row_end, gi_x, gi_y, gi_z, g_qi, g_sigi, g_epsi, du_dl, energy);
     }
 }
 

@@ -82,6 +82,10 @@ class Potential:
         """Rotating (default) or compacted tile sweep; identical results."""
         _lib.check(self._lib.tmnb_potential_set_pair_schedule(self._h, 1 if compact else 0))
 
+    def set_tile_rows(self, rows=16):
+        """Rows per neighbour-list tile: 16 (default), 32 or 8 slots (identical results)."""
+        _lib.check(self._lib.tmnb_potential_set_tile_rows(self._h, int(rows)))
+
     def set_rebuild_mode(self, fused=False, conditional=False):
         """Neighbour-list rebuild as five kernels (default) or one cooperative
         launch (fused); under stream capture as plain nodes (default) or a
@@ -368,28 +372,34 @@ class Potential:
         _lib.check(self._lib.tmnb_potential_check_device_error(self._h, ctypes.c_void_p(stream)))
 
     def get_nblist(self, stream=None):
-        """(perm [S] slot -> atom, tiles) of the last rebuild; tiles[rb] is an
-        array of the column SLOTS (map them to atoms through perm) listed for
-        row block rb, whose rows are slots rb*32 .. rb*32+31."""
-        S, RB, cap = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_longlong()
-        _lib.check(self._lib.tmnb_potential_nblist_shape(self._h, ctypes.byref(S), ctypes.byref(RB), ctypes.byref(cap)))
+        """(perm [S] slot -> atom, tiles, rows) of the last rebuild; tiles[g] is
+        an array of the column SLOTS (map them to atoms through perm) listed for
+        row group g, whose rows are slots g*rows .. g*rows+rows-1."""
+        S, G, cap = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_longlong()
+        _lib.check(self._lib.tmnb_potential_nblist_shape(self._h, ctypes.byref(S), ctypes.byref(G), ctypes.byref(cap)))
+        rows, CB = ctypes.c_int32(), ctypes.c_int32()
+        _lib.check(self._lib.tmnb_potential_nblist_rows(self._h, ctypes.byref(rows), ctypes.byref(CB)))
         perm = np.zeros(S.value, dtype=np.uint32)
-        nt = np.zeros(RB.value, dtype=np.int32)
+        nt = np.zeros(G.value, dtype=np.int32)
         cols = np.zeros(cap.value * 32, dtype=np.uint32)
         s = 0
         if stream is not None:
             s = stream.cuda_stream if hasattr(stream, "cuda_stream") else stream
         _lib.check(self._lib.tmnb_potential_copy_nblist(self._h, ctypes.c_void_p(s), _ptr(perm), _ptr(nt), _ptr(cols)))
-        R = RB.value
+        R, cb = rows.value, CB.value
+        m = 32 // R
         nr = getattr(self, "_group_rows", None)
         tiles = []
-        for rb in range(R if nr is None else (nr + 31) // 32):
-            # row block rb's first tile: upper triangle, or (interaction group)
-            # R - nr//32 tiles per row block
-            off = rb * R - (rb * (rb - 1)) // 2 if nr is None else rb * (R - nr // 32)
-            c = cols[off * 32 : (off + nt[rb]) * 32]
+        for g in range(G.value):
+            if nr is None:
+                # upper triangle: group g reaches the column blocks from b = g*R/32 on
+                b = g // m
+                off = m * (b * cb - (b * (b - 1)) // 2) + (g - b * m) * (cb - b)
+            else:
+                off = g * (cb - nr // 32)
+            c = cols[off * 32 : (off + nt[g]) * 32]
             tiles.append(c[c < S.value])
-        return perm, tiles
+        return perm, tiles, R
 
     def nblist_stats(self, stream=None):
         """(tiles, work items, rebuilds) of the last neighbour-list build (synchronises)."""
