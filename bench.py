@@ -663,7 +663,10 @@ def run_batch_form():
         mode="eval",
         steps=2,
         repeats=1,
-        candidates=[dict(chunk=c, padding=p, grid_bits_offset=0, pair_ctas_per_sm=0) for c in (1, 2, 4, 8) for p in (0.06, 0.1)],
+        candidates=[
+            dict(chunk=c, padding=p, grid_bits_offset=0, pair_ctas_per_sm=0, rows=r)
+            for r in (16, 32) for c in (1, 2, 4, 8) for p in (0.06, 0.1)
+        ],
     )
     t_eval = timed(lambda: b.evaluate(), 3)
     batch_evals = 3 * n_rep / t_eval
@@ -710,7 +713,10 @@ def run_batch_form():
         mode="md",
         steps=20,
         repeats=1,
-        candidates=[dict(chunk=c, padding=p, grid_bits_offset=0, pair_ctas_per_sm=0) for c in (1, 2, 4, 8) for p in (0.06, 0.1)],
+        candidates=[
+            dict(chunk=c, padding=p, grid_bits_offset=0, pair_ctas_per_sm=0, rows=r)
+            for r in (16, 32) for c in (1, 2, 4, 8) for p in (0.06, 0.1)
+        ],
     )
     t_md = timed(lambda: b.md(BATCH_CHUNK, chunk=BATCH_CHUNK, use_graph=True), 1)
     md_replica_steps = n_rep * BATCH_CHUNK / t_md

@@ -511,6 +511,11 @@ tmnb_status tmnb_batch_bytes_in_use(tmnb_batch *b, unsigned long long *bytes);
  * occupancy). Applies to every replica (re-laid out, list rebuilt). */
 tmnb_status tmnb_batch_set_tuning(tmnb_batch *b, int chunk, double padding, int grid_bits_offset, int pair_ctas_per_sm);
 
+/* Rows per neighbour-list tile of every replica: 16 (default), 32 or 8 slots
+ * (identical results; as tmnb_potential_set_tile_rows). Every replica is
+ * re-laid out and rebuilds its list. */
+tmnb_status tmnb_batch_set_tile_rows(tmnb_batch *b, int rows);
+
 /* One evaluation of every replica (outputs overwritten; read them with
  * tmnb_batch_get). Asynchronous on the batch's stream. */
 tmnb_status tmnb_batch_evaluate(tmnb_batch *b, int compute_du_dx, int compute_du_dp, int compute_du_dl, int compute_u);

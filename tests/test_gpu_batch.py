@@ -113,7 +113,13 @@ def test_replica_md_equals_single_system_context():
 def test_graph_replay_equals_eager_and_tuning_changes_no_result():
     systems = _systems()[:3]
     runs = []
-    for use_graph, tuning in [(True, None), (False, None), (True, dict(chunk=2, padding=0.06, grid_bits_offset=1))]:
+    for use_graph, tuning in [
+        (True, None),
+        (False, None),
+        (True, dict(chunk=2, padding=0.06, grid_bits_offset=1)),
+        (True, dict(chunk=1, rows=32)),
+        (True, dict(chunk=4, rows=8)),
+    ]:
         b = ReplicaBatch()
         if tuning:
             b.set_tuning(**tuning)

@@ -101,6 +101,8 @@ def _declare(lib):
     lib.tmnb_potential_set_rebuild_mode.restype = ctypes.c_int
     lib.tmnb_potential_set_tile_rows.argtypes = [vp, i]
     lib.tmnb_potential_set_tile_rows.restype = ctypes.c_int
+    lib.tmnb_batch_set_tile_rows.argtypes = [vp, i]
+    lib.tmnb_batch_set_tile_rows.restype = ctypes.c_int
     lib.tmnb_potential_nblist_rows.argtypes = [vp, ctypes.POINTER(ctypes.c_int32), ctypes.POINTER(ctypes.c_int32)]
     lib.tmnb_potential_nblist_rows.restype = ctypes.c_int
     lib.tmnb_potential_adjoint_device.argtypes = [vp, i, i, vp, vp, vp, d, vp, d, vp, vp, vp]

@@ -46,7 +46,7 @@ class ReplicaBatch:
         _lib.check(self._lib.tmnb_batch_create(ctypes.byref(h)))
         self._h = h
         self._n = {}
-        self.tuning = {"chunk": 4, "padding": 0.1, "grid_bits_offset": 0, "pair_ctas_per_sm": 0}
+        self.tuning = {"chunk": 4, "padding": 0.1, "grid_bits_offset": 0, "pair_ctas_per_sm": 0, "rows": 16}
 
     def __del__(self):
         h, self._h = getattr(self, "_h", None), None
@@ -122,12 +122,18 @@ class ReplicaBatch:
         return sorted(self._n)
 
     # -- work ------------------------------------------------------------------
-    def set_tuning(self, chunk=4, padding=0.1, grid_bits_offset=0, pair_ctas_per_sm=0):
+    def set_tuning(self, chunk=4, padding=0.1, grid_bits_offset=0, pair_ctas_per_sm=0, rows=16):
+        """Schedule of every replica: tiles per work item, neighbour-list
+        padding, Hilbert grid offset, pair-kernel CTAs per SM (0: occupancy)
+        and rows per tile (32, 16 or 8). Results do not depend on it."""
+        if rows != self.tuning.get("rows", 16):
+            _lib.check(self._lib.tmnb_batch_set_tile_rows(self._h, int(rows)))
         _lib.check(
             self._lib.tmnb_batch_set_tuning(self._h, int(chunk), float(padding), int(grid_bits_offset), int(pair_ctas_per_sm))
         )
         self.tuning = {
             "chunk": chunk, "padding": padding, "grid_bits_offset": grid_bits_offset, "pair_ctas_per_sm": pair_ctas_per_sm,
+            "rows": rows,
         }
 
     def evaluate(self, du_dx=True, du_dp=True, du_dl=True, u=True):

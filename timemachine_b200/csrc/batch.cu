@@ -38,6 +38,7 @@ constexpr int TERM_BLOCK = 128; // bonded terms per block
 // Device-side descriptor of one replica (pointers into its arena).
 struct Rep {
     int N, RB, grid_bits, M;
+    int rows, NG; // slots per row group of the tile list, row groups
     int n_bonds, n_angles;
     int chunk, item_cap;
     double lambda, beta, cutoff, padding;
@@ -188,7 +189,10 @@ __device__ __forceinline__ void lj_first_rep(const Rep &r, int rb) {
         return;
     }
     const unsigned lt = (1u << lane) - 1u;
-    const int pos = lj ? __popc(m & lt) : __popc(m) + __popc(vm & ~m & lt);
+    const int seg = lane / r.rows; // LJ atoms first within each row group
+    const unsigned segm = (r.rows == TILE ? FULL_MASK : ((1u << r.rows) - 1u)) << (seg * r.rows);
+    const int pos = seg * r.rows +
+                    (lj ? __popc(m & lt & segm) : __popc(m & segm) + __popc(vm & ~m & lt & segm));
     __syncwarp();
     if (valid && lo + pos != s) {
         const int ns = lo + pos;
@@ -213,8 +217,8 @@ __global__ void k_b_bounds(const Rep *__restrict__ reps, const int2 *__restrict_
     block_bounds_warp(r.N, m.y, r.box, r.posw, r.bb_ctr, r.bb_ext);
 }
 
-__global__ void __launch_bounds__(TB_WARPS * 32) k_b_tiles(const Rep *__restrict__ reps, const int2 *__restrict__ rbmap) {
-    const int2 m = rbmap[blockIdx.x];
+__global__ void __launch_bounds__(TB_WARPS * 32) k_b_tiles(const Rep *__restrict__ reps, const int2 *__restrict__ gmap) {
+    const int2 m = gmap[blockIdx.x]; // (replica, row group)
     const Rep &r = reps[m.x];
     if (!r.state->rebuild || r.state->error) {
         return;
@@ -222,11 +226,11 @@ __global__ void __launch_bounds__(TB_WARPS * 32) k_b_tiles(const Rep *__restrict
     TileArgs ta;
     ta.S = r.N;
     ta.RB = r.RB;
-    ta.rows = TILE;
+    ta.rows = r.rows;
     ta.group = 0;
     ta.row_end = r.N;
     ta.col_begin = 0;
-    ta.n_row_blocks = r.RB;
+    ta.n_row_blocks = r.NG;
     ta.cb_first = 0;
     ta.radius = (float)(r.cutoff + r.padding + 1e-5);
     ta.box = r.box;
@@ -337,7 +341,7 @@ __device__ __forceinline__ PairArgs pair_args(const Rep &r) {
 }
 
 // Persistent pair kernel over every replica's work units.
-template <bool U, bool DX, bool DL, bool DP>
+template <bool U, bool DX, bool DL, bool DP, int RG>
 __global__ void __launch_bounds__(128) k_b_pair(const Rep *__restrict__ reps, int R, const int *__restrict__ prefix, int *counter) {
     const int lane = threadIdx.x & 31;
     const int total = prefix[R];
@@ -381,18 +385,16 @@ __global__ void __launch_bounds__(128) k_b_pair(const Rep *__restrict__ reps, in
             continue;
         }
         const int4 it = r.items[local];
-        const unsigned i = (unsigned)(it.x * TILE + lane);
+        const unsigned i = (unsigned)(it.x * RG + (lane & (RG - 1)));
         unsigned long long gi_x = 0, gi_y = 0, gi_z = 0, g_qi = 0, g_sigi = 0, g_epsi = 0, du_dl = 0, energy = 0;
         for (int t = 0; t < it.z; t++) {
             const long long tile = (long long)it.y + t;
             const unsigned j = r.tile_cols[tile * TILE + lane];
-            tile_pass<float, U, DX, DL, DP, false, false>(
+            tile_pass<float, U, DX, DL, DP, false, false, RG>(
                 nullptr, a, lane, S, i, j, 0, a.acc, box_x, box_y, box_z, inv_box_x, inv_box_y, inv_box_z, cutoff_squared, beta,
                 gi_x, gi_y, gi_z, g_qi, g_sigi, g_epsi, du_dl, energy);
         }
-        if (i < S) {
-            flush_row<U, DX, DL, DP>(a.acc, i, gi_x, gi_y, gi_z, g_qi, g_sigi, g_epsi, du_dl, energy);
-        }
+        flush_row_rg<RG, U, DX, DL, DP>(a.acc, i, i < S, gi_x, gi_y, gi_z, g_qi, g_sigi, g_epsi, du_dl, energy);
     }
 }
 
@@ -535,9 +537,16 @@ __global__ void k_b_step_done(const Rep *__restrict__ reps, int R) {
 }
 
 typedef void (*bpair_t)(const Rep *, int, const int *, int *);
-template <int I> constexpr bpair_t bpair() { return &k_b_pair<(I >> 3) & 1, (I >> 2) & 1, (I >> 1) & 1, I & 1>; }
+template <int I, int RG> constexpr bpair_t bpair() {
+    return &k_b_pair<(I >> 3) & 1, (I >> 2) & 1, (I >> 1) & 1, I & 1, RG>;
+}
+// [row-group size index: 0 -> 32, 1 -> 16, 2 -> 8][output flags]
 template <int... Is> struct BPairTable {
-    static void fill(bpair_t *out) { ((out[Is] = bpair<Is>()), ...); }
+    static void fill(bpair_t (*out)[16]) {
+        ((out[0][Is] = bpair<Is, 32>()), ...);
+        ((out[1][Is] = bpair<Is, 16>()), ...);
+        ((out[2][Is] = bpair<Is, 8>()), ...);
+    }
 };
 
 size_t align256(size_t b) { return (b + 255) & ~size_t(255); }
@@ -587,6 +596,19 @@ class BatchEngine {
         bits_off_ = grid_bits_offset;
         pair_ctas_ = pair_ctas_per_sm;
         // every replica is re-laid out; the new geometry takes effect at its (forced) rebuild
+        for (auto &kv : reps_) {
+            reconfigure(*kv.second);
+        }
+        table_dirty_ = true;
+    }
+
+    // Slots per row group of the replicas' tile lists (32, 16 or 8); every
+    // replica is re-laid out and rebuilds its list.
+    void set_tile_rows(int rows) {
+        if (rows != 32 && rows != 16 && rows != 8) {
+            throw Error(TMNB_ERR_INVALID_ARGUMENT, "rows per tile must be 32, 16 or 8");
+        }
+        rows_ = rows;
         for (auto &kv : reps_) {
             reconfigure(*kv.second);
         }
@@ -785,7 +807,7 @@ class BatchEngine {
         size_t posw, prm, lamdep, keys, perm, slot_of, nb_x, nb_box, bins_count, bins_cursor, bb_ctr, bb_ext, rb_ntiles;
         size_t tile_cols, items, acc, du_dx, du_dp, du_dl, u, md_step, state;
         size_t total;
-        int RB, grid_bits, item_cap;
+        int RB, NG, grid_bits, item_cap;
         long long tiles;
     };
 
@@ -832,11 +854,12 @@ class BatchEngine {
     Layout layout(int N, int M, int B, int A) const {
         Layout L{};
         L.RB = (N + TILE - 1) / TILE;
+        L.NG = (N + rows_ - 1) / rows_;
         L.grid_bits = grid_bits_for(N);
-        L.tiles = tile_offset(L.RB, L.RB);
+        L.tiles = tile_base_rows(L.NG, rows_, L.RB, 0, 0);
         long long cap = 0;
-        for (int rb = 0; rb < L.RB; rb++) {
-            cap += ((L.RB - rb) + chunk_ - 1) / chunk_;
+        for (int g = 0; g < L.NG; g++) {
+            cap += ((L.RB - (long long)g * rows_ / TILE) + chunk_ - 1) / chunk_;
         }
         L.item_cap = (int)std::max(1LL, cap);
         const size_t bins = (size_t)1 << (3 * L.grid_bits);
@@ -872,7 +895,7 @@ class BatchEngine {
         L.bins_cursor = take(4 * bins);
         L.bb_ctr = take(16 * (size_t)L.RB);
         L.bb_ext = take(16 * (size_t)L.RB);
-        L.rb_ntiles = take(4 * (size_t)L.RB);
+        L.rb_ntiles = take(4 * (size_t)L.NG);
         L.tile_cols = take(4 * (size_t)TILE * L.tiles);
         L.items = take(16 * (size_t)L.item_cap);
         L.acc = take(64 * (size_t)N);
@@ -894,6 +917,8 @@ class BatchEngine {
         Rep &r = slot.rep;
         r.N = s.N;
         r.RB = L.RB;
+        r.rows = rows_;
+        r.NG = L.NG;
         r.grid_bits = L.grid_bits;
         r.M = s.M;
         r.n_bonds = s.B;
@@ -1016,7 +1041,7 @@ class BatchEngine {
         CK(cudaStreamSynchronize(stream_));
         drop_graphs();
         std::vector<Rep> table;
-        std::vector<int2> ablk, rbmap, bmap, amap;
+        std::vector<int2> ablk, rbmap, gmap, bmap, amap;
         int q = 0;
         for (auto &kv : reps_) {
             const Rep &r = kv.second->rep;
@@ -1026,6 +1051,9 @@ class BatchEngine {
             }
             for (int rb = 0; rb < r.RB; rb++) {
                 rbmap.push_back(make_int2(q, rb));
+            }
+            for (int g = 0; g < r.NG; g++) {
+                gmap.push_back(make_int2(q, g));
             }
             for (int b0 = 0; b0 < r.n_bonds; b0 += TERM_BLOCK) {
                 bmap.push_back(make_int2(q, b0));
@@ -1038,12 +1066,14 @@ class BatchEngine {
         R_ = q;
         n_ablk_ = (int)ablk.size();
         n_rb_ = (int)rbmap.size();
+        n_gmap_ = (int)gmap.size();
         n_bmap_ = (int)bmap.size();
         n_amap_ = (int)amap.size();
         if (R_ > 0) {
             table_.upload(table.data(), table.size());
             ablk_.upload(ablk.data(), ablk.size());
             rbmap_.upload(rbmap.data(), rbmap.size());
+            gmap_.upload(gmap.data(), gmap.size());
             if (n_bmap_) {
                 bmap_.upload(bmap.data(), bmap.size());
             }
@@ -1055,9 +1085,11 @@ class BatchEngine {
         table_dirty_ = false;
     }
 
+    bpair_t pair_kernel(int flags) const { return pair_kernels_[rows_ == 32 ? 0 : (rows_ == 16 ? 1 : 2)][flags]; }
+
     int pair_grid(int flags) {
         int per_sm = 0;
-        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pair_kernels_[flags], 128, 0));
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, pair_kernel(flags), 128, 0));
         per_sm = std::max(1, per_sm);
         if (pair_ctas_ > 0) {
             per_sm = std::min(per_sm, pair_ctas_);
@@ -1071,9 +1103,9 @@ class BatchEngine {
         k_b_scan<<<R_, 1024, 0, stream_>>>(table_.p);
         k_b_scatter<<<n_ablk_, ATOM_BLOCK, 0, stream_>>>(table_.p, ablk_.p);
         k_b_bounds<<<(n_rb_ * 32 + 255) / 256, 256, 0, stream_>>>(table_.p, rbmap_.p, n_rb_);
-        k_b_tiles<<<n_rb_, TB_WARPS * 32, 0, stream_>>>(table_.p, rbmap_.p);
+        k_b_tiles<<<n_gmap_, TB_WARPS * 32, 0, stream_>>>(table_.p, gmap_.p);
         k_b_units<<<1, 1024, 0, stream_>>>(table_.p, R_, prefix_.p, counter_.p);
-        pair_kernels_[flags]<<<pair_grid(flags), 128, 0, stream_>>>(table_.p, R_, prefix_.p, counter_.p);
+        pair_kernel(flags)<<<pair_grid(flags), 128, 0, stream_>>>(table_.p, R_, prefix_.p, counter_.p);
         k_b_finalize<<<n_ablk_, ATOM_BLOCK, 0, stream_>>>(table_.p, ablk_.p, flags);
         k_b_zero_acc<<<n_ablk_, ATOM_BLOCK, 0, stream_>>>(table_.p, ablk_.p, flags);
     }
@@ -1134,11 +1166,12 @@ class BatchEngine {
     std::map<int, std::unique_ptr<Slot>> reps_;
     int next_id_ = 0;
     bool table_dirty_ = true;
-    int R_ = 0, n_ablk_ = 0, n_rb_ = 0, n_bmap_ = 0, n_amap_ = 0;
+    int R_ = 0, n_ablk_ = 0, n_rb_ = 0, n_gmap_ = 0, n_bmap_ = 0, n_amap_ = 0;
     DevBuf<Rep> table_;
-    DevBuf<int2> ablk_, rbmap_, bmap_, amap_;
+    DevBuf<int2> ablk_, rbmap_, gmap_, bmap_, amap_;
     DevBuf<int> prefix_, counter_;
-    bpair_t pair_kernels_[16];
+    bpair_t pair_kernels_[3][16];
+    int rows_ = 16; // slots per row group of every replica's tile list
     std::map<int, cudaGraphExec_t> graphs_;
     int chunk_ = 4;
     double padding_ = 0.1;
@@ -1278,6 +1311,13 @@ tmnb_status tmnb_batch_bytes_in_use(tmnb_batch *b, unsigned long long *bytes) {
         return null_argument();
     }
     return tmb::guarded([&] { *bytes = b->impl->bytes_in_use(); });
+}
+
+tmnb_status tmnb_batch_set_tile_rows(tmnb_batch *b, int rows) {
+    if (tmnb_status s = check_batch(b)) {
+        return s;
+    }
+    return tmb::guarded([&] { b->impl->set_tile_rows(rows); });
 }
 
 tmnb_status tmnb_batch_set_tuning(tmnb_batch *b, int chunk, double padding, int grid_bits_offset, int pair_ctas_per_sm) {
