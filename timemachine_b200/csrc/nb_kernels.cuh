@@ -1009,7 +1009,7 @@ struct PairArgs {
     int negated;
     Accum acc;             // block 0
     size_t acc_block;      // elements between accumulator blocks
-    const int2 *dep_tiles; // [n_dep] (row block, tile) of the lambda-dependent tiles (multi-window)
+    const int2 *dep_tiles; // [n_dep] (row group, tile) of the lambda-dependent tiles (multi-window)
     DevState *state;
 };
 
@@ -1125,8 +1125,9 @@ __device__ __forceinline__ void pair_terms(
     }
 }
 
-// One 32x32 tile: lane owns row slot i; the column atoms rotate through the
-// lanes by one position per round (32 rounds), carrying their accumulators.
+// One tile of RG rows x 32 columns: lane l owns row slot i (row l mod RG);
+// the column atoms rotate through the lanes of each RG-lane group by one
+// position per round (RG rounds), carrying their accumulators.
 // Per-pair arithmetic and validity follow
 // timemachine/cpp/src/kernels/k_nonbonded.cuh:424-546; the column
 // contribution of du_dx is the exact negation of the row contribution
@@ -1202,7 +1203,7 @@ __device__ __forceinline__ void sweep_tile(
             delta_w = fsub(ci_w, cj_w);
             d2 = add_w2(d2, delta_w);
         }
-        // CHECK: the tile holds atoms of the row block itself, so i < j decides
+        // CHECK: the tile holds atoms of the row group itself, so i < j decides
         // which lane evaluates each pair. Otherwise every column slot exceeds
         // every row slot, and padding rows/columns carry NaN coordinates,
         // which fail the cutoff test.
@@ -1549,7 +1550,7 @@ __device__ __forceinline__ void sweep_tile_compact(
     }
 }
 
-// One tile of row block rows (lane = row slot i) against the 32 column slots
+// One tile of a row group's rows (lane: row slot i) against the 32 column slots
 // j, for one window: load, sweep, column atomics. Row accumulators are
 // returned to the caller.
 template <typename Real, bool U, bool DX, bool DL, bool DP, bool INTERP, bool COMPACT = false, int RG = TILE>
@@ -1671,7 +1672,7 @@ __device__ __forceinline__ void tile_pass(
         return;
     }
     unsigned long long gj_x = 0, gj_y = 0, gj_z = 0, g_qj = 0, g_sigj = 0, g_epsj = 0;
-    // Only a tile holding atoms of the row block itself (the diagonal block)
+    // Only a tile holding atoms of the row group itself (the diagonal block)
     // needs the per-pair i < j test. The diagonal block is the first
     // candidate of the list builder's first warp, so a full one fills a tile
     // of its own; the flag is computed per tile either way.
@@ -1823,7 +1824,7 @@ static __global__ void k_dep_tiles(DepArgs a, DevState *state) {
 }
 
 // Persistent pair kernel over dynamically scheduled work units:
-//   [0, n_items)                 tile work items (row block, first tile, count);
+//   [0, n_items)                 tile work items (row group, first tile, count);
 //   MULTI only: [n_items, + n_dep*K)  one lambda-dependent tile at one window;
 //   then                         chunks of 32 scaled pairs (one per lane).
 // MULTI (K > 1 windows): the tile items skip lambda-dependent tiles and add
