@@ -713,10 +713,18 @@ class NonbondedPotential : public PotentialBase {
         return c;
     }
 
+    // persistent grid of the pair kernel k: occupancy x SMs (cached per kernel)
     int pair_grid(pair_kernel_t k, size_t smem) {
+        for (const auto &e : grid_cache_) {
+            if (e.first == k) {
+                return e.second;
+            }
+        }
         int per_sm = 0;
         CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, 128, smem));
-        return std::max(1, per_sm) * num_sms();
+        const int grid = std::max(1, per_sm) * num_sms();
+        grid_cache_.emplace_back(k, grid);
+        return grid;
     }
 
     // Returns the sticky device error (and clears it).
@@ -879,6 +887,7 @@ class NonbondedPotential : public PotentialBase {
     int cb_first_ = 0;     // interaction group: first column block
     int grid_bits_ = 4;
     int chunk_ = 1; // item capacity: one item per tile at most
+    std::vector<std::pair<pair_kernel_t, int>> grid_cache_;
     // slots per row group of the tile list; 16 measured fastest on B200 at
     // 22,840 atoms (MD step -7 %, 12-window call -6 % against 32)
     int rows_ = 16;
