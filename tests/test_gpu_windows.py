@@ -69,6 +69,36 @@ def test_interpolated_windows_equal_single_window(name):
     _assert_windows_equal(impl, g["x"], g["params"], g["box"], lams)
 
 
+def test_windows_follow_changed_lambda_dependence_without_rebuild():
+    """Interpolated parameters decide which atoms are lambda-dependent (p0 !=
+    p1). A multi-window call keeps its list of lambda-dependent tiles across
+    calls; when new parameters change that set while the atoms stay put (no
+    neighbour-list rebuild), the list must be redone: the windows equal a
+    fresh potential's."""
+    s = _ligand_system()
+    make = lambda: P.NonbondedInterpolated(
+        s.exclusion_idxs, s.scales, s.lambda_plane_idxs, np.zeros_like(s.lambda_offset_idxs), s.beta, s.cutoff
+    ).unbound_impl(np.float32)
+    lig = np.flatnonzero(s.lambda_offset_idxs != 0)
+    p_a = np.concatenate([s.params, s.params])
+    p_a[s.N + lig[: lig.size // 2], 0] *= 0.5  # first half of the ligand's charges change with lambda
+    p_b = np.concatenate([s.params, s.params])
+    p_b[s.N + lig[lig.size // 2 :], 0] *= 0.5  # now the other half
+    lams = np.linspace(0.0, 1.0, 6)
+    impl = make()
+    impl.execute_windows_fixed(s.x, p_a, s.box, lams)
+    rebuilds = impl.nblist_stats()[2]
+    got = impl.execute_windows_fixed(s.x, p_b, s.box, lams)
+    assert impl.nblist_stats()[2] == rebuilds  # same list, new lambda dependence
+    want = make().execute_windows_fixed(s.x, p_b, s.box, lams)
+    for c in (0, 1):
+        np.testing.assert_array_equal(got[c], want[c])
+    for c in (2, 3):
+        np.testing.assert_array_equal(got[c].sum(axis=1, dtype=np.uint64), want[c].sum(axis=1, dtype=np.uint64))
+    single = _single(impl, s.x, p_b, s.box, lams)
+    np.testing.assert_array_equal(got[0], single[0])
+
+
 def test_all_pairs_subset_and_pair_list_windows():
     rng = np.random.default_rng(2022)
     c = small_water_case(rng, 600)

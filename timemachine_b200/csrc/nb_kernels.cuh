@@ -41,6 +41,7 @@ struct DevState {
     unsigned total_tiles; // tiles produced by the last rebuild
     int rebuilds;         // number of rebuilds performed (diagnostics)
     int n_dep;            // lambda-dependent tiles listed by k_dep_tiles (multi-window calls)
+    int dep_dirty;        // 1: the list of lambda-dependent tiles must be redone (rebuild, or lamdep changed)
     unsigned prep_done;   // completion counter of k_check_prepare (graph-conditional rebuilds)
     int items_chunk;      // tiles per work item in the list of the last rebuild
     unsigned bar_count;   // grid barrier of k_rebuild: arrivals in the current phase
@@ -134,7 +135,6 @@ static __global__ void k_check_prepare(
     const int tid = blockIdx.x * blockDim.x + threadIdx.x;
     if (tid == 0) {
         state->next_item = 0;
-        state->n_dep = 0;
         state->bar_count = 0; // no k_rebuild of this state runs concurrently (stream order)
         if (nb_x != nullptr) {
             // Orthorhombic box whose every edge is at least twice cutoff+padding
@@ -174,7 +174,13 @@ static __global__ void k_check_prepare(
                 state->rebuild = 1; // benign race: every writer stores 1
             }
         }
+        const unsigned char dep_before = a.slots.lamdep[s];
         prepare_slot(a, s, atom);
+        if (a.slots.lamdep[s] != dep_before) {
+            // the lambda-dependent tiles change with it (benign race: every writer stores the same)
+            state->dep_dirty = 1;
+            state->n_dep = 0;
+        }
     }
     if (set_cond) {
         // The last block to finish sets the graph condition that gates the
@@ -847,6 +853,8 @@ __device__ __forceinline__ void build_tiles_cta(const TileArgs &a, const int rb,
     if (threadIdx.x == 0) {
         state->n_items = carry;
         state->items_chunk = a.chunk;
+        state->dep_dirty = 1; // the lambda-dependent tiles follow the new list
+        state->n_dep = 0;
         state->rebuilds += 1;
         state->done_ctas = 0;
         state->rebuild = 0;
@@ -1799,9 +1807,11 @@ struct DepArgs {
     int2 *dep_tiles;
 };
 
+// The list only changes with the tile list or the atoms' lambda dependence,
+// so a call with neither keeps the previous one (state->dep_dirty).
 static __global__ void k_dep_tiles(DepArgs a, DevState *state) {
     grid_dependency_wait();
-    if (state->error) {
+    if (state->error || !state->dep_dirty) {
         return;
     }
     const int lane = threadIdx.x & 31;
@@ -1862,6 +1872,9 @@ __global__ void __launch_bounds__(128) k_pair(PairArgs a) {
     const unsigned S = (unsigned)a.S;
     const int n_items = a.state->n_items;
     const int n_dep_units = MULTI ? a.state->n_dep * a.K : 0;
+    if (MULTI && blockIdx.x == 0 && threadIdx.x == 0) {
+        a.state->dep_dirty = 0; // k_dep_tiles (before this launch) has redone the list
+    }
     const int n_tiles_units = n_items + n_dep_units;
     const int n_total = n_tiles_units + (a.M + TILE - 1) / TILE;
 
