@@ -342,7 +342,7 @@ __device__ __forceinline__ PairArgs pair_args(const Rep &r) {
 
 // Persistent pair kernel over every replica's work units.
 template <bool U, bool DX, bool DL, bool DP, int RG>
-__global__ void __launch_bounds__(128) k_b_pair(const Rep *__restrict__ reps, int R, const int *__restrict__ prefix, int *counter) {
+__global__ void __launch_bounds__(128, (DX && !U && !DL && !DP) ? 8 : 5) k_b_pair(const Rep *__restrict__ reps, int R, const int *__restrict__ prefix, int *counter) {
     const int lane = threadIdx.x & 31;
     const int total = prefix[R];
     for (;;) {
