@@ -66,8 +66,6 @@ def parse():
         "the command profiled by ncu for the committed kernel summaries",
     )
     ap.add_argument("--profile-outputs", default="all", choices=["all", "du_dx", "u"])
-    ap.add_argument("--pair-schedule", default="rotating", choices=["rotating", "compact"],
-                    help="tile schedule of the pair kernel for --profile runs")
     ap.add_argument(
         "--profile-mode",
         default="windows",
@@ -131,7 +129,6 @@ def run_profile(args, local):
     s, x, p, lambdas = build_workload(0)
     impl = P.Nonbonded(s.exclusion_idxs, s.scales, s.lambda_plane_idxs, s.lambda_offset_idxs, s.beta, s.cutoff)
     impl = impl.unbound_impl(np.float32)
-    impl.set_pair_schedule(compact=args.pair_schedule == "compact")
     dev = torch.device("cuda", local)
     dx = torch.as_tensor(x, device=dev)
     dp = torch.as_tensor(p, device=dev).reshape(-1)

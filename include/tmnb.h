@@ -60,8 +60,12 @@ const char *tmnb_version(void);
  * neighbour list. Replaces the constructor
  * timemachine/cpp/src/nonbonded_all_pairs.cu:16-141 as bound at
  * timemachine/cpp/src/wrap_kernels.cpp:835-893 (NonbondedAllPairs_f32 and
- * NonbondedAllPairsInterpolated_f32). precision: 32 (FP32 pair arithmetic).
- * The lambda transforms are the identity ("lambda"), the reference default.
+ * NonbondedAllPairsInterpolated_f32, and the _f64 forms). precision: 32
+ * (FP32 pair arithmetic, bit-exact to the reference's _f32 kernels) or 64
+ * (FP64 pair arithmetic, the reference's _f64 kernels; 16-row tiles only).
+ * The lambda transforms start as the identity ("lambda"), the reference
+ * default; tmnb_potential_set_lambda_transforms sets others. The same
+ * precision values apply to every nonbonded constructor below.
  */
 tmnb_status tmnb_all_pairs_create(
     int N,
@@ -402,30 +406,29 @@ int tmnb_potential_num_params(const tmnb_potential *pot);
 int tmnb_potential_num_atoms(const tmnb_potential *pot);
 
 /*
- * Tile schedule of the pair kernel (no reference counterpart): 0 (default)
- * the rotating sweep, which evaluates a tile in 32 lane-rotation rounds; 1
- * the compacted sweep, which tests all 32x32 slots of a tile first and then
- * evaluates only the in-cutoff pairs, 32 at a time. The results are
- * identical; the switch exists for measurement. The compacted sweep runs on
- * 32-row tiles: selecting it sets the tile rows to 32, and setting other tile
- * rows (tmnb_potential_set_tile_rows) returns to the rotating sweep.
+ * Lambda transforms of a nonbonded handle: the four C-expression schedules
+ * in `lambda` that the reference constructors take as their last four
+ * arguments (transform_lambda_charge, _sigma, _epsilon, _w;
+ * timemachine/cpp/src/wrap_kernels.cpp:843-893, :901-958, :962-1013) and
+ * compile at run time (timemachine/cpp/src/kernels/k_lambda_transformer_jit.cuh).
+ * Here each expression is parsed once and evaluated on the host per call
+ * (value and exact derivative), so nothing is compiled at run time. NULL
+ * keeps "lambda". Non-interpolated handles use only the w schedule, as the
+ * reference's do. Supported: numeric literals (C integer rules), lambda, PI,
+ * + - * / % (unary + - !), comparisons, && ||, ?:, parentheses, and sin cos
+ * tan asin acos atan atan2 sinh cosh tanh exp log log10 sqrt pow fabs abs
+ * fmin fmax min max floor ceil. A parse error returns TMNB_ERR_INVALID_ARGUMENT
+ * with the offending position. The replica batch and the allocation-free
+ * entry point use the identity only; the adjoint needs the identity w schedule.
  */
-tmnb_status tmnb_potential_set_pair_schedule(tmnb_potential *pot, int compact);
+tmnb_status tmnb_potential_set_lambda_transforms(
+    tmnb_potential *pot, const char *charge, const char *sigma, const char *epsilon, const char *w);
 
-/*
- * How the neighbour list is rebuilt (no reference counterpart; the results
- * are identical in every mode, the switches exist for measurement):
- *   fused = 1: the sort, block bounds and tile build run as one cooperative
- *     launch with grid barriers between the phases, so a call that keeps its
- *     list pays one launch that returns at once; 0 (default): five kernels,
- *     each returning at once when no rebuild is due. On a 22,840-atom MD step
- *     the cooperative launch measured ~10 us slower per step.
- *   conditional = 1: inside a stream capture the rebuild launches go under a
- *     conditional graph node switched on by the rebuild check; 0 (default):
- *     plain nodes. On a 22,840-atom MD step the conditional form measured
- *     ~8 us slower per step than plain nodes.
- */
-tmnb_status tmnb_potential_set_rebuild_mode(tmnb_potential *pot, int fused, int conditional);
+/* Value f and derivative df/dlambda of one lambda-transform expression at
+ * lambda, as the staging uses them (host only, no GPU needed; no reference
+ * counterpart -- the reference evaluates its compiled transforms on the
+ * device). TMNB_ERR_INVALID_ARGUMENT on a parse error. */
+tmnb_status tmnb_lambda_transform_eval(const char *expression, double lambda, double *f, double *df);
 
 /*
  * Adjoint (no reference counterpart: the reference differentiates its jax

@@ -16,7 +16,11 @@ It restates the reference's jax implementation (jax is not installed here):
   d - box*floor(d/box + 0.5) (jax_utils.py:70-77) with an aperiodic 4th
   dimension, LJ kept where eps_ij != 0 and d < cutoff, electrostatics zeroed
   where d > cutoff, each pair counted once;
-- :341-354 interpolated: p = (1 - lambda) p0 + lambda p1.
+- :341-354 interpolated: p = (1 - lambda) p0 + lambda p1;
+- lambda transforms (tests/test_parameter_interpolation.py:73-150, the
+  reference's test of the four transform expressions): w uses f_w(lambda) and
+  each parameter column its own f(lambda), p = (1 - f) p0 + f p1, with the
+  transforms given here as torch functions of lambda.
 
 Derivatives come from torch float64 autograd, as the reference tests take
 jax.grad(argnums=(0, 1, 3)) (tests/common.py:448-450). Instead of the dense
@@ -71,13 +75,23 @@ def exclusion_masks(pairs, N, exclusion_idxs, scales):
     return cm, lm
 
 
-def energy(x, params, box, lam, plane, offset, beta, cutoff, pairs, charge_mask, lj_mask, interpolated=False):
-    """Total nonbonded energy (torch float64 scalar), differentiable in x, params, lam."""
+def _identity(lam):
+    return lam
+
+
+def energy(x, params, box, lam, plane, offset, beta, cutoff, pairs, charge_mask, lj_mask, interpolated=False,
+           transforms=None):
+    """Total nonbonded energy (torch float64 scalar), differentiable in x, params, lam.
+
+    transforms: None (identity) or (f_charge, f_sigma, f_epsilon, f_w), torch
+    functions of lambda."""
     diag = torch.diagonal(box)
     N = x.shape[0]
+    fq, fs, fe, fw = transforms if transforms is not None else (_identity,) * 4
     if interpolated:
-        params = (1 - lam) * params[:N] + lam * params[N:]
-    w = cutoff * (plane + offset * lam)
+        f = torch.stack([fq(lam), fs(lam), fe(lam)]).reshape(1, 3)
+        params = (1 - f) * params[:N] + f * params[N:]
+    w = cutoff * (plane + offset * fw(lam))
     i = torch.as_tensor(pairs[:, 0])
     j = torch.as_tensor(pairs[:, 1])
     dx = x[i] - x[j]
@@ -116,6 +130,7 @@ class Oracle:
         scales=None,
         interpolated=False,
         atom_idxs=None,
+        transforms=None,
     ):
         self.plane = np.asarray(lambda_plane_idxs, dtype=np.float64)
         self.offset = np.asarray(lambda_offset_idxs, dtype=np.float64)
@@ -125,6 +140,7 @@ class Oracle:
         self.scales = None if scales is None else np.asarray(scales)
         self.interpolated = interpolated
         self.atom_idxs = atom_idxs
+        self.transforms = transforms
 
     def pairs(self, x, box):
         return candidate_pairs(x, box, self.cutoff, self.atom_idxs)
@@ -153,13 +169,15 @@ class Oracle:
             cm,
             lm,
             self.interpolated,
+            self.transforms,
         )
         gx, gp, gl = torch.autograd.grad(u, [tx, tp, tl], allow_unused=True)
         gl = 0.0 if gl is None else float(gl)
         return gx.numpy(), gp.numpy(), gl, float(u.detach())
 
 
-def pair_list_oracle(x, params, box, lam, plane, offset, beta, cutoff, pair_idxs, scales, interpolated=False):
+def pair_list_oracle(x, params, box, lam, plane, offset, beta, cutoff, pair_idxs, scales, interpolated=False,
+                     transforms=None):
     """Energy/derivatives of the listed pairs only, each scaled by (charge_scale, lj_scale)
     (tests/nonbonded/test_nonbonded_pair_list.py:35-47: nonbonded_v3_on_specific_pairs x scales)."""
     pair_idxs = np.asarray(pair_idxs, dtype=np.int64).reshape(-1, 2)
@@ -181,13 +199,15 @@ def pair_list_oracle(x, params, box, lam, plane, offset, beta, cutoff, pair_idxs
         scales[:, 0],
         scales[:, 1],
         interpolated,
+        transforms,
     )
     gx, gp, gl = torch.autograd.grad(u, [tx, tp, tl], allow_unused=True)
     gl = 0.0 if gl is None else float(gl)
     return gx.numpy(), gp.numpy(), gl, float(u.detach())
 
 
-def interaction_group_oracle(x, params, box, lam, plane, offset, beta, cutoff, row_idxs, interpolated=False):
+def interaction_group_oracle(x, params, box, lam, plane, offset, beta, cutoff, row_idxs, interpolated=False,
+                             transforms=None):
     """Pairs (a, b) with a among row_idxs and b among the other atoms
     (timemachine/potentials/nonbonded.py:329-338, nonbonded_v3_interaction_groups
     over pairs_from_interaction_groups), unscaled."""
@@ -198,7 +218,7 @@ def interaction_group_oracle(x, params, box, lam, plane, offset, beta, cutoff, r
     pairs = candidate_pairs(x, box, cutoff)
     pairs = pairs[rows[pairs[:, 0]] != rows[pairs[:, 1]]]
     ones = np.ones((len(pairs), 2))
-    return pair_list_oracle(x, params, box, lam, plane, offset, beta, cutoff, pairs, ones, interpolated)
+    return pair_list_oracle(x, params, box, lam, plane, offset, beta, cutoff, pairs, ones, interpolated, transforms)
 
 
 def force_vjp_oracle(x, params, box, lam, plane, offset, beta, cutoff, exclusion_idxs, scales, g_du_dx, g_du_dl,

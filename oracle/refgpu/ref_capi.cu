@@ -38,20 +38,38 @@ namespace {
 
 thread_local std::string g_err;
 
-std::string jit_source(const std::string &kernel_dir) {
+std::string jit_source(
+    const std::string &kernel_dir,
+    const char *tq = nullptr,
+    const char *ts = nullptr,
+    const char *te = nullptr,
+    const char *tw = nullptr) {
     // the reference's constructor binding reads and patches this file
-    // (timemachine/cpp/src/wrap_kernels.cpp:869-879) with identity transforms
+    // (timemachine/cpp/src/wrap_kernels.cpp:869-879) with the four transforms
     std::ifstream t(kernel_dir + "/k_lambda_transformer_jit.cuh");
     if (!t) {
         throw std::runtime_error("cannot read " + kernel_dir + "/k_lambda_transformer_jit.cuh");
     }
     std::string src((std::istreambuf_iterator<char>(t)), std::istreambuf_iterator<char>());
     src = std::regex_replace(src, std::regex("KERNEL_DIR"), kernel_dir);
-    src = std::regex_replace(src, std::regex("CUSTOM_EXPRESSION_CHARGE"), "lambda");
-    src = std::regex_replace(src, std::regex("CUSTOM_EXPRESSION_SIGMA"), "lambda");
-    src = std::regex_replace(src, std::regex("CUSTOM_EXPRESSION_EPSILON"), "lambda");
-    src = std::regex_replace(src, std::regex("CUSTOM_EXPRESSION_W"), "lambda");
+    src = std::regex_replace(src, std::regex("CUSTOM_EXPRESSION_CHARGE"), tq ? tq : "lambda");
+    src = std::regex_replace(src, std::regex("CUSTOM_EXPRESSION_SIGMA"), ts ? ts : "lambda");
+    src = std::regex_replace(src, std::regex("CUSTOM_EXPRESSION_EPSILON"), te ? te : "lambda");
+    src = std::regex_replace(src, std::regex("CUSTOM_EXPRESSION_W"), tw ? tw : "lambda");
     return src;
+}
+
+// Applies f to the AllPairs part, whatever its precision and parameter mode.
+template <typename F> void with_all_pairs(timemachine::Potential *p, F &&f) {
+    if (auto *a = dynamic_cast<timemachine::NonbondedAllPairs<float, false> *>(p)) {
+        f(a);
+    } else if (auto *b = dynamic_cast<timemachine::NonbondedAllPairs<float, true> *>(p)) {
+        f(b);
+    } else if (auto *c = dynamic_cast<timemachine::NonbondedAllPairs<double, false> *>(p)) {
+        f(c);
+    } else if (auto *d = dynamic_cast<timemachine::NonbondedAllPairs<double, true> *>(p)) {
+        f(d);
+    }
 }
 
 struct RefNonbonded {
@@ -95,25 +113,38 @@ void *tmref_nonbonded_create(
     const int *offset,
     double beta,
     double cutoff,
-    int interpolated) {
+    int interpolated,
+    int precision,     // 32 (_f32 kernels) or 64 (_f64 kernels)
+    const char *tq,    // lambda transforms (NULL: "lambda")
+    const char *ts,
+    const char *te,
+    const char *tw) {
     RefNonbonded *h = nullptr;
     int rc = guarded([&] {
-        const std::string src = jit_source(kernel_dir);
+        const std::string src = jit_source(kernel_dir, tq, ts, te, tw);
         std::vector<int> pl(plane, plane + N), of(offset, offset + N);
         std::vector<int> ex(exclusion_idxs, exclusion_idxs + 2 * (size_t)M);
         std::vector<double> sc(scales, scales + 2 * (size_t)M);
         auto r = std::make_unique<RefNonbonded>();
         r->interpolated = interpolated != 0;
-        if (interpolated) {
-            r->all_pairs = std::make_shared<timemachine::NonbondedAllPairs<float, true>>(
-                pl, of, beta, cutoff, std::nullopt, src);
-            r->exclusions = std::make_shared<timemachine::NonbondedPairList<float, true, true>>(
-                ex, sc, pl, of, beta, cutoff, src);
+        auto build = [&](auto real_tag) {
+            using Real = decltype(real_tag);
+            if (interpolated) {
+                r->all_pairs = std::make_shared<timemachine::NonbondedAllPairs<Real, true>>(
+                    pl, of, beta, cutoff, std::nullopt, src);
+                r->exclusions = std::make_shared<timemachine::NonbondedPairList<Real, true, true>>(
+                    ex, sc, pl, of, beta, cutoff, src);
+            } else {
+                r->all_pairs = std::make_shared<timemachine::NonbondedAllPairs<Real, false>>(
+                    pl, of, beta, cutoff, std::nullopt, src);
+                r->exclusions = std::make_shared<timemachine::NonbondedPairList<Real, true, false>>(
+                    ex, sc, pl, of, beta, cutoff, src);
+            }
+        };
+        if (precision == 64) {
+            build(double{});
         } else {
-            r->all_pairs = std::make_shared<timemachine::NonbondedAllPairs<float, false>>(
-                pl, of, beta, cutoff, std::nullopt, src);
-            r->exclusions = std::make_shared<timemachine::NonbondedPairList<float, true, false>>(
-                ex, sc, pl, of, beta, cutoff, src);
+            build(float{});
         }
         r->fanout = std::make_shared<timemachine::FanoutSummedPotential>(
             std::vector<std::shared_ptr<timemachine::Potential>>{r->all_pairs, r->exclusions});
@@ -126,24 +157,12 @@ void tmref_nonbonded_destroy(void *h) { delete static_cast<RefNonbonded *>(h); }
 
 int tmref_set_nblist_padding(void *h, double padding) {
     auto *r = static_cast<RefNonbonded *>(h);
-    return guarded([&] {
-        if (r->interpolated) {
-            static_cast<timemachine::NonbondedAllPairs<float, true> *>(r->all_pairs.get())->set_nblist_padding(padding);
-        } else {
-            static_cast<timemachine::NonbondedAllPairs<float, false> *>(r->all_pairs.get())->set_nblist_padding(padding);
-        }
-    });
+    return guarded([&] { with_all_pairs(r->all_pairs.get(), [&](auto *a) { a->set_nblist_padding(padding); }); });
 }
 
 int tmref_disable_hilbert_sort(void *h) {
     auto *r = static_cast<RefNonbonded *>(h);
-    return guarded([&] {
-        if (r->interpolated) {
-            static_cast<timemachine::NonbondedAllPairs<float, true> *>(r->all_pairs.get())->disable_hilbert_sort();
-        } else {
-            static_cast<timemachine::NonbondedAllPairs<float, false> *>(r->all_pairs.get())->disable_hilbert_sort();
-        }
-    });
+    return guarded([&] { with_all_pairs(r->all_pairs.get(), [&](auto *a) { a->disable_hilbert_sort(); }); });
 }
 
 int tmref_execute_device(
@@ -180,17 +199,26 @@ void *tmref_group_create(
     const int *offset,
     double beta,
     double cutoff,
-    int interpolated) {
+    int interpolated,
+    int precision) { // 32 or 64
     RefPot *h = nullptr;
     int rc = guarded([&] {
         const std::string src = jit_source(kernel_dir);
         std::vector<int> pl(plane, plane + N), of(offset, offset + N);
         std::set<int> rows(row_idxs, row_idxs + NR);
         auto r = std::make_unique<RefPot>();
-        if (interpolated) {
-            r->pot = std::make_shared<timemachine::NonbondedInteractionGroup<float, true>>(rows, pl, of, beta, cutoff, src);
+        auto build = [&](auto real_tag) {
+            using Real = decltype(real_tag);
+            if (interpolated) {
+                r->pot = std::make_shared<timemachine::NonbondedInteractionGroup<Real, true>>(rows, pl, of, beta, cutoff, src);
+            } else {
+                r->pot = std::make_shared<timemachine::NonbondedInteractionGroup<Real, false>>(rows, pl, of, beta, cutoff, src);
+            }
+        };
+        if (precision == 64) {
+            build(double{});
         } else {
-            r->pot = std::make_shared<timemachine::NonbondedInteractionGroup<float, false>>(rows, pl, of, beta, cutoff, src);
+            build(float{});
         }
         h = r.release();
     });

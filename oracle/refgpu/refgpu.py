@@ -22,11 +22,13 @@ def available():
     return os.path.exists(LIB_PATH) and os.path.exists(os.path.join(KERNEL_DIR, "k_lambda_transformer_jit.cuh"))
 
 
-def build(reference_root="/root/reference"):
-    """Build oracle/_ref from the reference tree (only where the tree exists)."""
+def build(reference_root=None):
+    """Build oracle/_ref from the reference tree (only where the tree exists):
+    reference_root, else $TMNB_REFERENCE_ROOT."""
     import subprocess
 
-    if not os.path.isdir(reference_root):
+    reference_root = reference_root or os.environ.get("TMNB_REFERENCE_ROOT")
+    if not reference_root or not os.path.isdir(reference_root):
         return False
     subprocess.run(["make", "-C", HERE, f"REF={reference_root}", "-j8"], check=True)
     return True
@@ -41,14 +43,15 @@ def lib():
         vp, i, d = ctypes.c_void_p, ctypes.c_int, ctypes.c_double
         L.tmref_last_error.restype = ctypes.c_char_p
         L.tmref_nonbonded_create.restype = vp
-        L.tmref_nonbonded_create.argtypes = [ctypes.c_char_p, i, vp, vp, i, vp, vp, d, d, i]
+        cp = ctypes.c_char_p
+        L.tmref_nonbonded_create.argtypes = [cp, i, vp, vp, i, vp, vp, d, d, i, i, cp, cp, cp, cp]
         L.tmref_nonbonded_destroy.argtypes = [vp]
         L.tmref_set_nblist_padding.argtypes = [vp, d]
         L.tmref_disable_hilbert_sort.argtypes = [vp]
         L.tmref_execute_device.argtypes = [vp, i, i, vp, vp, vp, d, vp, vp, vp, vp, vp]
         L.tmref_execute_host.argtypes = [vp, i, i, vp, vp, vp, d, vp, vp, vp, vp]
         L.tmref_group_create.restype = vp
-        L.tmref_group_create.argtypes = [ctypes.c_char_p, i, vp, i, vp, vp, d, d, i]
+        L.tmref_group_create.argtypes = [ctypes.c_char_p, i, vp, i, vp, vp, d, d, i, i]
         L.tmref_pot_destroy.argtypes = [vp]
         L.tmref_pot_execute_host.argtypes = [vp, i, i, vp, vp, vp, d, vp, vp, vp, vp]
         L.tmref_md_create.restype = vp
@@ -69,9 +72,11 @@ def _check(rc):
 
 
 class RefNonbonded:
-    """FanoutSummedPotential([NonbondedAllPairs_f32, NonbondedPairList_f32_negated]) of the reference."""
+    """FanoutSummedPotential([NonbondedAllPairs_f32, NonbondedPairList_f32_negated]) of the reference
+    (the _f64 kernels with precision=64; transforms: the four lambda-transform expressions)."""
 
-    def __init__(self, exclusion_idxs, scales, plane, offset, beta, cutoff, interpolated=False):
+    def __init__(self, exclusion_idxs, scales, plane, offset, beta, cutoff, interpolated=False, precision=32,
+                 transforms=None):
         L = lib()
         exclusion_idxs = np.asarray(exclusion_idxs).reshape(-1, 2)
         scales = np.asarray(scales).reshape(-1, 2)
@@ -89,8 +94,10 @@ class RefNonbonded:
         e, s, pl, of = self._keep
         self.N = pl.size
         self.interpolated = interpolated
+        t = [None] * 4 if transforms is None else [x.encode() for x in transforms]
         self._h = L.tmref_nonbonded_create(
-            KERNEL_DIR.encode(), pl.size, _p(e), _p(s), e.shape[0], _p(pl), _p(of), beta, cutoff, 1 if interpolated else 0
+            KERNEL_DIR.encode(), pl.size, _p(e), _p(s), e.shape[0], _p(pl), _p(of), beta, cutoff,
+            1 if interpolated else 0, int(precision), *t,
         )
         if not self._h:
             raise RuntimeError(L.tmref_last_error().decode())
@@ -133,9 +140,9 @@ class RefNonbonded:
 
 
 class RefInteractionGroup:
-    """NonbondedInteractionGroup(_Interpolated)_f32 of the reference."""
+    """NonbondedInteractionGroup(_Interpolated)_f32 (or _f64, precision=64) of the reference."""
 
-    def __init__(self, row_idxs, plane, offset, beta, cutoff, interpolated=False):
+    def __init__(self, row_idxs, plane, offset, beta, cutoff, interpolated=False, precision=32):
         L = lib()
         self._keep = [
             np.ascontiguousarray(row_idxs, dtype=np.int32),
@@ -144,7 +151,8 @@ class RefInteractionGroup:
         ]
         r, pl, of = self._keep
         self._h = L.tmref_group_create(
-            KERNEL_DIR.encode(), pl.size, _p(r), r.size, _p(pl), _p(of), beta, cutoff, 1 if interpolated else 0
+            KERNEL_DIR.encode(), pl.size, _p(r), r.size, _p(pl), _p(of), beta, cutoff, 1 if interpolated else 0,
+            int(precision),
         )
         if not self._h:
             raise RuntimeError(L.tmref_last_error().decode())

@@ -73,4 +73,8 @@ def convert(ref_root):
 
 
 if __name__ == "__main__":
-    convert(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    # the reference source tree: first argument, else $TMNB_REFERENCE_ROOT
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("TMNB_REFERENCE_ROOT")
+    if not root:
+        sys.exit("usage: make_golden.py <reference tree>  (or set TMNB_REFERENCE_ROOT)")
+    convert(root)

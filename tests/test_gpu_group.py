@@ -96,7 +96,9 @@ def test_fixed_point_identity_all_equals_rows_plus_cols_plus_group():
             a, r, cc, g = (o[c] for o in outs)
             if c >= 2:
                 a, r, cc, g = (v.sum(dtype=np.uint64) for v in (a, r, cc, g))
-            np.testing.assert_array_equal(a, r + cc + g, err_msg=f"{name} lambda={lam}")
+            # uint64 sums wrap modulo 2^64, as the fixed-point accumulators do
+            total = np.add(np.add(r, cc, dtype=np.uint64), g, dtype=np.uint64)
+            np.testing.assert_array_equal(a, total, err_msg=f"{name} lambda={lam}")
 
 
 def test_multi_window_equals_single_window():

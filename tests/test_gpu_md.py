@@ -75,19 +75,17 @@ def test_graph_replay_equals_eager_bitwise():
 
 
 @pytest.mark.parametrize("n_waters,edge,dt", [(500, 2.9, 2.0e-3), (3000, 4.48, 0.5e-3)])
-def test_rebuild_modes_graph_and_eager_agree(n_waters, edge, dt):
-    """Every rebuild mode (one cooperative launch or five kernels; plain or
-    conditional graph nodes) and eager launches give the same trajectory, du_dl
-    and number of rebuilds; captured steps also record the potentials on
-    parallel branches. The larger box takes the tile build's shifted-image
-    test, the smaller one its per-pair wrapped test."""
+def test_rebuild_cadence_graph_and_eager_agree(n_waters, edge, dt):
+    """Graph-replayed and eager steps give the same trajectory, du_dl and
+    number of rebuilds, with several rebuilds and steps without one in
+    between; captured steps also record the potentials on parallel branches.
+    The larger box takes the tile build's shifted-image test, the smaller one
+    its per-pair wrapped test."""
     s = testsystems.build_system(n_waters, edge, seed=7, n_ligand=10)
     lam = np.full(120, 0.3)
     runs = []
-    modes = [(True, False, False), (True, True, False), (True, True, True), (True, False, True), (False, False, False)]
-    for use_graphs, fused, conditional in modes:
+    for use_graphs in (True, False):
         ctx, bps = _context(s, use_graphs, dt=dt, barostat_interval=25)
-        bps[2].potential.set_rebuild_mode(fused=fused, conditional=conditional)
         dl, _, _ = ctx.multiple_steps(lam, store_du_dl_interval=20)
         rebuilds = bps[2].potential.nblist_stats()[2]
         runs.append((ctx.get_x_t(), ctx.get_v_t(), ctx.get_box(), dl, rebuilds))

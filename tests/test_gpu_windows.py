@@ -190,33 +190,3 @@ def test_windows_bitexact_against_reference_build():
         np.testing.assert_array_equal(mdp[k], rdp)
         assert mdl[k].sum(dtype=np.uint64) == rdl.sum(dtype=np.uint64)
         assert mu[k].sum(dtype=np.uint64) == ru.sum(dtype=np.uint64)
-
-
-@pytest.mark.parametrize("case", ["ligand", "golden_repro", "pair_list"])
-def test_compacted_and_rotating_tile_sweeps_agree_bitwise(case):
-    """The two tile schedules of the pair kernel evaluate the same pairs with
-    the same arithmetic: raw outputs agree bit for bit (one and 7 windows)."""
-    if case == "ligand":
-        s = _ligand_system()
-        make = lambda: P.Nonbonded(s.exclusion_idxs, s.scales, s.lambda_plane_idxs, s.lambda_offset_idxs, s.beta,
-                                   s.cutoff).unbound_impl(np.float32)
-        x, p, box = s.x, s.params, s.box
-    elif case == "golden_repro":
-        g = load_golden("repro")
-        make = lambda: P.NonbondedInterpolated(g["exclusion_idxs"], g["scales"], g["lambda_plane_idxs"],
-                                               g["lambda_offset_idxs"], g["beta"], g["cutoff"]).unbound_impl(np.float32)
-        x, p, box = g["x"], g["params"], g["box"]
-    else:
-        c = small_water_case(np.random.default_rng(7), 900)
-        make = lambda: P.NonbondedPairListNegated(c["exclusion_idxs"], c["scales"], c["plane"], c["offset"], 2.0,
-                                                  1.0).unbound_impl(np.float32)
-        x, p, box = c["x"], c["params"], c["box"]
-    a, b = make(), make()
-    b.set_pair_schedule(compact=True)
-    for lams in [np.array([0.3]), np.linspace(0.0, 1.0, 7)]:
-        ra = a.execute_windows_fixed(x, p, box, lams)
-        rb = b.execute_windows_fixed(x, p, box, lams)
-        np.testing.assert_array_equal(ra[0], rb[0])
-        np.testing.assert_array_equal(ra[1], rb[1])
-        np.testing.assert_array_equal(ra[2].sum(axis=1, dtype=np.uint64), rb[2].sum(axis=1, dtype=np.uint64))
-        np.testing.assert_array_equal(ra[3].sum(axis=1, dtype=np.uint64), rb[3].sum(axis=1, dtype=np.uint64))

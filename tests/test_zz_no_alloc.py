@@ -116,3 +116,36 @@ def test_static_entry_rejects_sizes_beyond_capacity():
     assert rc == 1  # TMNB_ERR_INVALID_ARGUMENT
     msg = lib.tmnb_last_error().decode()
     assert "exceeds the static scratch capacity of 32768 atoms" in msg
+
+
+def test_static_entry_reports_bad_pairs_and_recovers():
+    """A pair index outside [0, N) or a pair with src == dst is found on the
+    device and returned as TMNB_ERR_INVALID_ARGUMENT with the outputs left
+    unchanged (the pair kernel returns before reading any pair); the next
+    valid call starts clean and matches the allocating entry point."""
+    lib = _lib.lib()
+    c = _case(False)
+    N = c["x"].shape[0]
+    stream = torch.cuda.current_stream().cuda_stream
+    for bad in ([[0, N], [1, 2]], [[3, 3], [1, 2]]):
+        pairs = _dev(np.asarray(bad), torch.int32)
+        scales = _dev(np.ones((2, 2)), torch.float64)
+        plane = _dev(c["plane"], torch.int32)
+        offset = _dev(c["offset"], torch.int32)
+        x, p, box = _dev(c["x"], torch.float64), _dev(c["params"], torch.float64), _dev(c["box"], torch.float64)
+        outs = _zeros(N)
+        rc = lib.tmnb_pair_list_execute_static(
+            N, 2, _addr(pairs), _addr(scales), _addr(plane), _addr(offset), 2.0, 1.0, 0, _addr(x), _addr(p),
+            _addr(box), 0.4, *[_addr(o) for o in outs], ctypes.c_void_p(stream),
+        )
+        torch.cuda.synchronize()
+        assert rc == 1  # TMNB_ERR_INVALID_ARGUMENT
+        assert "pair index out of range [0, N) or src == dst" in lib.tmnb_last_error().decode()
+        for o in outs:
+            assert not torch.any(o != 0)
+    ref = _zeros(N)
+    _allocating(c, False, 0.4, ref)
+    got = _zeros(N)
+    _static(c, False, 0.4, got)
+    for r, g in zip(ref, got):
+        np.testing.assert_array_equal(g.cpu().numpy(), r.cpu().numpy())

@@ -22,19 +22,64 @@ NVCC_FLAGS = [
     "arch=compute_100a,code=sm_100a",
     "-Xcompiler",
     "-fPIC",
-    "-shared",
 ]
 
-SOURCES = ["nonbonded.cu", "md.cu", "bonded.cu", "batch.cu", "static_pairlist.cu"]
+# The pair-kernel variants are split over their own translation units
+# (pair_*.cu) so that they compile in parallel.
+SOURCES = [
+    "nonbonded.cu",
+    "md.cu",
+    "bonded.cu",
+    "batch.cu",
+    "static_pairlist.cu",
+    "pair_f32_r32.cu",
+    "pair_f32_r32_interp.cu",
+    "pair_f32_r16.cu",
+    "pair_f32_r16_interp.cu",
+    "pair_f32_r8.cu",
+    "pair_f32_r8_interp.cu",
+    "pair_f64_r16.cu",
+    "pair_f64_r16_interp.cu",
+]
+BUILD_DIR = os.path.join(HERE, "_build")
 
 
-def build(verbose: bool = False) -> str:
-    """Compile libtmnb.so for sm_100a (nvcc cross-compiles without a GPU)."""
+def build(verbose: bool = False, jobs: int = 0) -> str:
+    """Compile libtmnb.so for sm_100a (nvcc cross-compiles without a GPU).
+
+    Each source compiles to its own object in parallel; an object is rebuilt
+    when it is older than its source or than any header of csrc/ and include/.
+    """
     nvcc = os.environ.get("NVCC", "nvcc")
-    cmd = [nvcc, *NVCC_FLAGS, "-I" + INCLUDE, "-o", LIB_PATH] + [os.path.join(CSRC, s) for s in SOURCES]
+    os.makedirs(BUILD_DIR, exist_ok=True)
+    headers = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".hpp", ".h"))]
+    headers += [os.path.join(INCLUDE, f) for f in os.listdir(INCLUDE)]
+    newest_header = max(os.path.getmtime(h) for h in headers)
+    objs, todo = [], []
+    for src in SOURCES:
+        path = os.path.join(CSRC, src)
+        obj = os.path.join(BUILD_DIR, src[:-3] + ".o")
+        objs.append(obj)
+        if not os.path.exists(obj) or os.path.getmtime(obj) < max(os.path.getmtime(path), newest_header):
+            todo.append([nvcc, *NVCC_FLAGS, "-I" + INCLUDE, "-c", path, "-o", obj])
+    jobs = jobs or max(1, min(len(todo), os.cpu_count() or 1))
+    running = []
+    failed = []
+    while todo or running:
+        while todo and len(running) < jobs:
+            cmd = todo.pop(0)
+            if verbose:
+                print(" ".join(cmd), flush=True)
+            running.append((cmd, subprocess.Popen(cmd)))
+        cmd, proc = running.pop(0)
+        if proc.wait() != 0:
+            failed.append(cmd[-3])
+    if failed:
+        raise RuntimeError("nvcc failed on " + ", ".join(failed))
+    link = [nvcc, "-shared", "-gencode", "arch=compute_100a,code=sm_100a", "-o", LIB_PATH, *objs]
     if verbose:
-        print(" ".join(cmd))
-    subprocess.run(cmd, check=True)
+        print(" ".join(link), flush=True)
+    subprocess.run(link, check=True)
     return LIB_PATH
 
 
@@ -95,10 +140,11 @@ def _declare(lib):
     lib.tmnb_harmonic_angle_create.argtypes = [i, i, vp, vp, vp, ctypes.POINTER(vp)]
     lib.tmnb_pair_list_execute_static.argtypes = [i, i, vp, vp, vp, vp, d, d, i, vp, vp, vp, d, vp, vp, vp, vp, vp]
     lib.tmnb_pair_list_execute_static.restype = ctypes.c_int
-    lib.tmnb_potential_set_pair_schedule.argtypes = [vp, i]
-    lib.tmnb_potential_set_pair_schedule.restype = ctypes.c_int
-    lib.tmnb_potential_set_rebuild_mode.argtypes = [vp, i, i]
-    lib.tmnb_potential_set_rebuild_mode.restype = ctypes.c_int
+    cp = ctypes.c_char_p
+    lib.tmnb_potential_set_lambda_transforms.argtypes = [vp, cp, cp, cp, cp]
+    lib.tmnb_potential_set_lambda_transforms.restype = ctypes.c_int
+    lib.tmnb_lambda_transform_eval.argtypes = [cp, d, c_double_p, c_double_p]
+    lib.tmnb_lambda_transform_eval.restype = ctypes.c_int
     lib.tmnb_potential_set_tile_rows.argtypes = [vp, i]
     lib.tmnb_potential_set_tile_rows.restype = ctypes.c_int
     lib.tmnb_batch_set_tile_rows.argtypes = [vp, i]

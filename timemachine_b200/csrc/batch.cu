@@ -311,6 +311,9 @@ __device__ __forceinline__ PairArgs pair_args(const Rep &r) {
     a.posw = r.posw;
     a.prm = r.prm;
     a.dprm = nullptr;
+    a.posw64 = nullptr;
+    a.prm64 = nullptr;
+    a.dprm64 = nullptr;
     a.lamdep = r.lamdep;
     a.box = r.box;
     a.beta = r.beta;
@@ -390,8 +393,8 @@ __global__ void __launch_bounds__(128, (DX && !U && !DL && !DP) ? 8 : 5) k_b_pai
         for (int t = 0; t < it.z; t++) {
             const long long tile = (long long)it.y + t;
             const unsigned j = r.tile_cols[tile * TILE + lane];
-            tile_pass<float, U, DX, DL, DP, false, false, RG>(
-                nullptr, a, lane, S, i, j, 0, a.acc, box_x, box_y, box_z, inv_box_x, inv_box_y, inv_box_z, cutoff_squared, beta,
+            tile_pass<float, U, DX, DL, DP, false, RG>(
+                a, lane, S, i, j, 0, a.acc, box_x, box_y, box_z, inv_box_x, inv_box_y, inv_box_z, cutoff_squared, beta,
                 gi_x, gi_y, gi_z, g_qi, g_sigi, g_epsi, du_dl, energy);
         }
         flush_row_rg<RG, U, DX, DL, DP>(a.acc, i, i < S, gi_x, gi_y, gi_z, g_qi, g_sigi, g_epsi, du_dl, energy);

@@ -42,16 +42,12 @@ struct DevState {
     int rebuilds;         // number of rebuilds performed (diagnostics)
     int n_dep;            // lambda-dependent tiles listed by k_dep_tiles (multi-window calls)
     int dep_dirty;        // 1: the list of lambda-dependent tiles must be redone (rebuild, or lamdep changed)
-    unsigned prep_done;   // completion counter of k_check_prepare (graph-conditional rebuilds)
     int items_chunk;      // tiles per work item in the list of the last rebuild
-    unsigned bar_count;   // grid barrier of k_rebuild: arrivals in the current phase
-    unsigned bar_gen;     // grid barrier of k_rebuild: completed phases
 };
 
 // Error codes written into DevState::error (mirrored in include/tmnb.h).
 constexpr int DEV_ERR_NONORTHO_BOX = 3;
 constexpr int DEV_ERR_BOX_TOO_SMALL = 4;
-constexpr int DEV_ERR_BARRIER_TIMEOUT = 6; // a grid barrier gave up waiting (bounded spin)
 
 // Up to this many lambda windows are evaluated together (one launch sequence).
 constexpr int MAX_WINDOWS = TMNB_MAX_WINDOWS;
@@ -59,8 +55,23 @@ constexpr int MAX_WINDOWS = TMNB_MAX_WINDOWS;
 struct SlotArrays {
     float4 *posw;            // [K][S] x, y, z, w(lambda_k)
     float4 *prm;             // [K][S] q, sig, eps, dw/dlambda (parameters at lambda_k)
-    float4 *dprm;            // [S] dq/dl, dsig/dl, deps/dl, 0 (interpolated only)
+    float4 *dprm;            // [K][S] dq/dl, dsig/dl, deps/dl, 0 (interpolated only)
     unsigned char *lamdep;   // [S] 1 when the atom's staged values depend on lambda
+    // FP64 pair arithmetic only (nullptr otherwise): the same values unrounded
+    double4 *posw64;         // [K][S]
+    double4 *prm64;          // [K][S]
+    double4 *dprm64;         // [K][S] (interpolated only)
+};
+
+// One lambda window as the staging sees it: the values f(lambda) and
+// derivatives g = df/dlambda of the four lambda transforms (charge, sigma,
+// epsilon, w) of timemachine/cpp/src/kernels/k_lambda_transformer_jit.cuh:8-22,
+// evaluated on the host for each call (identity transform: f = lambda, g = 1).
+struct LambdaWindow {
+    double f_q, g_q;
+    double f_s, g_s;
+    double f_e, g_e;
+    double f_w, g_w;
 };
 
 struct PrepareArgs {
@@ -70,7 +81,7 @@ struct PrepareArgs {
     const double *p;            // [N,3] or [2N,3] (interpolated)
     const double *box;          // [3,3]
     int K;                      // lambda windows
-    double lambdas[MAX_WINDOWS];
+    LambdaWindow lam[MAX_WINDOWS];
     double cutoff;
     double padding;
     const int *plane;           // [N]
@@ -79,45 +90,67 @@ struct PrepareArgs {
     SlotArrays slots;
 };
 
-// Stage one atom into its slot, for every window. w = cutoff*(plane + offset*lambda),
-// dw/dlambda = offset*cutoff (timemachine/cpp/src/kernels/k_lambda_transformer_jit.cuh:25-55
-// with the identity lambda transform); interpolated parameters
-// p = (1-lambda) p0 + lambda p1, dp/dlambda = p1 - p0 (same file :57-98).
-// An atom is lambda-dependent when its w or its parameters change with lambda
-// (offset != 0, or p0 != p1); pairs of lambda-independent atoms give the same
-// per-pair values in every window.
+// Stage one atom into its slot, for every window k, with the transforms of
+// window k: w = cutoff*(plane + offset*f_w), dw/dlambda = offset*g_w*cutoff
+// (timemachine/cpp/src/kernels/k_lambda_transformer_jit.cuh:25-55);
+// interpolated parameters p = (1-f) p0 + f p1 and dp/dlambda = g (p1 - p0)
+// per parameter column (same file :57-98). The atom is lambda-dependent when
+// its offset is nonzero, its end states differ, or any window stages values
+// other than window 0's: pairs of lambda-independent atoms give the same
+// per-pair values in every window, bit for bit.
 __device__ __forceinline__ void prepare_slot(const PrepareArgs &a, int s, int atom) {
     const int plane = a.plane[atom];
     const int offset = a.offset[atom];
-    const double f_lambda_grad = 1.0;
-    const double dw_dl = offset * f_lambda_grad * a.cutoff;
     const double *xa = a.x + 3 * (size_t)atom;
-    const float fx = (float)xa[0], fy = (float)xa[1], fz = (float)xa[2];
-    bool dep = offset != 0;
+    const double x0 = xa[0], x1 = xa[1], x2 = xa[2];
+    const float fx = (float)x0, fy = (float)x1, fz = (float)x2;
     const double *p0 = a.p + 3 * (size_t)atom;
-    const double *p1 = a.p + 3 * ((size_t)a.N + atom);
+    const double q0 = p0[0], s0 = p0[1], e0 = p0[2];
+    double q1 = q0, s1 = s0, e1 = e0;
+    bool dep = offset != 0;
     if (a.interpolated) {
-        double dq = f_lambda_grad * (p1[0] - p0[0]);
-        double ds = f_lambda_grad * (p1[1] - p0[1]);
-        double de = f_lambda_grad * (p1[2] - p0[2]);
-        a.slots.dprm[s] = make_float4((float)dq, (float)ds, (float)de, 0.0f);
-        dep = dep || p0[0] != p1[0] || p0[1] != p1[1] || p0[2] != p1[2];
+        const double *p1 = a.p + 3 * ((size_t)a.N + atom);
+        q1 = p1[0];
+        s1 = p1[1];
+        e1 = p1[2];
+        dep = dep || q0 != q1 || s0 != s1 || e0 != e1;
     }
-    a.slots.lamdep[s] = dep ? 1 : 0;
+    double first[6] = {0, 0, 0, 0, 0, 0};
     for (int k = 0; k < a.K; k++) {
-        const double f_lambda = a.lambdas[k];
-        const double w = (plane + offset * f_lambda) * a.cutoff;
+        const LambdaWindow &L = a.lam[k];
+        const double w = (plane + offset * L.f_w) * a.cutoff;
+        const double dw_dl = offset * L.g_w * a.cutoff;
+        double v[6] = {q0, s0, e0, 0.0, 0.0, 0.0};
+        if (a.interpolated) {
+            v[0] = (1 - L.f_q) * q0 + L.f_q * q1;
+            v[1] = (1 - L.f_s) * s0 + L.f_s * s1;
+            v[2] = (1 - L.f_e) * e0 + L.f_e * e1;
+            v[3] = L.g_q * (q1 - q0);
+            v[4] = L.g_s * (s1 - s0);
+            v[5] = L.g_e * (e1 - e0);
+        }
         const size_t o = (size_t)k * a.S + s;
         a.slots.posw[o] = make_float4(fx, fy, fz, (float)w);
+        a.slots.prm[o] = make_float4((float)v[0], (float)v[1], (float)v[2], (float)dw_dl);
         if (a.interpolated) {
-            double pq = (1 - f_lambda) * p0[0] + f_lambda * p1[0];
-            double ps = (1 - f_lambda) * p0[1] + f_lambda * p1[1];
-            double pe = (1 - f_lambda) * p0[2] + f_lambda * p1[2];
-            a.slots.prm[o] = make_float4((float)pq, (float)ps, (float)pe, (float)dw_dl);
-        } else {
-            a.slots.prm[o] = make_float4((float)p0[0], (float)p0[1], (float)p0[2], (float)dw_dl);
+            a.slots.dprm[o] = make_float4((float)v[3], (float)v[4], (float)v[5], 0.0f);
+        }
+        if (a.slots.posw64 != nullptr) {
+            a.slots.posw64[o] = make_double4(x0, x1, x2, w);
+            a.slots.prm64[o] = make_double4(v[0], v[1], v[2], dw_dl);
+            if (a.interpolated) {
+                a.slots.dprm64[o] = make_double4(v[3], v[4], v[5], 0.0);
+            }
+        }
+        for (int c = 0; c < 6; c++) {
+            if (k == 0) {
+                first[c] = v[c];
+            } else if (v[c] != first[c]) {
+                dep = true;
+            }
         }
     }
+    a.slots.lamdep[s] = dep ? 1 : 0;
 }
 
 // ---------------------------------------------------------------------------
@@ -128,14 +161,11 @@ static __global__ void k_check_prepare(
     const unsigned *__restrict__ perm, // [S] slot -> atom
     const double *__restrict__ nb_x,   // [N,3] coordinates at the last rebuild (nullptr: no neighbour list)
     const double *__restrict__ nb_box, // [9]
-    DevState *state,
-    const int set_cond = 0,                // 1: publish the rebuild decision to `cond`
-    const cudaGraphConditionalHandle cond = 0) {
+    DevState *state) {
     grid_dependency_wait();
     const int tid = blockIdx.x * blockDim.x + threadIdx.x;
     if (tid == 0) {
         state->next_item = 0;
-        state->bar_count = 0; // no k_rebuild of this state runs concurrently (stream order)
         if (nb_x != nullptr) {
             // Orthorhombic box whose every edge is at least twice cutoff+padding
             // (timemachine/cpp/src/nonbonded_all_pairs.cu:315-329); checked in
@@ -180,24 +210,6 @@ static __global__ void k_check_prepare(
             // the lambda-dependent tiles change with it (benign race: every writer stores the same)
             state->dep_dirty = 1;
             state->n_dep = 0;
-        }
-    }
-    if (set_cond) {
-        // The last block to finish sets the graph condition that gates the
-        // rebuild chain (keys, scan, scatter, bounds, tiles): a step that
-        // keeps its list skips those launches entirely. Every thread fences
-        // its own stores to state->rebuild before the block counts itself done.
-        __threadfence();
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            const unsigned prev = atomicAdd(&state->prep_done, 1u);
-            if (prev == gridDim.x - 1) {
-                __threadfence();
-                const int rebuild = *((volatile int *)&state->rebuild);
-                const int error = *((volatile int *)&state->error);
-                cudaGraphSetConditional(cond, (rebuild != 0 && error == 0) ? 1u : 0u);
-                state->prep_done = 0;
-            }
         }
     }
 }
@@ -873,101 +885,6 @@ static __global__ void __launch_bounds__(TB_WARPS * 32) k_build_tiles(TileArgs a
 static __global__ void k_clear_rebuild(DevState *state) { state->rebuild = 0; }
 
 // ---------------------------------------------------------------------------
-// The whole rebuild (sort keys, cell scan, scatter + restaging, block bounds,
-// tile build) as one cooperative launch with grid barriers between the
-// phases. A step that keeps its list pays one launch that returns at once
-// instead of five.
-// ---------------------------------------------------------------------------
-constexpr unsigned BARRIER_SPIN_LIMIT = 1u << 22; // x >= 64 ns sleeps: well above any phase
-
-// Grid-wide barrier for a cooperative launch (all blocks co-resident). The
-// wait is bounded: on timeout it records DEV_ERR_BARRIER_TIMEOUT and every
-// block leaves at its next barrier. Returns false once an error is recorded.
-__device__ __forceinline__ bool grid_barrier(DevState *st) {
-    __threadfence();
-    __syncthreads();
-    if (threadIdx.x == 0) {
-        const unsigned gen = *((volatile unsigned *)&st->bar_gen);
-        __threadfence();
-        if (atomicAdd(&st->bar_count, 1u) == gridDim.x - 1) {
-            atomicExch(&st->bar_count, 0u);
-            __threadfence();
-            atomicAdd(&st->bar_gen, 1u);
-        } else {
-            unsigned it = 0;
-            while (*((volatile unsigned *)&st->bar_gen) == gen) {
-                if (++it > BARRIER_SPIN_LIMIT) {
-                    atomicExch(&st->error, DEV_ERR_BARRIER_TIMEOUT);
-                    break;
-                }
-                __nanosleep(64);
-            }
-        }
-        __threadfence();
-    }
-    __syncthreads();
-    return *((volatile int *)&st->error) == 0;
-}
-
-struct RebuildArgs {
-    SortArgs sa;
-    PrepareArgs pa;
-    unsigned *perm;   // [S] slot -> atom
-    int *slot_of;     // [N] atom -> slot (nullptr: not needed)
-    double *nb_x;     // [N,3] coordinates of the rebuild
-    double *nb_box;   // [9]
-    TileArgs ta;      // ta.posw / ta.bb_ctr / ta.bb_ext are the block-bounds buffers too
-};
-
-static __global__ void __launch_bounds__(TB_WARPS * 32) k_rebuild(RebuildArgs r, DevState *state) {
-    if (!state->rebuild || state->error) {
-        return;
-    }
-    const int S = r.sa.S;
-    const int tid = blockIdx.x * blockDim.x + threadIdx.x;
-    const int nth = gridDim.x * blockDim.x;
-    if (r.sa.hilbert) {
-        for (int k = tid; k < S; k += nth) {
-            bin_key(r.sa, k);
-        }
-    }
-    if (!grid_barrier(state)) {
-        return;
-    }
-    if (blockIdx.x == 0) {
-        bin_scan_cta(r.sa, state);
-    }
-    if (!grid_barrier(state)) {
-        return;
-    }
-    if (tid < 9) {
-        r.nb_box[tid] = r.sa.box[tid];
-    }
-    for (int k = tid; k < S; k += nth) {
-        const int atom = set_atom(r.sa, k);
-        const int s = scatter_slot(r.sa, k, r.perm, r.slot_of, r.nb_x);
-        prepare_slot(r.pa, s, atom);
-    }
-    if (!grid_barrier(state)) {
-        return;
-    }
-    {
-        const int warp = tid >> 5;
-        const int n_warps = nth >> 5;
-        for (int rb = warp; rb < r.ta.RB; rb += n_warps) {
-            lj_first_warp(r.pa, S, r.sa.n_first, rb, r.perm, r.slot_of, r.ta.rows);
-            block_bounds_warp(S, rb, r.sa.box, r.ta.posw, const_cast<float4 *>(r.ta.bb_ctr), const_cast<float4 *>(r.ta.bb_ext));
-        }
-    }
-    if (!grid_barrier(state)) {
-        return;
-    }
-    for (int rb = blockIdx.x; rb < r.ta.n_row_blocks; rb += gridDim.x) {
-        build_tiles_cta(r.ta, rb, state);
-    }
-}
-
-// ---------------------------------------------------------------------------
 // Pair kernel.
 // ---------------------------------------------------------------------------
 struct Accum {
@@ -1002,8 +919,11 @@ struct PairArgs {
     int K;                      // lambda windows
     const float4 *posw;         // [K][S]
     const float4 *prm;          // [K][S]
-    const float4 *dprm;         // [S]
+    const float4 *dprm;         // [K][S]
     const unsigned char *lamdep; // [S]
+    const double4 *posw64;      // [K][S] FP64 pair arithmetic (else nullptr)
+    const double4 *prm64;       // [K][S]
+    const double4 *dprm64;      // [K][S]
     const double *box;
     double beta;
     double cutoff;
@@ -1022,6 +942,26 @@ struct PairArgs {
 };
 
 __device__ __forceinline__ void red_add(unsigned long long *p, unsigned long long v) { atomicAdd(p, v); }
+
+// The staged slot arrays the pair arithmetic of type Real reads: FP32 float4
+// or FP64 double4 copies of the same values.
+template <typename Real> struct Staged;
+template <> struct Staged<float> {
+    using V = float4;
+    static __device__ __forceinline__ const float4 *posw(const PairArgs &a) { return a.posw; }
+    static __device__ __forceinline__ const float4 *prm(const PairArgs &a) { return a.prm; }
+    static __device__ __forceinline__ const float4 *dprm(const PairArgs &a) { return a.dprm; }
+    static __device__ __forceinline__ float4 make(float x, float y, float z, float w) { return make_float4(x, y, z, w); }
+};
+template <> struct Staged<double> {
+    using V = double4;
+    static __device__ __forceinline__ const double4 *posw(const PairArgs &a) { return a.posw64; }
+    static __device__ __forceinline__ const double4 *prm(const PairArgs &a) { return a.prm64; }
+    static __device__ __forceinline__ const double4 *dprm(const PairArgs &a) { return a.dprm64; }
+    static __device__ __forceinline__ double4 make(double x, double y, double z, double w) {
+        return make_double4(x, y, z, w);
+    }
+};
 
 // The arithmetic of one in-range pair (row atom i, column atom j) from its
 // minimum-image deltas and 4D d2: adds the row's and the column's fixed-point
@@ -1098,23 +1038,23 @@ __device__ __forceinline__ void pair_terms(
         // The column's term llrint(-y) equals -llrint(y) (round-half-even is
         // odd) except where the conversion saturates (|y| >= 2^63) or y is NaN;
         // those lanes add the difference afterwards.
-        const float ex = static_cast<float>(FX_EXPONENT);
-        const float yx = fmul(fmul(prefactor, delta_x), ex);
-        const float yy = fmul(fmul(prefactor, delta_y), ex);
-        const float yz = fmul(fmul(prefactor, delta_z), ex);
-        const unsigned long long fx = static_cast<unsigned long long>(llrintf(yx));
-        const unsigned long long fy = static_cast<unsigned long long>(llrintf(yy));
-        const unsigned long long fz = static_cast<unsigned long long>(llrintf(yz));
+        const Real ex = static_cast<Real>(FX_EXPONENT);
+        const Real yx = fmul(fmul(prefactor, delta_x), ex);
+        const Real yy = fmul(fmul(prefactor, delta_y), ex);
+        const Real yz = fmul(fmul(prefactor, delta_z), ex);
+        const unsigned long long fx = fixed_round(yx);
+        const unsigned long long fy = fixed_round(yy);
+        const unsigned long long fz = fixed_round(yz);
         gi_x += fx;
         gi_y += fy;
         gi_z += fz;
         gj_x -= fx;
         gj_y -= fy;
         gj_z -= fz;
-        if (!(fabsf(yx) < 0x1p63f) || !(fabsf(yy) < 0x1p63f) || !(fabsf(yz) < 0x1p63f)) {
-            gj_x += static_cast<unsigned long long>(llrintf(-yx)) + fx;
-            gj_y += static_cast<unsigned long long>(llrintf(-yy)) + fy;
-            gj_z += static_cast<unsigned long long>(llrintf(-yz)) + fz;
+        if (!fixed_in_range(yx) || !fixed_in_range(yy) || !fixed_in_range(yz)) {
+            gj_x += fixed_round(-yx) + fx;
+            gj_y += fixed_round(-yy) + fy;
+            gj_z += fixed_round(-yz) + fz;
         }
     }
     if (DP) {
@@ -1270,16 +1210,17 @@ __device__ __forceinline__ void scaled_pair(
     const Real inv_box_y,
     const Real inv_box_z,
     const Real cutoff_squared) {
+    using St = Staged<Real>;
     const size_t wo = (size_t)window * a.S;
-    const float4 pwi = a.posw[wo + si];
-    const float4 pwj = a.posw[wo + sj];
-    const float4 pri = a.prm[wo + si];
-    const float4 prj = a.prm[wo + sj];
-    float4 dpi = make_float4(0.f, 0.f, 0.f, 0.f);
-    float4 dpj = dpi;
+    const typename St::V pwi = St::posw(a)[wo + si];
+    const typename St::V pwj = St::posw(a)[wo + sj];
+    const typename St::V pri = St::prm(a)[wo + si];
+    const typename St::V prj = St::prm(a)[wo + sj];
+    typename St::V dpi = St::make(0, 0, 0, 0);
+    typename St::V dpj = dpi;
     if (INTERP) {
-        dpi = a.dprm[si];
-        dpj = a.dprm[sj];
+        dpi = St::dprm(a)[wo + si];
+        dpj = St::dprm(a)[wo + sj];
     }
     const Real ci_x = pwi.x, ci_y = pwi.y, ci_z = pwi.z, ci_w = pwi.w;
     const Real cj_x = pwj.x, cj_y = pwj.y, cj_z = pwj.z, cj_w = pwj.w;
@@ -1366,204 +1307,11 @@ __device__ __forceinline__ void scaled_pair(
     }
 }
 
-// ---------------------------------------------------------------------------
-// Compacted tile sweep. Of a tile's 32x32 pair slots only about a third lie
-// within the cutoff; the rotating sweep issues the full pair arithmetic for a
-// round whenever any lane's slot is in range. Here a cheap pass first tests
-// every slot (the same 4D d2 as the pair arithmetic, so the same decisions)
-// and records each row's in-range columns as a bit mask; the in-range pairs
-// are then numbered row by row and evaluated 32 at a time, one per lane, so
-// the expensive arithmetic runs with (nearly) all lanes busy. Row
-// contributions are summed over each batch's contiguous runs of equal rows
-// (segmented warp scan) into shared memory; column contributions go to
-// shared memory with atomics. Fixed-point integer sums make the result
-// independent of this order.
-// ---------------------------------------------------------------------------
-struct TileSmem {
-    float4 rpos[TILE], rprm[TILE], rdp[TILE]; // row atoms: x, y, z, w / q, sig, eps, dw_dl / dp_dl
-    float4 cpos[TILE], cprm[TILE], cdp[TILE]; // column atoms
-    unsigned cslot[TILE];                     // column slots (S or more: empty)
-    unsigned long long racc[8][TILE];         // per row: x, y, z, q, sig, eps, du_dl, u
-    unsigned long long cacc[6][TILE];         // per column: x, y, z, q, sig, eps
-};
-
-// Bit position of the (k+1)-th set bit of m (k < popc(m)).
-__device__ __forceinline__ int nth_set_bit(unsigned m, int k) {
-    int pos = 0;
-    for (int w = 16; w > 0; w >>= 1) {
-        const int c = __popc(m & ((1u << w) - 1u));
-        if (k >= c) {
-            k -= c;
-            m >>= w;
-            pos += w;
-        }
-    }
-    return pos;
-}
-
-// Inclusive scan over lanes whose keys are equal (equal keys are contiguous);
-// take[s]: lane - 2^s has the same key.
-__device__ __forceinline__ unsigned long long seg_scan(unsigned long long v, const int lane, const bool (&take)[5]) {
-#pragma unroll
-    for (int s = 0; s < 5; s++) {
-        const unsigned long long up = __shfl_up_sync(FULL_MASK, v, 1 << s);
-        if (take[s]) {
-            v += up;
-        }
-    }
-    return v;
-}
-
-template <typename Real, bool U, bool DX, bool DL, bool DP, bool INTERP, bool ALCH>
-__device__ __forceinline__ void sweep_tile_compact(
-    TileSmem &sm,
-    const int lane,
-    const unsigned S,
-    const unsigned i,
-    const Real ci_x,
-    const Real ci_y,
-    const Real ci_z,
-    const Real ci_w,
-    const Real box_x,
-    const Real box_y,
-    const Real box_z,
-    const Real inv_box_x,
-    const Real inv_box_y,
-    const Real inv_box_z,
-    const Real cutoff_squared,
-    const Real beta) {
-    // pass 1: in-range mask of this lane's row against the 32 columns
-    unsigned mask = 0;
-#pragma unroll 4
-    for (int c = 0; c < TILE; c++) {
-        const float4 pc = sm.cpos[c];
-        const unsigned jc = sm.cslot[c];
-        Real delta_x = min_image(fsub(ci_x, pc.x), box_x, inv_box_x);
-        Real delta_y = min_image(fsub(ci_y, pc.y), box_y, inv_box_y);
-        Real delta_z = min_image(fsub(ci_z, pc.z), box_z, inv_box_z);
-        Real d2 = dist2(delta_x, delta_y, delta_z);
-        if (ALCH) {
-            d2 = add_w2(d2, fsub(ci_w, pc.w));
-        }
-        const bool valid = i < S && jc < S && i < jc;
-        mask |= (valid && d2 < cutoff_squared) ? (1u << c) : 0u;
-    }
-    // number the in-range pairs row by row
-    const int cnt = __popc(mask);
-    int incl = cnt;
-#pragma unroll
-    for (int o = 1; o < TILE; o <<= 1) {
-        const int n = __shfl_up_sync(FULL_MASK, incl, o);
-        if (lane >= o) {
-            incl += n;
-        }
-    }
-    const int excl = incl - cnt;
-    const int total = __shfl_sync(FULL_MASK, incl, TILE - 1);
-    // pass 2: 32 pairs at a time
-    for (int base = 0; base < total; base += TILE) {
-        const int g = base + lane;
-        const bool active = g < total;
-        int L = 0; // owner row: the last lane whose first pair number is <= g
-#pragma unroll
-        for (int step = 16; step > 0; step >>= 1) {
-            const int e = __shfl_sync(FULL_MASK, excl, L + step);
-            if (e <= g) {
-                L += step;
-            }
-        }
-        const int first = __shfl_sync(FULL_MASK, excl, L);
-        const unsigned mL = __shfl_sync(FULL_MASK, mask, L);
-        const int c = active ? nth_set_bit(mL, g - first) : 0;
-        unsigned long long gi_x = 0, gi_y = 0, gi_z = 0, g_qi = 0, g_sigi = 0, g_epsi = 0, du_dl = 0, energy = 0;
-        unsigned long long gj_x = 0, gj_y = 0, gj_z = 0, g_qj = 0, g_sigj = 0, g_epsj = 0;
-        if (active) {
-            const float4 pi = sm.rpos[L], ri = sm.rprm[L];
-            const float4 pj = sm.cpos[c], rj = sm.cprm[c];
-            float4 di = make_float4(0.f, 0.f, 0.f, 0.f), dj = di;
-            if (INTERP) {
-                di = sm.rdp[L];
-                dj = sm.cdp[c];
-            }
-            const Real delta_x = min_image(fsub((Real)pi.x, (Real)pj.x), box_x, inv_box_x);
-            const Real delta_y = min_image(fsub((Real)pi.y, (Real)pj.y), box_y, inv_box_y);
-            const Real delta_z = min_image(fsub((Real)pi.z, (Real)pj.z), box_z, inv_box_z);
-            Real d2 = dist2(delta_x, delta_y, delta_z);
-            Real delta_w = 0;
-            if (ALCH) {
-                delta_w = fsub((Real)pi.w, (Real)pj.w);
-                d2 = add_w2(d2, delta_w);
-            }
-            pair_terms<Real, U, DX, DL, DP, INTERP, ALCH>(
-                delta_x, delta_y, delta_z, delta_w, d2, ri.x, ri.y, ri.z, ri.w, di.x, di.y, di.z, rj.x, rj.y, rj.z,
-                rj.w, dj.x, dj.y, dj.z, beta, gi_x, gi_y, gi_z, g_qi, g_sigi, g_epsi, du_dl, energy, gj_x, gj_y, gj_z,
-                g_qj, g_sigj, g_epsj);
-        }
-        // rows: sums over runs of equal rows; the run's last lane stores
-        const int owner = active ? L : -1;
-        bool take[5];
-#pragma unroll
-        for (int s2 = 0; s2 < 5; s2++) {
-            const int o = __shfl_up_sync(FULL_MASK, owner, 1 << s2);
-            take[s2] = lane >= (1 << s2) && o == owner;
-        }
-        const int next = __shfl_down_sync(FULL_MASK, owner, 1);
-        const bool last = active && (lane == TILE - 1 || next != owner);
-        if (DX) {
-            gi_x = seg_scan(gi_x, lane, take);
-            gi_y = seg_scan(gi_y, lane, take);
-            gi_z = seg_scan(gi_z, lane, take);
-            if (last) {
-                sm.racc[0][L] += gi_x;
-                sm.racc[1][L] += gi_y;
-                sm.racc[2][L] += gi_z;
-            }
-        }
-        if (DP) {
-            g_qi = seg_scan(g_qi, lane, take);
-            g_sigi = seg_scan(g_sigi, lane, take);
-            g_epsi = seg_scan(g_epsi, lane, take);
-            if (last) {
-                sm.racc[3][L] += g_qi;
-                sm.racc[4][L] += g_sigi;
-                sm.racc[5][L] += g_epsi;
-            }
-        }
-        if (DL && ALCH) {
-            du_dl = seg_scan(du_dl, lane, take);
-            if (last) {
-                sm.racc[6][L] += du_dl;
-            }
-        }
-        if (U) {
-            energy = seg_scan(energy, lane, take);
-            if (last) {
-                sm.racc[7][L] += energy;
-            }
-        }
-        // columns: shared-memory atomics (a column can recur within a batch)
-        if (active) {
-            if (DX) {
-                atomicAdd(&sm.cacc[0][c], gj_x);
-                atomicAdd(&sm.cacc[1][c], gj_y);
-                atomicAdd(&sm.cacc[2][c], gj_z);
-            }
-            if (DP) {
-                atomicAdd(&sm.cacc[3][c], g_qj);
-                atomicAdd(&sm.cacc[4][c], g_sigj);
-                atomicAdd(&sm.cacc[5][c], g_epsj);
-            }
-        }
-        __syncwarp();
-    }
-}
-
 // One tile of a row group's rows (lane: row slot i) against the 32 column slots
 // j, for one window: load, sweep, column atomics. Row accumulators are
 // returned to the caller.
-template <typename Real, bool U, bool DX, bool DL, bool DP, bool INTERP, bool COMPACT = false, int RG = TILE>
+template <typename Real, bool U, bool DX, bool DL, bool DP, bool INTERP, int RG = TILE>
 __device__ __forceinline__ void tile_pass(
-    TileSmem *sm, // COMPACT: this warp's shared staging (accumulators zero on entry and on return)
     const PairArgs &a,
     const int lane,
     const unsigned S,
@@ -1587,98 +1335,31 @@ __device__ __forceinline__ void tile_pass(
     unsigned long long &g_epsi,
     unsigned long long &du_dl,
     unsigned long long &energy) {
+    using St = Staged<Real>;
+    using V = typename St::V;
     const size_t wo = (size_t)window * a.S;
     const bool row_ok = i < (unsigned)a.row_end;
     const bool col_ok = j < S;
     const unsigned i_eff = row_ok ? i : 0xffffffffu; // invalid rows pair with nothing
     // padding rows and columns: NaN coordinates (no pair passes the cutoff test), w = 0
-    const float nan = __int_as_float(0x7fffffff);
-    const float4 pwi = row_ok ? a.posw[wo + i] : make_float4(nan, nan, nan, 0.f);
-    const float4 pri = row_ok ? a.prm[wo + i] : make_float4(0.f, 0.f, 0.f, 0.f);
-    const float4 pwj = col_ok ? a.posw[wo + j] : make_float4(nan, nan, nan, 0.f);
-    const float4 prj = col_ok ? a.prm[wo + j] : make_float4(0.f, 0.f, 0.f, 0.f);
-    float4 dpi = make_float4(0.f, 0.f, 0.f, 0.f);
-    float4 dpj = dpi;
+    const Real nan = static_cast<Real>(__int_as_float(0x7fffffff));
+    const V pwi = row_ok ? St::posw(a)[wo + i] : St::make(nan, nan, nan, 0);
+    const V pri = row_ok ? St::prm(a)[wo + i] : St::make(0, 0, 0, 0);
+    const V pwj = col_ok ? St::posw(a)[wo + j] : St::make(nan, nan, nan, 0);
+    const V prj = col_ok ? St::prm(a)[wo + j] : St::make(0, 0, 0, 0);
+    V dpi = St::make(0, 0, 0, 0);
+    V dpj = dpi;
     if (INTERP) {
         if (row_ok) {
-            dpi = a.dprm[i];
+            dpi = St::dprm(a)[wo + i];
         }
         if (col_ok) {
-            dpj = a.dprm[j];
+            dpj = St::dprm(a)[wo + j];
         }
     }
-    const bool row_alch = pwi.w != 0.f || (INTERP && (dpi.x != 0.f || dpi.y != 0.f || dpi.z != 0.f));
-    const bool col_alch = pwj.w != 0.f || (INTERP && (dpj.x != 0.f || dpj.y != 0.f || dpj.z != 0.f));
+    const bool row_alch = pwi.w != 0 || (INTERP && (dpi.x != 0 || dpi.y != 0 || dpi.z != 0));
+    const bool col_alch = pwj.w != 0 || (INTERP && (dpj.x != 0 || dpj.y != 0 || dpj.z != 0));
     const bool alch = __any_sync(FULL_MASK, row_alch || col_alch);
-    if (COMPACT && RG == TILE) {
-        sm->rpos[lane] = pwi;
-        sm->rprm[lane] = pri;
-        sm->cpos[lane] = pwj;
-        sm->cprm[lane] = prj;
-        if (INTERP) {
-            sm->rdp[lane] = dpi;
-            sm->cdp[lane] = dpj;
-        }
-        sm->cslot[lane] = col_ok ? j : 0xffffffffu;
-        __syncwarp();
-        if (alch) {
-            sweep_tile_compact<Real, U, DX, DL, DP, INTERP, true>(
-                *sm, lane, S, i_eff, pwi.x, pwi.y, pwi.z, pwi.w, box_x, box_y, box_z, inv_box_x, inv_box_y, inv_box_z,
-                cutoff_squared, beta);
-        } else {
-            sweep_tile_compact<Real, U, DX, DL, DP, INTERP, false>(
-                *sm, lane, S, i_eff, pwi.x, pwi.y, pwi.z, pwi.w, box_x, box_y, box_z, inv_box_x, inv_box_y, inv_box_z,
-                cutoff_squared, beta);
-        }
-        __syncwarp();
-        // this tile's row sums into the caller's row accumulators; column sums out
-        if (DX) {
-            gi_x += sm->racc[0][lane];
-            gi_y += sm->racc[1][lane];
-            gi_z += sm->racc[2][lane];
-            sm->racc[0][lane] = 0;
-            sm->racc[1][lane] = 0;
-            sm->racc[2][lane] = 0;
-        }
-        if (DP) {
-            g_qi += sm->racc[3][lane];
-            g_sigi += sm->racc[4][lane];
-            g_epsi += sm->racc[5][lane];
-            sm->racc[3][lane] = 0;
-            sm->racc[4][lane] = 0;
-            sm->racc[5][lane] = 0;
-        }
-        if (DL) {
-            du_dl += sm->racc[6][lane];
-            sm->racc[6][lane] = 0;
-        }
-        if (U) {
-            energy += sm->racc[7][lane];
-            sm->racc[7][lane] = 0;
-        }
-        if (DX) {
-            if (col_ok) {
-                red_add(acc_out.x + j, sm->cacc[0][lane]);
-                red_add(acc_out.y + j, sm->cacc[1][lane]);
-                red_add(acc_out.z + j, sm->cacc[2][lane]);
-            }
-            sm->cacc[0][lane] = 0;
-            sm->cacc[1][lane] = 0;
-            sm->cacc[2][lane] = 0;
-        }
-        if (DP) {
-            if (col_ok) {
-                red_add(acc_out.q + j, sm->cacc[3][lane]);
-                red_add(acc_out.sig + j, sm->cacc[4][lane]);
-                red_add(acc_out.eps + j, sm->cacc[5][lane]);
-            }
-            sm->cacc[3][lane] = 0;
-            sm->cacc[4][lane] = 0;
-            sm->cacc[5][lane] = 0;
-        }
-        __syncwarp();
-        return;
-    }
     unsigned long long gj_x = 0, gj_y = 0, gj_z = 0, g_qj = 0, g_sigj = 0, g_epsj = 0;
     // Only a tile holding atoms of the row group itself (the diagonal block)
     // needs the per-pair i < j test. The diagonal block is the first
@@ -1840,28 +1521,19 @@ static __global__ void k_dep_tiles(DepArgs a, DevState *state) {
 // MULTI (K > 1 windows): the tile items skip lambda-dependent tiles and add
 // into the shared accumulator block; each (tile, window) unit adds into the
 // window's block; a lambda-dependent scaled pair is evaluated for every window.
-template <typename Real, bool U, bool DX, bool DL, bool DP, bool INTERP, bool MULTI, bool COMPACT = false, int RG = TILE>
+template <typename Real, bool U, bool DX, bool DL, bool DP, bool INTERP, bool MULTI, int RG = TILE>
 // Occupancy, measured on B200: all four outputs at 6 CTAs/SM (80 registers,
-// no spills; 12-window call -3.5 % against 5), forces only at 8 (64).
-__global__ void __launch_bounds__(128, (U && DX && DL && DP && !INTERP && !COMPACT) ? 6 : ((DX && !U && !DL && !DP) ? 8 : 1)) k_pair(PairArgs a) {
+// no spills; 12-window call -3.5 % against 5), forces only at 8 (64). FP64
+// variants are left to the compiler.
+__global__ void __launch_bounds__(
+    128,
+    sizeof(Real) != 4 ? 1 : ((U && DX && DL && DP && !INTERP) ? 6 : ((DX && !U && !DL && !DP) ? 8 : 1)))
+    k_pair(PairArgs a) {
     grid_dependency_wait();
     if (a.state->error) {
         return;
     }
     const int lane = threadIdx.x & 31;
-    // COMPACT: one TileSmem per warp in dynamic shared memory (4 * sizeof(TileSmem) bytes)
-    extern __shared__ __align__(16) unsigned char k_pair_smem[];
-    TileSmem *sm = nullptr;
-    if (COMPACT) {
-        sm = reinterpret_cast<TileSmem *>(k_pair_smem) + (threadIdx.x >> 5);
-        for (int f = 0; f < 8; f++) {
-            sm->racc[f][lane] = 0;
-        }
-        for (int f = 0; f < 6; f++) {
-            sm->cacc[f][lane] = 0;
-        }
-        __syncwarp();
-    }
     const Real box_x = a.box[0 * 3 + 0];
     const Real box_y = a.box[1 * 3 + 1];
     const Real box_z = a.box[2 * 3 + 2];
@@ -1918,8 +1590,8 @@ __global__ void __launch_bounds__(128, (U && DX && DL && DP && !INTERP && !COMPA
             const unsigned j = a.tile_cols[(long long)dt.y * TILE + lane];
             const Accum wk = acc_block(a.acc, a.acc_block, 1 + k);
             unsigned long long wx = 0, wy = 0, wz = 0, wq = 0, ws = 0, we = 0, wl = 0, wu = 0;
-            tile_pass<Real, U, DX, DL, DP, INTERP, COMPACT, RG>(
-                sm, a, lane, S, i, j, k, wk, box_x, box_y, box_z, inv_box_x, inv_box_y, inv_box_z, cutoff_squared, beta,
+            tile_pass<Real, U, DX, DL, DP, INTERP, RG>(
+                a, lane, S, i, j, k, wk, box_x, box_y, box_z, inv_box_x, inv_box_y, inv_box_z, cutoff_squared, beta,
                 wx, wy, wz, wq, ws, we, wl, wu);
             flush_row_rg<RG, U, DX, DL, DP>(wk, i, i < (unsigned)a.row_end, wx, wy, wz, wq, ws, we, wl, wu);
             continue;
@@ -1934,8 +1606,8 @@ __global__ void __launch_bounds__(128, (U && DX && DL && DP && !INTERP && !COMPA
             if (MULTI && __any_sync(FULL_MASK, row_dep || (j < S && a.lamdep[j]))) {
                 continue; // evaluated per window by the (tile, window) units
             }
-            tile_pass<Real, U, DX, DL, DP, INTERP, COMPACT, RG>(
-                sm, a, lane, S, i, j, 0, a.acc, box_x, box_y, box_z, inv_box_x, inv_box_y, inv_box_z, cutoff_squared,
+            tile_pass<Real, U, DX, DL, DP, INTERP, RG>(
+                a, lane, S, i, j, 0, a.acc, box_x, box_y, box_z, inv_box_x, inv_box_y, inv_box_z, cutoff_squared,
                 beta, gi_x, gi_y, gi_z, g_qi, g_sigi, g_epsi, du_dl, energy);
         }
         flush_row_rg<RG, U, DX, DL, DP>(
@@ -1955,7 +1627,7 @@ struct FinalizeArgs {
     int N;
     int S;
     int K;
-    double lambdas[MAX_WINDOWS];
+    double f_dp[MAX_WINDOWS][3]; // interpolated: f(lambda_k) of the charge, sigma and epsilon transforms
     const int *set_atoms; // [S] atoms of the evaluated set in ascending order, nullptr: 0..S-1
     const int *slot_of;   // [N] atom -> slot, nullptr: identity
     int take;             // 1: zero each accumulator after reading it; 0: the caller zeroes them
@@ -2031,7 +1703,7 @@ static __global__ void k_finalize(FinalizeArgs a) {
                 unsigned long long *out = a.du_dp + a.stride_p * k;
                 for (int d = 0; d < 3; d++) {
                     if (a.interpolated) {
-                        const double f = a.lambdas[k];
+                        const double f = a.f_dp[k][d];
                         unsigned long long lo = interp_part(1 - f, v0[d], ex[d]) + interp_part(1 - f, v1[d], ex[d]);
                         unsigned long long hi = interp_part(f, v0[d], ex[d]) + interp_part(f, v1[d], ex[d]);
                         atomicAdd(out + 3 * (size_t)atom + d, lo);

@@ -65,6 +65,16 @@ namespace tmb {
 // stream serialization).
 __device__ __forceinline__ void grid_dependency_wait() { asm volatile("griddepcontrol.wait;" ::: "memory"); }
 
+// explicit-rounding helpers (FP32 and FP64)
+__device__ __forceinline__ float fmul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ float fadd(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ float fsub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ float ffma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double fmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ double fadd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ double fsub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ double ffma(double a, double b, double c) { return __fma_rn(a, b, c); }
+
 // Fixed-point exponents of the accumulators.
 constexpr unsigned long long FX_EXPONENT = 0x1000000000ULL;     // 2^36: du_dx, u, du_dl, du_dq
 constexpr unsigned long long FX_EXPONENT_SIG = 0x2000000000ULL; // 2^37: du_dsig
@@ -74,34 +84,37 @@ __device__ __forceinline__ unsigned long long to_fixed(float v, unsigned long lo
     return static_cast<unsigned long long>(llrintf(__fmul_rn(v, static_cast<float>(exponent))));
 }
 __device__ __forceinline__ unsigned long long to_fixed(double v, unsigned long long exponent) {
-    return static_cast<unsigned long long>(llrint(v * exponent));
+    return static_cast<unsigned long long>(llrint(__dmul_rn(v, static_cast<double>(exponent))));
 }
+
+// Round-half-even to int64 of an already scaled value (llrintf / llrint), and
+// the magnitude from which that conversion saturates.
+__device__ __forceinline__ unsigned long long fixed_round(float y) {
+    return static_cast<unsigned long long>(llrintf(y));
+}
+__device__ __forceinline__ unsigned long long fixed_round(double y) {
+    return static_cast<unsigned long long>(llrint(y));
+}
+__device__ __forceinline__ bool fixed_in_range(float y) { return fabsf(y) < 0x1p63f; }
+__device__ __forceinline__ bool fixed_in_range(double y) { return fabs(y) < 0x1p63; }
 
 // Fixed-point encodings of a pair term v and of its negation -v, for the two
 // atoms of the pair. llrint is odd under round-half-even, so the second is
 // -first (one conversion instead of two) -- except where the conversion
 // saturates (|v * 2^e| >= 2^63) or v is NaN, where the negated value is
 // converted on its own to keep the reference's exact result.
+template <typename Real>
 __device__ __forceinline__ void to_fixed_pair(
-    float v, unsigned long long exponent, unsigned long long &pos, unsigned long long &neg) {
-    const float y = __fmul_rn(v, static_cast<float>(exponent));
-    pos = static_cast<unsigned long long>(llrintf(y));
-    if (fabsf(y) < 0x1p63f) { // strictly inside the int64 range
+    Real v, unsigned long long exponent, unsigned long long &pos, unsigned long long &neg) {
+    const Real y = fmul(v, static_cast<Real>(exponent));
+    pos = fixed_round(y);
+    if (fixed_in_range(y)) { // strictly inside the int64 range
         neg = 0ULL - pos;
     } else {
-        neg = static_cast<unsigned long long>(llrintf(-y));
+        neg = fixed_round(-y);
     }
 }
 
-// explicit-rounding FP32 helpers
-__device__ __forceinline__ float fmul(float a, float b) { return __fmul_rn(a, b); }
-__device__ __forceinline__ float fadd(float a, float b) { return __fadd_rn(a, b); }
-__device__ __forceinline__ float fsub(float a, float b) { return __fsub_rn(a, b); }
-__device__ __forceinline__ float ffma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
-__device__ __forceinline__ double fmul(double a, double b) { return __dmul_rn(a, b); }
-__device__ __forceinline__ double fadd(double a, double b) { return __dadd_rn(a, b); }
-__device__ __forceinline__ double fsub(double a, double b) { return __dsub_rn(a, b); }
-__device__ __forceinline__ double ffma(double a, double b, double c) { return __fma_rn(a, b, c); }
 
 // a*b + c*d with both products rounded before the sum.
 template <typename Real> __device__ __forceinline__ Real sum_of_products_rn(Real a, Real b, Real c, Real d) {

@@ -11,8 +11,9 @@
 //              one row atom and one column atom (the complement); slots hold
 //              the spatially sorted rows, then the sorted columns.
 #include "engine.hpp"
+#include "lambda_transform.hpp"
 #include "nb_adjoint.cuh"
-#include "nb_kernels.cuh"
+#include "pair_kernels.hpp"
 
 #include <algorithm>
 #include <cmath>
@@ -27,48 +28,9 @@ namespace tmb {
 
 enum class Kind { AllPairs, PairList, Nonbonded, Group };
 
-typedef void (*pair_kernel_t)(PairArgs);
-
-template <int I> struct PairKernelTable {
-    static constexpr bool U = (I >> 3) & 1;
-    static constexpr bool DX = (I >> 2) & 1;
-    static constexpr bool DL = (I >> 1) & 1;
-    static constexpr bool DP = (I >> 0) & 1;
-};
-
-// kernel index: bit3 U, bit2 DU_DX, bit1 DU_DL, bit0 DU_DP (+16 when interpolated),
-// the same flag order as timemachine/cpp/src/nonbonded_all_pairs.cu:374-379.
-template <int I, bool INTERP, bool MULTI, bool COMPACT, int RG> constexpr pair_kernel_t pair_kernel() {
-    return &k_pair<float, PairKernelTable<I>::U, PairKernelTable<I>::DX, PairKernelTable<I>::DL, PairKernelTable<I>::DP,
-                   INTERP, MULTI, COMPACT, RG>;
-}
-// schedules: 0 rotating sweep, 32-slot row groups; 1 compacted sweep, 32-slot
-// row groups; 2 rotating, 16-slot row groups; 3 rotating, 8-slot row groups
-constexpr int N_SCHED = 4;
-template <int... Is> struct KernelList {
-    // [schedule][kidx]; single: one lambda window; multi: K > 1 windows sharing
-    // lambda-independent tiles
-    template <bool INTERP> static void fill_interp(pair_kernel_t (*single)[16], pair_kernel_t (*multi)[16]) {
-        ((single[0][Is] = pair_kernel<Is, INTERP, false, false, 32>()), ...);
-        ((multi[0][Is] = pair_kernel<Is, INTERP, true, false, 32>()), ...);
-        ((single[1][Is] = pair_kernel<Is, INTERP, false, true, 32>()), ...);
-        ((multi[1][Is] = pair_kernel<Is, INTERP, true, true, 32>()), ...);
-        ((single[2][Is] = pair_kernel<Is, INTERP, false, false, 16>()), ...);
-        ((multi[2][Is] = pair_kernel<Is, INTERP, true, false, 16>()), ...);
-        ((single[3][Is] = pair_kernel<Is, INTERP, false, false, 8>()), ...);
-        ((multi[3][Is] = pair_kernel<Is, INTERP, true, false, 8>()), ...);
-    }
-    static void fill(pair_kernel_t (*single)[16], pair_kernel_t (*multi)[16], bool interp) {
-        if (interp) {
-            fill_interp<true>(single, multi);
-        } else {
-            fill_interp<false>(single, multi);
-        }
-    }
-};
-// dynamic shared memory of the compacted pair kernel (one TileSmem per warp)
-constexpr size_t COMPACT_SMEM = 4 * sizeof(TileSmem);
-using AllKernels = KernelList<0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 14, 15>;
+// Pair-kernel tables: [0] 32-row, [1] 16-row, [2] 8-row tiles (FP32); FP64
+// potentials use 16-row tiles only.
+inline int row_table(int rows) { return rows == 32 ? 0 : (rows == 16 ? 1 : 2); }
 
 class NonbondedPotential : public PotentialBase {
   public:
@@ -85,8 +47,10 @@ class NonbondedPotential : public PotentialBase {
         const double *scales,
         int M,
         bool negated,
-        bool interpolated)
-        : kind_(kind), N_(N), beta_(beta), cutoff_(cutoff), interp_(interpolated), negated_(negated), M_(M),
+        bool interpolated,
+        bool fp64 = false)
+        : kind_(kind), N_(N), beta_(beta), cutoff_(cutoff), interp_(interpolated), negated_(negated), fp64_(fp64),
+          M_(M),
           h_plane_(plane, plane + N), h_offset_(offset, offset + N),
           h_atom_idxs_(atom_idxs ? std::vector<int>(atom_idxs, atom_idxs + K) : std::vector<int>()),
           h_pairs_(pair_idxs ? std::vector<int>(pair_idxs, pair_idxs + 2 * (size_t)M) : std::vector<int>()),
@@ -190,6 +154,13 @@ class NonbondedPotential : public PotentialBase {
         if (interp_) {
             dprm_.alloc(S_);
         }
+        if (fp64_) {
+            posw64_.alloc(S_);
+            prm64_.alloc(S_);
+            if (interp_) {
+                dprm64_.alloc(S_);
+            }
+        }
         split_pair_dp_ = interp_ && kind == Kind::Nonbonded;
         acc_.alloc(acc_block_elems());
         acc_.zero();
@@ -213,17 +184,25 @@ class NonbondedPotential : public PotentialBase {
             bb_ext_.alloc(RB_);
             alloc_list(); // row groups of rows_ slots
         }
-        if (has_nblist_) {
-            // created here, not during a capture (stream creation is not
-            // allowed inside a global-mode capture)
-            CK(cudaStreamCreateWithFlags(&body_stream_, cudaStreamNonBlocking));
-            rebuild_grid();
-        }
         state_.alloc(1);
         DevState st{};
         st.rebuild = has_nblist_ ? 1 : 0;
         CK(cudaMemcpy(state_.p, &st, sizeof(st), cudaMemcpyHostToDevice));
-        AllKernels::fill(kernels_, kernels_multi_, interp_);
+        if (fp64_) {
+            if (interp_) {
+                pair_kernels_f64_r16_interp(kernels_[1]);
+            } else {
+                pair_kernels_f64_r16(kernels_[1]);
+            }
+        } else if (interp_) {
+            pair_kernels_f32_r32_interp(kernels_[0]);
+            pair_kernels_f32_r16_interp(kernels_[1]);
+            pair_kernels_f32_r8_interp(kernels_[2]);
+        } else {
+            pair_kernels_f32_r32(kernels_[0]);
+            pair_kernels_f32_r16(kernels_[1]);
+            pair_kernels_f32_r8(kernels_[2]);
+        }
         CK(cudaDeviceSynchronize());
     }
 
@@ -231,9 +210,6 @@ class NonbondedPotential : public PotentialBase {
         if (timing_) {
             cudaEventDestroy(ev_pair_[0]);
             cudaEventDestroy(ev_pair_[1]);
-        }
-        if (body_stream_) {
-            cudaStreamDestroy(body_stream_);
         }
     }
 
@@ -291,8 +267,8 @@ class NonbondedPotential : public PotentialBase {
         if (rows != 32 && rows != 16 && rows != 8) {
             throw Error(TMNB_ERR_INVALID_ARGUMENT, "rows per tile must be 32, 16 or 8");
         }
-        if (rows != 32) {
-            compact_ = false; // the compacted sweep runs on 32-row tiles only
+        if (fp64_ && rows != 16) {
+            throw Error(TMNB_ERR_UNSUPPORTED, "FP64 potentials use tiles of 16 rows");
         }
         if (!has_nblist_ || rows == rows_) {
             rows_ = rows;
@@ -332,14 +308,13 @@ class NonbondedPotential : public PotentialBase {
             h_scales_.empty() ? nullptr : h_scales_.data(),
             M_,
             negated_,
-            interp_);
+            interp_,
+            fp64_);
         c->padding_ = padding_;
         c->hilbert_ = hilbert_;
         c->set_chunk(chunk_);
-        c->compact_ = compact_;
-        c->fused_rebuild_ = fused_rebuild_;
         c->set_row_group(rows_);
-        c->conditional_rebuild_ = conditional_rebuild_;
+        c->xf_ = xf_;
         return c;
     }
 
@@ -363,16 +338,32 @@ class NonbondedPotential : public PotentialBase {
         padding_ = p;
     }
     void disable_hilbert() { hilbert_ = false; }
-    // the compacted sweep runs on 32-row tiles only
-    void set_compact(bool on) {
-        if (on) {
-            set_row_group(32);
+
+    // The four lambda schedules (timemachine/cpp/src/wrap_kernels.cpp:843-893);
+    // nullptr keeps the identity "lambda". Parse errors throw.
+    void set_transforms(const char *q, const char *sig, const char *eps, const char *w) {
+        LambdaTransforms t;
+        try {
+            t.charge = LambdaExpr(q ? q : "lambda");
+            t.sigma = LambdaExpr(sig ? sig : "lambda");
+            t.epsilon = LambdaExpr(eps ? eps : "lambda");
+            t.w = LambdaExpr(w ? w : "lambda");
+        } catch (const std::invalid_argument &e) {
+            throw Error(TMNB_ERR_INVALID_ARGUMENT, e.what());
         }
-        compact_ = on;
+        // (non-interpolated potentials, like the reference's, read only the w schedule)
+        xf_ = t;
     }
-    void set_rebuild_mode(bool fused, bool conditional) {
-        fused_rebuild_ = fused;
-        conditional_rebuild_ = conditional;
+    const LambdaTransforms &transforms() const { return xf_; }
+
+    // f and df/dlambda of the four schedules at one lambda
+    LambdaWindow lambda_window(double lambda) const {
+        LambdaWindow L;
+        xf_.charge.eval(lambda, L.f_q, L.g_q);
+        xf_.sigma.eval(lambda, L.f_s, L.g_s);
+        xf_.epsilon.eval(lambda, L.f_e, L.g_e);
+        xf_.w.eval(lambda, L.f_w, L.g_w);
+        return L;
     }
 
     int row_end() const { return kind_ == Kind::Group ? NR_ : S_; }
@@ -386,6 +377,16 @@ class NonbondedPotential : public PotentialBase {
         if (posw_.n < (size_t)K * S_) {
             posw_.alloc((size_t)K * S_);
             prm_.alloc((size_t)K * S_);
+            if (interp_) {
+                dprm_.alloc((size_t)K * S_);
+            }
+            if (fp64_) {
+                posw64_.alloc((size_t)K * S_);
+                prm64_.alloc((size_t)K * S_);
+                if (interp_) {
+                    dprm64_.alloc((size_t)K * S_);
+                }
+            }
         }
         const size_t need = acc_block_elems() * (K > 1 ? 1 + K : 1);
         if (acc_.n < need) {
@@ -460,7 +461,7 @@ class NonbondedPotential : public PotentialBase {
         pa.box = d_box;
         pa.K = K;
         for (int k = 0; k < MAX_WINDOWS; k++) {
-            pa.lambdas[k] = k < K ? lambdas[k] : 0.0;
+            pa.lam[k] = lambda_window(k < K ? lambdas[k] : 0.0);
         }
         pa.cutoff = cutoff_;
         pa.padding = padding_;
@@ -471,60 +472,18 @@ class NonbondedPotential : public PotentialBase {
         pa.slots.prm = prm_.p;
         pa.slots.dprm = dprm_.p;
         pa.slots.lamdep = lamdep_.p;
+        pa.slots.posw64 = posw64_.p;
+        pa.slots.prm64 = prm64_.p;
+        pa.slots.dprm64 = dprm64_.p;
 
         const int tpb = 256;
         const int sgrid = std::max(1, std::min((S_ + tpb - 1) / tpb, 8 * num_sms()));
-        // Inside a stream capture the rebuild chain goes into the body of a
-        // conditional graph node that k_check_prepare switches on only when the
-        // list must be rebuilt (the chain's kernels also test the flag
-        // themselves, so both forms compute the same list).
-        cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
-        cudaGraph_t cap_graph = nullptr;
-        if (has_nblist_ && conditional_rebuild_ && body_stream_) {
-            CK(cudaStreamGetCaptureInfo(stream, &cap, nullptr, &cap_graph, nullptr, nullptr));
-        }
-        const bool conditional = cap == cudaStreamCaptureStatusActive;
-        cudaGraphConditionalHandle cond = 0;
-        if (conditional) {
-            CK(cudaGraphConditionalHandleCreate(&cond, cap_graph, 1, cudaGraphCondAssignDefault));
-        }
         launch_dependent(
             k_check_prepare, dim3(sgrid), dim3(tpb), 0, stream, pa, (const unsigned *)perm_.p,
-            (const double *)(has_nblist_ ? nb_x_.p : nullptr), (const double *)nb_box_.p, state_.p, conditional ? 1 : 0,
-            cond);
+            (const double *)(has_nblist_ ? nb_x_.p : nullptr), (const double *)nb_box_.p, state_.p);
         CK(cudaPeekAtLastError());
-
         if (has_nblist_) {
-            cudaStream_t chain = stream;
-            if (conditional) {
-                const cudaGraphNode_t *deps = nullptr;
-                size_t n_deps = 0;
-                CK(cudaStreamGetCaptureInfo(stream, &cap, nullptr, &cap_graph, &deps, &n_deps));
-                cudaGraphNodeParams cp = {};
-                cp.type = cudaGraphNodeTypeConditional;
-                cp.conditional.handle = cond;
-                cp.conditional.type = cudaGraphCondTypeIf;
-                cp.conditional.size = 1;
-                cudaGraphNode_t node;
-                CK(cudaGraphAddNode(&node, cap_graph, deps, n_deps, &cp));
-                CK(cudaStreamUpdateCaptureDependencies(stream, &node, 1, cudaStreamSetCaptureDependencies));
-                chain = body_stream_;
-                CK(cudaStreamBeginCaptureToGraph(
-                    chain, cp.conditional.phGraph_out[0], nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed));
-            }
-            try {
-                record_rebuild_chain(d_x, d_box, pa, sgrid, tpb, chain, K);
-            } catch (...) {
-                if (conditional) {
-                    cudaGraph_t body;
-                    cudaStreamEndCapture(chain, &body);
-                }
-                throw;
-            }
-            if (conditional) {
-                cudaGraph_t body;
-                CK(cudaStreamEndCapture(chain, &body));
-            }
+            record_rebuild_chain(d_x, d_box, pa, sgrid, tpb, stream, K);
         }
 
         const int kidx = (d_du_dp ? 1 : 0) | (d_du_dl ? 2 : 0) | (d_du_dx ? 4 : 0) | (d_u ? 8 : 0);
@@ -550,6 +509,9 @@ class NonbondedPotential : public PotentialBase {
             a.posw = posw_.p;
             a.prm = prm_.p;
             a.dprm = dprm_.p;
+            a.posw64 = posw64_.p;
+            a.prm64 = prm64_.p;
+            a.dprm64 = dprm64_.p;
             a.box = d_box;
             a.beta = beta_;
             a.cutoff = cutoff_;
@@ -563,9 +525,9 @@ class NonbondedPotential : public PotentialBase {
             a.acc = accum();
             a.dep_tiles = dep_tiles_.p;
             a.state = state_.p;
-            const int ci = compact_ ? 1 : (rows_ == 16 ? 2 : (rows_ == 8 ? 3 : 0));
-            pair_kernel_t k = K > 1 ? kernels_multi_[ci][kidx] : kernels_[ci][kidx];
-            const size_t smem = compact_ ? COMPACT_SMEM : 0;
+            const PairKernels &table = kernels_[row_table(rows_)];
+            pair_kernel_t k = K > 1 ? table.multi[kidx] : table.single[kidx];
+            const size_t smem = 0;
             if (timing_) {
                 CK(cudaEventRecord(ev_pair_[0], stream));
             }
@@ -586,7 +548,9 @@ class NonbondedPotential : public PotentialBase {
             fa.acc_block = acc_block_elems();
             fa.K = K;
             for (int w = 0; w < MAX_WINDOWS; w++) {
-                fa.lambdas[w] = pa.lambdas[w];
+                fa.f_dp[w][0] = pa.lam[w].f_q;
+                fa.f_dp[w][1] = pa.lam[w].f_s;
+                fa.f_dp[w][2] = pa.lam[w].f_e;
             }
             fa.stride_x = 3 * (size_t)N_;
             fa.stride_p = (size_t)P;
@@ -649,44 +613,17 @@ class NonbondedPotential : public PotentialBase {
         // single window (a finer tail: -8 % per MD step, -10 % per call), four
         // for several windows (fewer row flushes: -3 %)
         ta.chunk = K > 1 ? 4 : 1;
-        if (fused_rebuild_) {
-            RebuildArgs r;
-            r.sa = sa;
-            r.pa = pa;
-            r.perm = perm_.p;
-            r.slot_of = slot_of_.p;
-            r.nb_x = nb_x_.p;
-            r.nb_box = nb_box_.p;
-            r.ta = ta;
-            DevState *st = state_.p;
-            void *args[] = {&r, &st};
-            CK(cudaLaunchCooperativeKernel(
-                (const void *)k_rebuild, dim3(rebuild_grid()), dim3(TB_WARPS * 32), args, 0, stream));
-        } else {
-            const DevState *cst = state_.p;
-            launch_dependent(k_bin_keys, dim3(sgrid), dim3(tpb), 0, stream, sa, cst);
-            launch_dependent(k_bin_scan, dim3(1), dim3(1024), 0, stream, sa, state_.p);
-            launch_dependent(
-                k_bin_scatter, dim3(sgrid), dim3(tpb), 0, stream, sa, pa, perm_.p, slot_of_.p, nb_x_.p, nb_box_.p, cst);
-            const int bb_grid = std::max(1, (RB_ * 32 + tpb - 1) / tpb);
-            launch_dependent(
-                k_block_bounds, dim3(bb_grid), dim3(tpb), 0, stream, S_, d_box, (const float4 *)posw_.p, bb_ctr_.p,
-                bb_ext_.p, cst, pa, sa.n_first, perm_.p, slot_of_.p, rows_);
-            launch_dependent(k_build_tiles, dim3(n_row_blocks_), dim3(TB_WARPS * 32), 0, stream, ta, state_.p);
-        }
+        const DevState *cst = state_.p;
+        launch_dependent(k_bin_keys, dim3(sgrid), dim3(tpb), 0, stream, sa, cst);
+        launch_dependent(k_bin_scan, dim3(1), dim3(1024), 0, stream, sa, state_.p);
+        launch_dependent(
+            k_bin_scatter, dim3(sgrid), dim3(tpb), 0, stream, sa, pa, perm_.p, slot_of_.p, nb_x_.p, nb_box_.p, cst);
+        const int bb_grid = std::max(1, (RB_ * 32 + tpb - 1) / tpb);
+        launch_dependent(
+            k_block_bounds, dim3(bb_grid), dim3(tpb), 0, stream, S_, d_box, (const float4 *)posw_.p, bb_ctr_.p,
+            bb_ext_.p, cst, pa, sa.n_first, perm_.p, slot_of_.p, rows_);
+        launch_dependent(k_build_tiles, dim3(n_row_blocks_), dim3(TB_WARPS * 32), 0, stream, ta, state_.p);
         CK(cudaPeekAtLastError());
-    }
-
-    // Blocks of the cooperative rebuild: all co-resident (occupancy x SMs),
-    // and no more than the phases can use.
-    int rebuild_grid() {
-        if (rebuild_grid_ == 0) {
-            int per_sm = 0;
-            CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_rebuild, TB_WARPS * 32, 0));
-            const int want = std::max(n_row_blocks_, (S_ + TB_WARPS * 32 - 1) / (TB_WARPS * 32));
-            rebuild_grid_ = std::max(1, std::min(std::max(1, per_sm) * num_sms(), want));
-        }
-        return rebuild_grid_;
     }
 
     Accum accum() const {
@@ -738,9 +675,6 @@ class NonbondedPotential : public PotentialBase {
             if (st.error == DEV_ERR_NONORTHO_BOX) {
                 throw Error(TMNB_ERR_NONORTHO_BOX, "Provided non-ortholinear box, unable to compute nonbonded energy");
             }
-            if (st.error == DEV_ERR_BARRIER_TIMEOUT) {
-                throw Error(TMNB_ERR_INTERNAL, "neighbour-list rebuild: a grid barrier timed out");
-            }
             throw Error(
                 TMNB_ERR_BOX_TOO_SMALL,
                 "Cutoff with padding is more than half of the box width, neighborlist is no longer reliable");
@@ -786,6 +720,9 @@ class NonbondedPotential : public PotentialBase {
         cudaStream_t stream) {
         if (interp_ || kind_ == Kind::Group) {
             throw Error(TMNB_ERR_UNSUPPORTED, "the adjoint covers non-interpolated AllPairs, PairList and Nonbonded");
+        }
+        if (!xf_.w.is_identity()) {
+            throw Error(TMNB_ERR_UNSUPPORTED, "the adjoint covers the identity lambda transform of w only");
         }
         if (!d_g_dx || !d_grad_p || !d_grad_w) {
             throw Error(TMNB_ERR_INVALID_ARGUMENT, "upstream gradient and outputs must be non-null");
@@ -877,6 +814,8 @@ class NonbondedPotential : public PotentialBase {
     double padding_ = 0.1;
     bool interp_;
     bool negated_;
+    bool fp64_;
+    LambdaTransforms xf_;
     bool hilbert_ = true;
     bool has_nblist_ = false;
     bool split_pair_dp_ = false;
@@ -899,6 +838,7 @@ class NonbondedPotential : public PotentialBase {
     DevBuf<double> scales_;
     DevBuf<unsigned> perm_;
     DevBuf<float4> posw_, prm_, dprm_;
+    DevBuf<double4> posw64_, prm64_, dprm64_;
     DevBuf<unsigned char> lamdep_;
     DevBuf<unsigned long long> acc_;
     DevBuf<double> nb_x_, nb_box_;
@@ -910,20 +850,7 @@ class NonbondedPotential : public PotentialBase {
     DevBuf<int4> items_;
     DevBuf<int2> dep_tiles_;
     DevBuf<DevState> state_;
-    pair_kernel_t kernels_[N_SCHED][16];
-    pair_kernel_t kernels_multi_[N_SCHED][16];
-    bool compact_ = false; // compacted tile sweep (same results as the rotating sweep)
-    // the rebuild as one cooperative launch (k_rebuild) instead of five kernels
-    // (off by default: on a 22,840-atom MD step the cooperative launch measured
-    // ~10 us slower per step than the five kernels that return at once)
-    bool fused_rebuild_ = false;
-    int rebuild_grid_ = 0;
-    // captured launches put the rebuild chain under a conditional graph node
-    // (off by default: measured slower on a 23k-atom MD step than plain nodes
-    // that return at once, and ncu cannot profile the kernel nodes of graphs
-    // that hold conditional nodes)
-    bool conditional_rebuild_ = false;
-    cudaStream_t body_stream_ = nullptr; // captures the conditional node's body
+    PairKernels kernels_[3] = {};
 
     // pair-kernel timing
     bool timing_ = false;
@@ -1005,8 +932,8 @@ tmnb_status check_handle(const tmnb_potential *p) {
 }
 
 tmnb_status check_precision(int precision) {
-    if (precision != 32) {
-        tmb::g_last_error = "only precision=32 (FP32 pair arithmetic) is built";
+    if (precision != 32 && precision != 64) {
+        tmb::g_last_error = "precision must be 32 (FP32 pair arithmetic) or 64 (FP64)";
         return TMNB_ERR_UNSUPPORTED;
     }
     return TMNB_OK;
@@ -1053,7 +980,8 @@ tmnb_status tmnb_all_pairs_create(
             nullptr,
             0,
             false,
-            interpolated != 0);
+            interpolated != 0,
+            precision == 64);
         *out = h.release();
     });
 }
@@ -1091,7 +1019,8 @@ tmnb_status tmnb_interaction_group_create(
             nullptr,
             0,
             false,
-            interpolated != 0);
+            interpolated != 0,
+            precision == 64);
         *out = h.release();
     });
 }
@@ -1131,7 +1060,8 @@ tmnb_status tmnb_pair_list_create(
             scales,
             M,
             negated != 0,
-            interpolated != 0);
+            interpolated != 0,
+            precision == 64);
         *out = h.release();
     });
 }
@@ -1170,7 +1100,8 @@ tmnb_status tmnb_nonbonded_create(
             scales,
             M,
             true,
-            interpolated != 0);
+            interpolated != 0,
+            precision == 64);
         *out = h.release();
     });
 }
@@ -1351,18 +1282,26 @@ tmnb_status tmnb_potential_disable_hilbert_sort(tmnb_potential *pot) {
     return tmb::guarded([&] { as_nb(pot)->disable_hilbert(); });
 }
 
-tmnb_status tmnb_potential_set_pair_schedule(tmnb_potential *pot, int compact) {
-    if (tmnb_status s = check_handle(pot)) {
-        return s;
+tmnb_status tmnb_lambda_transform_eval(const char *expression, double lambda, double *f, double *df) {
+    if (!expression || !f || !df) {
+        tmb::g_last_error = "null argument";
+        return TMNB_ERR_INVALID_ARGUMENT;
     }
-    return tmb::guarded([&] { as_nb(pot)->set_compact(compact != 0); });
+    return tmb::guarded([&] {
+        try {
+            tmb::LambdaExpr(expression).eval(lambda, *f, *df);
+        } catch (const std::invalid_argument &e) {
+            throw tmb::Error(TMNB_ERR_INVALID_ARGUMENT, e.what());
+        }
+    });
 }
 
-tmnb_status tmnb_potential_set_rebuild_mode(tmnb_potential *pot, int fused, int conditional) {
+tmnb_status tmnb_potential_set_lambda_transforms(
+    tmnb_potential *pot, const char *charge, const char *sigma, const char *epsilon, const char *w) {
     if (tmnb_status s = check_handle(pot)) {
         return s;
     }
-    return tmb::guarded([&] { as_nb(pot)->set_rebuild_mode(fused != 0, conditional != 0); });
+    return tmb::guarded([&] { as_nb(pot)->set_transforms(charge, sigma, epsilon, w); });
 }
 
 tmnb_status tmnb_potential_set_tile_rows(tmnb_potential *pot, int rows) {

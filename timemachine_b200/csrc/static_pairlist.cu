@@ -29,11 +29,12 @@ constexpr size_t OFF_LAMDEP = OFF_PERM + align256(sizeof(unsigned) * SMAX);     
 constexpr size_t OFF_STATE = OFF_LAMDEP + align256(SMAX);                          // DevState
 constexpr size_t SCRATCH_BYTES = OFF_STATE + align256(sizeof(DevState));           // 3.16 MiB
 
-// Zero at module load. The accumulators and the device state must be zero
-// when a call starts: k_finalize takes (reads and zeroes) every accumulator,
-// and the entry point reads and clears the error word before returning, so
-// each call leaves them at zero for the next. The slot order section holds
-// the identity, written once by the set-up.
+// Zero at module load. The accumulators and the device state's error word
+// must be zero when a call starts: each call clears both on its stream before
+// its first kernel (so a call that failed half-way cannot leak into the
+// next), k_finalize takes (reads and zeroes) every accumulator it reads, and
+// the error word is read back at the end. The slot order section holds the
+// identity, written once by the set-up.
 static __device__ __align__(256) unsigned char g_static_scratch[SCRATCH_BYTES];
 
 constexpr int DEV_ERR_BAD_PAIR = 5;
@@ -59,7 +60,8 @@ __global__ void k_static_check_pairs(int N, int M, const int *pairs, DevState *s
 typedef void (*static_pair_kernel_t)(PairArgs);
 
 template <int I> constexpr static_pair_kernel_t static_kernel() {
-    return &k_pair<float, (I >> 3) & 1, (I >> 2) & 1, (I >> 1) & 1, (I >> 0) & 1, false, false>;
+    return &k_pair<float, bool((I >> 3) & 1), bool((I >> 2) & 1), bool((I >> 1) & 1), bool((I >> 0) & 1), false,
+                   false>;
 }
 template <int... Is> struct StaticKernels {
     static void fill(static_pair_kernel_t *out) { ((out[Is] = static_kernel<Is>()), ...); }
@@ -185,7 +187,9 @@ void execute_static(
     pa.box = d_box;
     pa.K = 1;
     for (int k = 0; k < MAX_WINDOWS; k++) {
-        pa.lambdas[k] = k == 0 ? lambda : 0.0;
+        // identity lambda transform: f = lambda, df/dlambda = 1
+        const double l = k == 0 ? lambda : 0.0;
+        pa.lam[k] = LambdaWindow{l, 1.0, l, 1.0, l, 1.0, l, 1.0};
     }
     pa.cutoff = cutoff;
     pa.padding = 0.0;
@@ -196,6 +200,15 @@ void execute_static(
     pa.slots.prm = prm;
     pa.slots.dprm = nullptr;
     pa.slots.lamdep = lamdep;
+    pa.slots.posw64 = nullptr;
+    pa.slots.prm64 = nullptr;
+    pa.slots.dprm64 = nullptr;
+
+    // Every call starts from a clean state on the caller's stream: the error
+    // word and the accumulators are cleared here, not only at the end of the
+    // previous call, so a call that stopped half-way leaves nothing behind.
+    CK(cudaMemsetAsync(&state->error, 0, sizeof(int), stream));
+    CK(cudaMemsetAsync(acc, 0, sizeof(unsigned long long) * 8 * (size_t)SMAX, stream));
 
     const int tpb = 256;
     const int sgrid = std::max(1, std::min((N + tpb - 1) / tpb, 8 * num_sms()));
@@ -216,6 +229,9 @@ void execute_static(
         a.posw = posw;
         a.prm = prm;
         a.dprm = nullptr;
+        a.posw64 = nullptr;
+        a.prm64 = nullptr;
+        a.dprm64 = nullptr;
         a.lamdep = lamdep;
         a.box = d_box;
         a.beta = beta;
@@ -239,7 +255,7 @@ void execute_static(
         fa.S = N;
         fa.K = 1;
         for (int k = 0; k < MAX_WINDOWS; k++) {
-            fa.lambdas[k] = pa.lambdas[k];
+            fa.f_dp[k][0] = fa.f_dp[k][1] = fa.f_dp[k][2] = pa.lam[k].f_q;
         }
         fa.set_atoms = nullptr;
         fa.slot_of = nullptr;
@@ -260,13 +276,13 @@ void execute_static(
         CK(cudaPeekAtLastError());
     }
 
-    // report (and clear) a pair-index error found on the device
-    CK(cudaStreamSynchronize(stream));
+    // report (and clear) a pair-index error found on the device; all traffic
+    // stays on the caller's stream (no legacy-default-stream copies)
     int err = 0;
-    CK(cudaMemcpy(&err, &state->error, sizeof(int), cudaMemcpyDeviceToHost));
+    CK(cudaMemcpyAsync(&err, &state->error, sizeof(int), cudaMemcpyDeviceToHost, stream));
+    CK(cudaStreamSynchronize(stream));
     if (err != 0) {
-        const int zero = 0;
-        CK(cudaMemcpy(&state->error, &zero, sizeof(int), cudaMemcpyHostToDevice));
+        CK(cudaMemsetAsync(&state->error, 0, sizeof(int), stream));
         throw Error(TMNB_ERR_INVALID_ARGUMENT, "pair index out of range [0, N) or src == dst; outputs left unchanged");
     }
 }

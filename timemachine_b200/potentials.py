@@ -45,9 +45,47 @@ def _ptr(a):
 
 
 def _precision_bits(precision):
+    """np.float32 -> 32 (FP32 pair arithmetic, the reference's _f32 kernels);
+    np.float64 -> 64 (FP64 pair arithmetic, the reference's _f64 kernels)."""
     if precision == np.float64:
         return 64
-    return 32
+    if precision == np.float32:
+        return 32
+    raise RuntimeError(f"unsupported precision {precision!r}: use np.float32 or np.float64")
+
+
+_TRANSFORM_NAMES = ("transform_lambda_charge", "transform_lambda_sigma", "transform_lambda_epsilon", "transform_lambda_w")
+
+
+def _transforms(extra):
+    """The four lambda-transform expressions that follow a constructor's
+    regular arguments (timemachine/cpp/src/wrap_kernels.cpp:843-893), "lambda"
+    where absent."""
+    extra = list(extra)
+    if len(extra) > 4:
+        raise RuntimeError(f"expected at most 4 lambda transform expressions, got {len(extra)}")
+    out = []
+    for k, name in enumerate(_TRANSFORM_NAMES):
+        v = extra[k] if k < len(extra) else "lambda"
+        if not isinstance(v, str):
+            raise RuntimeError(f"{name} must be a string expression in lambda, got {v!r}")
+        out.append(v)
+    return out
+
+
+def _apply_transforms(handle, extra):
+    t = _transforms(extra)
+    if any(e.strip() != "lambda" for e in t):
+        _lib.check(_lib.lib().tmnb_potential_set_lambda_transforms(handle, *[e.encode() for e in t]))
+
+
+def lambda_transform(expression, lam):
+    """(f, df/dlambda) of one lambda-transform expression at lam, as the
+    potentials evaluate their schedules (host-side parser of the C ABI)."""
+    f, df = ctypes.c_double(), ctypes.c_double()
+    _lib.check(_lib.lib().tmnb_lambda_transform_eval(str(expression).encode(), float(lam), ctypes.byref(f),
+                                                     ctypes.byref(df)))
+    return f.value, df.value
 
 
 class Potential:
@@ -78,19 +116,10 @@ class Potential:
     def disable_hilbert_sort(self):
         _lib.check(self._lib.tmnb_potential_disable_hilbert_sort(self._h))
 
-    def set_pair_schedule(self, compact=False):
-        """Rotating (default) or compacted tile sweep; identical results."""
-        _lib.check(self._lib.tmnb_potential_set_pair_schedule(self._h, 1 if compact else 0))
-
     def set_tile_rows(self, rows=16):
-        """Rows per neighbour-list tile: 16 (default), 32 or 8 slots (identical results)."""
+        """Rows per neighbour-list tile: 16 (default), 32 or 8 slots (identical
+        results; FP64 potentials use 16)."""
         _lib.check(self._lib.tmnb_potential_set_tile_rows(self._h, int(rows)))
-
-    def set_rebuild_mode(self, fused=False, conditional=False):
-        """Neighbour-list rebuild as five kernels (default) or one cooperative
-        launch (fused); under stream capture as plain nodes (default) or a
-        conditional graph node. Identical results in every mode."""
-        _lib.check(self._lib.tmnb_potential_set_rebuild_mode(self._h, 1 if fused else 0, 1 if conditional else 0))
 
     def num_params(self):
         return self._lib.tmnb_potential_num_params(self._h)
@@ -458,8 +487,7 @@ class CustomOpWrapper:
 
 
 def _check_precision(precision):
-    if _precision_bits(precision) != 32:
-        raise RuntimeError("only float32 pair arithmetic is built on this backend (precision=np.float32)")
+    return _precision_bits(precision)
 
 
 def _plane_offset(plane, offset):
@@ -487,10 +515,11 @@ class NonbondedAllPairs(CustomOpWrapper):
     _interpolated = False
 
     def unbound_impl(self, precision):
-        _check_precision(precision)
+        bits = _check_precision(precision)
         plane, offset = _plane_offset(self.args[0], self.args[1])
         beta, cutoff = float(self.args[2]), float(self.args[3])
         atom_idxs = self.args[4] if len(self.args) > 4 else None
+        extra = self.args[5:]
         N = plane.size
         aidx, K = None, 0
         if atom_idxs is not None:
@@ -510,11 +539,13 @@ class NonbondedAllPairs(CustomOpWrapper):
                 _ptr(aidx),
                 K,
                 1 if self._interpolated else 0,
-                32,
+                bits,
                 ctypes.byref(h),
             )
         )
-        return Potential(h, "NonbondedAllPairs", self._interpolated)
+        pot = Potential(h, "NonbondedAllPairs", self._interpolated)
+        _apply_transforms(h, extra)
+        return pot
 
 
 class NonbondedAllPairsInterpolated(NonbondedAllPairs):
@@ -523,12 +554,13 @@ class NonbondedAllPairsInterpolated(NonbondedAllPairs):
 
 class NonbondedInteractionGroup(CustomOpWrapper):
     """timemachine/lib/potentials.py:389-399: pairs of one row atom and one
-    other atom. args: (row_atom_idxs, lambda_plane_idxs, lambda_offset_idxs, beta, cutoff)."""
+    other atom. args: (row_atom_idxs, lambda_plane_idxs, lambda_offset_idxs, beta, cutoff
+    [, 4 lambda transform expressions])."""
 
     _interpolated = False
 
     def unbound_impl(self, precision):
-        _check_precision(precision)
+        bits = _check_precision(precision)
         rows = np.ascontiguousarray(self.args[0], dtype=np.int32).reshape(-1)
         if len(set(rows.tolist())) != rows.size:
             # the binding's unique_idxs (timemachine/cpp/src/wrap_kernels.cpp:922)
@@ -546,11 +578,12 @@ class NonbondedInteractionGroup(CustomOpWrapper):
                 float(self.args[3]),
                 float(self.args[4]),
                 1 if self._interpolated else 0,
-                32,
+                bits,
                 ctypes.byref(h),
             )
         )
         pot = Potential(h, "NonbondedInteractionGroup", self._interpolated)
+        _apply_transforms(h, self.args[5:])
         pot._group_rows = rows.size
         return pot
 
@@ -560,13 +593,14 @@ class NonbondedInteractionGroupInterpolated(NonbondedInteractionGroup):
 
 
 class NonbondedPairList(CustomOpWrapper):
-    """args: (pair_idxs, scales, lambda_plane_idxs, lambda_offset_idxs, beta, cutoff)."""
+    """args: (pair_idxs, scales, lambda_plane_idxs, lambda_offset_idxs, beta, cutoff
+    [, 4 lambda transform expressions])."""
 
     _interpolated = False
     _negated = False
 
     def unbound_impl(self, precision):
-        _check_precision(precision)
+        bits = _check_precision(precision)
         pairs, scales, M = _pairs_scales(self.args[0], self.args[1])
         plane, offset = _plane_offset(self.args[2], self.args[3])
         h = ctypes.c_void_p()
@@ -583,11 +617,13 @@ class NonbondedPairList(CustomOpWrapper):
                 float(self.args[5]),
                 1 if self._negated else 0,
                 1 if self._interpolated else 0,
-                32,
+                bits,
                 ctypes.byref(h),
             )
         )
-        return Potential(h, "NonbondedPairList", self._interpolated)
+        pot = Potential(h, "NonbondedPairList", self._interpolated)
+        _apply_transforms(h, self.args[6:])
+        return pot
 
 
 class NonbondedPairListNegated(NonbondedPairList):
@@ -606,7 +642,14 @@ class NonbondedPairListNegatedInterpolated(NonbondedPairList):
 class Nonbonded(CustomOpWrapper):
     """timemachine/lib/potentials.py:269-344.
 
-    args: (exclusion_idxs, scale_factors, lambda_plane_idxs, lambda_offset_idxs, beta, cutoff)
+    args: (exclusion_idxs, scale_factors, lambda_plane_idxs, lambda_offset_idxs, beta, cutoff
+    [, 4 lambda transform expressions: NonbondedInterpolated only])
+
+    The reference's Nonbonded.unbound_impl does not pass args[6:] on to its
+    parts (timemachine/lib/potentials.py:284-301), so a non-identity
+    expression there would be dropped without notice: this class raises
+    instead. NonbondedInterpolated forwards them, as the reference's does
+    (timemachine/lib/potentials.py:355,365).
     """
 
     _interpolated = False
@@ -621,7 +664,13 @@ class Nonbonded(CustomOpWrapper):
         super().__init__(*args)
 
     def unbound_impl(self, precision):
-        _check_precision(precision)
+        bits = _check_precision(precision)
+        extra = _transforms(self.args[6:])
+        if not self._interpolated and any(e.strip() != "lambda" for e in extra):
+            raise RuntimeError(
+                "Nonbonded does not apply lambda transform expressions (the reference drops args[6:] here); "
+                "use NonbondedInterpolated, NonbondedAllPairs or NonbondedPairList to apply them"
+            )
         pairs, scales, M = _pairs_scales(self.get_exclusion_idxs(), self.get_scale_factors())
         plane, offset = _plane_offset(self.get_lambda_plane_idxs(), self.get_lambda_offset_idxs())
         h = ctypes.c_void_p()
@@ -637,11 +686,13 @@ class Nonbonded(CustomOpWrapper):
                 float(self.get_beta()),
                 float(self.get_cutoff()),
                 1 if self._interpolated else 0,
-                32,
+                bits,
                 ctypes.byref(h),
             )
         )
-        return Potential(h, "Nonbonded", self._interpolated)
+        pot = Potential(h, "Nonbonded", self._interpolated)
+        _apply_transforms(h, extra)
+        return pot
 
     def set_exclusion_idxs(self, x):
         self.args[0] = x
@@ -695,7 +746,8 @@ class _BondedWrapper(CustomOpWrapper):
     _ctor = "tmnb_harmonic_bond_create"
 
     def unbound_impl(self, precision):
-        _check_precision(precision)
+        if _check_precision(precision) != 32:
+            raise RuntimeError(f"{type(self).__name__} is built with FP32 arithmetic only (precision=np.float32)")
         idxs = np.ascontiguousarray(self.args[0], dtype=np.int32).reshape(-1, self._arity)
         T = idxs.shape[0]
         mult = self.args[1] if len(self.args) > 1 else None
@@ -723,4 +775,4 @@ def all_flag_combinations():
     return list(itertools.product([False, True], repeat=4))
 
 
-__all__ += ["all_flag_combinations", "FIXED_EXPONENT", "HarmonicBond", "HarmonicAngle"]
+__all__ += ["all_flag_combinations", "FIXED_EXPONENT", "HarmonicBond", "HarmonicAngle", "lambda_transform"]
