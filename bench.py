@@ -40,16 +40,69 @@ sys.path.insert(0, HERE)
 
 N_WINDOWS = 12
 SEED = 2024
-# FP32 operations per in-cutoff pair of the full evaluation (u, du_dx, du_dp,
-# du_dl; FMA = 2, rsqrt/exp/div = 1 each), counted on the per-pair expression
-# DAG: distance + minimum image 21, electrostatics + erfc 28, forces 6,
-# parameter derivatives 11, energy 1 -> 67; Lennard-Jones adds 26 for pairs
-# where both atoms carry epsilon.
-FLOPS_PER_PAIR = 67
-FLOPS_PER_LJ_PAIR = 26
+
+# FP32 operations of one in-cutoff pair of the full evaluation (u, du_dx,
+# du_dp, du_dl), counted on the per-pair arithmetic of the pair kernel
+# (timemachine_b200/csrc/nb_pair_math.cuh, pair_terms / sweep_tile in
+# nb_kernels.cuh), which restates timemachine/cpp/src/kernels/nonbonded_common.cuh:38-140
+# and k_nonbonded.cuh:424-512. FMA = 2; FMUL, FADD = 1; rsqrt, ex2 and the
+# IEEE reciprocal = 1 each; the fixed-point scalings (v * 2^e) are counted,
+# the float->int64 conversions and integer adds are not.
+FLOP_TABLE = {
+    "distance": {
+        "3 coordinate differences": 3,
+        "minimum image, 3 axes x (fmul by 1/L, 2 adds of the rounding constant, ffma)": 15,
+        "d^2 = ffma(dz,dz,ffma(dx,dx,dy*dy))": 5,
+    },
+    "electrostatics": {
+        "rsqrt": 1,
+        "d = d2*inv_d, inv_d2 = inv_d^2": 2,
+        "q_i q_j, (scale*q_i q_j)*inv_d": 3,
+        "beta*d, -(beta d)^2, exp via ex2 (fmul + ex2)": 4,
+        "1/(1 + 0.3275911 beta d): ffma + reciprocal": 3,
+        "A&S 7.1.26 polynomial: 4 ffma": 8,
+        "erfc = poly*t*e: 2 fmul": 2,
+        "2/sqrt(pi)*beta*d, ffma(cbd, e, erfc), -inv_d2 * (...)": 4,
+        "prefactor = qij_inv * factor": 1,
+        "energy qij_inv * erfc": 1,
+    },
+    "forces": {"3 x (prefactor*delta)*2^36": 6},
+    "charge derivatives": {"2 x (q_j*inv_d)*erfc": 4, "2 x fixed-point scaling": 2},
+    "energy": {"fixed-point scaling": 1},
+    "lennard_jones (both atoms carry epsilon)": {
+        "eps_ij, sig_ij, s, s^2, s^4, s^6, s^6/d^2, s^5/d (2)": 9,
+        "s^6 - 1": 1,
+        "(scale*eps_ij)*s^6/d^2": 2,
+        "ffma(s^6, 48, -24)": 2,
+        "prefactor ffma": 2,
+        "energy (3 fmul) + ffma": 5,
+        "2 s^6 - 1 (ffma)": 2,
+        "sigma gradient: 4 fmul": 4,
+        "epsilon gradient: 3 fmul": 3,
+        "2 x eps_grad*eps_j": 2,
+        "3 fixed-point scalings": 3,
+    },
+    "lambda-dependent pair (an atom with a nonzero lambda offset)": {
+        "dw, d^2 += dw^2 (fsub + ffma)": 3,
+        "du_dl = ffma(dw*prefactor, dw_dl_i - dw_dl_j, .): fmul + fsub + ffma": 4,
+        "fixed-point scaling": 1,
+    },
+}
+
+
+def _table_sum(*groups):
+    return sum(sum(FLOP_TABLE[g].values()) for g in groups)
+
+
+# 65 per plain pair, +35 where both atoms carry LJ, +8 where either atom is lambda-dependent
+FLOPS_PER_PAIR = _table_sum("distance", "electrostatics", "forces", "charge derivatives", "energy")
+FLOPS_PER_LJ_PAIR = _table_sum("lennard_jones (both atoms carry epsilon)")
+FLOPS_PER_ALCH_PAIR = _table_sum("lambda-dependent pair (an atom with a nonzero lambda offset)")
 # DRAM bytes (read + write) of one 12-window pair-kernel launch on this
 # workload, from an ncu capture of the same command (15.7 MB read, 0 written)
 PAIR_LAUNCH_DRAM_BYTES = 15.7e6
+# stages of a call timed by tmnb_potential_last_stage_ms
+STAGE_PREPARE, STAGE_REBUILD, STAGE_PAIR, STAGE_FINALIZE = 0, 1, 2, 3
 
 
 def parse():
@@ -259,9 +312,11 @@ def build_workload(rank):
 
 
 def count_pairs(s, x, lambdas):
-    """In-cutoff pairs (4D distance < cutoff) per window, and how many carry LJ;
-    plus the pairs one multi-window evaluation computes: pairs of two
-    lambda-independent atoms once, the others once per window."""
+    """In-cutoff pairs (4D distance < cutoff) per window: (pairs, LJ pairs,
+    lambda-dependent pairs), the excluded/scaled pairs included (the launch
+    evaluates them too); plus the same counts over what one multi-window
+    evaluation computes: pairs of two lambda-independent atoms once, the
+    others once per window."""
     from scipy.spatial import cKDTree
 
     L = np.diag(s.box)
@@ -272,21 +327,33 @@ def count_pairs(s, x, lambdas):
     d = x[i] - x[j]
     d -= L * np.round(d / L)
     d2 = (d * d).sum(1)
+    excl = np.sort(np.asarray(s.exclusion_idxs).reshape(-1, 2), axis=1)
+    # the scaled pairs are evaluated in the same launch: count them as pairs too
+    ei, ej = excl[:, 0], excl[:, 1]
+    de = x[ei] - x[ej]
+    de -= L * np.round(de / L)
+    i = np.concatenate([i, ei])
+    j = np.concatenate([j, ej])
+    d2 = np.concatenate([d2, (de * de).sum(1)])
     lj = (s.params[i, 2] != 0) & (s.params[j, 2] != 0)
-    excl = set(map(tuple, np.sort(s.exclusion_idxs, axis=1).tolist()))
     dep_atom = s.lambda_offset_idxs != 0
     dep = dep_atom[i] | dep_atom[j]
     out = []
-    shared = [0, 0]
+    shared = [0, 0, 0]
     for k, lam in enumerate(lambdas):
         w = s.cutoff * (s.lambda_plane_idxs + s.lambda_offset_idxs * lam)
         keep = d2 + (w[i] - w[j]) ** 2 < s.cutoff**2
-        out.append((int(keep.sum()), int((keep & lj).sum())))
+        out.append((int(keep.sum()), int((keep & lj).sum()), int((keep & dep).sum())))
         if k == 0:
-            shared = [int((keep & ~dep).sum()), int((keep & ~dep & lj).sum())]
+            shared = [int((keep & ~dep).sum()), int((keep & ~dep & lj).sum()), 0]
         shared[0] += int((keep & dep).sum())
         shared[1] += int((keep & dep & lj).sum())
+        shared[2] += int((keep & dep).sum())
     return out, len(excl), tuple(shared)
+
+
+def flops_of(pairs, lj_pairs, dep_pairs):
+    return pairs * FLOPS_PER_PAIR + lj_pairs * FLOPS_PER_LJ_PAIR + dep_pairs * FLOPS_PER_ALCH_PAIR
 
 
 def measured_peaks():
@@ -294,6 +361,73 @@ def measured_peaks():
         return json.load(open(os.path.join(HERE, "MEASURED_PEAKS.json")))
     except Exception:
         return {}
+
+
+def stage_ms(lib, impl, stage):
+    import ctypes
+
+    from timemachine_b200 import _lib
+
+    ms = ctypes.c_float()
+    _lib.check(lib.tmnb_potential_last_stage_ms(impl.handle, stage, ctypes.byref(ms)))
+    return ms.value
+
+
+def hbm_roofline(N, K, ms, tiles, items, peak):
+    """Achieved HBM GB/s of the bandwidth-bound stages of a K-window call,
+    from their algorithmic bytes (the data each must move once) and their
+    CUDA-event durations.
+
+    prepare (k_check_prepare): reads x, the list's x, params (f64, 24 B each),
+      plane + offset, slot order, lambda flag (13 B); writes K x 32 B of
+      staged float4 coordinates + parameters and the flag.
+    rebuild (sort, scatter, block bounds, tile build; on a rebuild call):
+      reads x twice (keys, scatter) and params (LJ order); writes the slot
+      order, the list's x, the staging (K x 32 B), bounds; the tiles
+      (tiles x 32 column slots x 4 B) and work items (16 B).
+    finalize (k_finalize + accumulator reset): reads the 8 accumulator arrays
+      of the shared block and of the K window blocks (8 B each); adds K
+      windows of outputs (du_dx, du_dp 24 B, du_dl, u 8 B: read + write);
+      zeroes the blocks it read.
+    """
+    blocks = 1 + K if K > 1 else 1
+    b_prepare = N * (24 + 24 + 24 + 13 + 1 + 32 * K)
+    b_rebuild = N * (24 * 2 + 24 + 8 + 24 + 32 * K) + (N // 32 + 1) * 32 + tiles * 32 * 4 + items * 16
+    b_finalize = N * (8 * 8 * blocks * 2 + K * 64 * 2)
+    out = {}
+    for name, b, t in [
+        ("k_check_prepare", b_prepare, ms["prepare"]),
+        ("rebuild_chain (k_bin_keys..k_build_tiles)", b_rebuild, ms["rebuild"]),
+        ("k_finalize + reset", b_finalize, ms["finalize"]),
+    ]:
+        gbs = b / (t * 1e-3) / 1e9
+        out[name] = {"bytes": int(b), "ms": t, "achieved_gbs": gbs, "frac": gbs / peak}
+    return out
+
+
+def output_errors(s, x, p, lam, fixed_by_precision):
+    """Relative errors of (du_dx, du_dp, du_dl, u) against the FP64 oracle at
+    one lambda window: forces by max_i |dF_i| / max(|F_i|, 1)
+    (tests/common.py:386-409), du_dp by max |d| / max |ref|, u and du_dl by
+    |d| / max(|ref|, 1)."""
+    from oracle.nonbonded_oracle import Oracle, force_error, rel_error
+    from timemachine_b200.fixed_point import du_dp_fixed_to_float, fixed_to_float, sum_fixed
+
+    o = Oracle(s.lambda_plane_idxs, s.lambda_offset_idxs, s.beta, s.cutoff, s.exclusion_idxs, s.scales)
+    r_dx, r_dp, r_dl, r_u = o(x, p, s.box, lam)
+    res = {"lambda": float(lam), "oracle": "FP64 restatement of the reference's nonbonded_v3 (oracle/)"}
+    for name, (fdx, fdp, fdl, fu) in fixed_by_precision.items():
+        dx = fixed_to_float(fdx)
+        dp = du_dp_fixed_to_float(fdp).reshape(p.shape)
+        dl = fixed_to_float(sum_fixed(fdl))
+        u = fixed_to_float(sum_fixed(fu))
+        res[name] = {
+            "du_dx": force_error(r_dx, dx),
+            "du_dp": rel_error(r_dp, dp),
+            "du_dl": abs(dl - r_dl) / max(abs(r_dl), 1.0),
+            "u": abs(u - r_u) / max(abs(r_u), 1.0),
+        }
+    return res
 
 
 def run_tmnb(args, world, rank, local):
@@ -321,12 +455,15 @@ def run_tmnb(args, world, rank, local):
     stream = torch.cuda.current_stream(dev)
     lib = _lib.lib()
 
-    def one_step():
+    def zero_outputs():
         o_dx.zero_()
         o_dp.zero_()
         o_dl.zero_()
         o_u.zero_()
-        impl.execute_windows_device(dx, dp, db, lambdas, o_dx, o_dp, o_dl, o_u, stream=stream)
+
+    def one_step(pot=impl):
+        zero_outputs()
+        pot.execute_windows_device(dx, dp, db, lambdas, o_dx, o_dp, o_dl, o_u, stream=stream)
 
     # the single-window calls use their own potential, as a caller making only
     # single-window calls would (its neighbour list is built by one of them)
@@ -340,14 +477,15 @@ def run_tmnb(args, world, rank, local):
             o_u[k].zero_()
             impl1.execute_device(dx, dp, db, float(lam), o_dx[k], o_dp[k], o_dl[k], o_u[k], stream=stream)
 
-    def timed(step_fn):
+    def timed(step_fn, steps=None):
+        steps = args.steps if steps is None else steps
         for _ in range(args.warmup):
             step_fn()
         torch.cuda.synchronize()
-        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+        evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(steps)]
         barrier(world)
         torch.cuda.synchronize()
-        for k in range(args.steps):
+        for k in range(steps):
             flush.zero_()
             evs[k][0].record(stream)
             step_fn()
@@ -365,35 +503,58 @@ def run_tmnb(args, world, rank, local):
     evals = args.steps * N_WINDOWS * world
     value = evals / (total_ms / 1e3)
     seq_value = evals / (seq_ms / 1e3)
+    f32_fixed = [t[6].cpu().numpy().view(np.uint64) for t in (o_dx, o_dp, o_dl, o_u)]
 
-    # pair-kernel duration of the multi-window launch (events on the launching stream)
+    # per-stage durations of the multi-window call (events on the launching stream)
     _lib.check(lib.tmnb_potential_enable_timing(impl.handle, 1))
-    pair_ms = []
+    st = {"prepare": [], "pair": [], "finalize": [], "rebuild": []}
     for _ in range(5):
         flush.zero_()
         one_step()
-        ms = ctypes.c_float()
-        _lib.check(lib.tmnb_potential_last_pair_kernel_ms(impl.handle, ctypes.byref(ms)))
-        pair_ms.append(ms.value)
+        for name, k in [("prepare", STAGE_PREPARE), ("pair", STAGE_PAIR), ("finalize", STAGE_FINALIZE)]:
+            st[name].append(stage_ms(lib, impl, k))
+    # rebuild calls: the coordinates alternate by 0.06 nm (> padding / 2), so every call rebuilds
+    dx_shift = dx.clone()
+    dx_shift[:, 0] += 0.06
+    for k in range(6):
+        flush.zero_()
+        zero_outputs()
+        impl.execute_windows_device(dx_shift if k % 2 == 0 else dx, dp, db, lambdas, o_dx, o_dp, o_dl, o_u,
+                                    stream=stream)
+        st["rebuild"].append(stage_ms(lib, impl, STAGE_REBUILD))
     _lib.check(lib.tmnb_potential_enable_timing(impl.handle, 0))
+    pair_ms = st["pair"]
     _lib.check(lib.tmnb_potential_enable_timing(impl1.handle, 1))
     pair_ms_single = []
     for _ in range(2):
         for lam in lambdas:
             flush.zero_()
             impl1.execute_device(dx, dp, db, float(lam), o_dx[0], o_dp[0], o_dl[0], o_u[0], stream=stream)
-            ms = ctypes.c_float()
-            _lib.check(lib.tmnb_potential_last_pair_kernel_ms(impl1.handle, ctypes.byref(ms)))
-            pair_ms_single.append(ms.value)
+            pair_ms_single.append(stage_ms(lib, impl1, STAGE_PAIR))
     _lib.check(lib.tmnb_potential_enable_timing(impl1.handle, 0))
     peak = ctypes.c_double()
     _lib.check(lib.tmnb_probe_fp32_peak(ctypes.byref(peak)))
-    counts, n_excl, (shared_pairs, shared_lj) = count_pairs(s, x, lambdas)
-    flops_launch = shared_pairs * FLOPS_PER_PAIR + shared_lj * FLOPS_PER_LJ_PAIR
+    counts, n_excl, shared = count_pairs(s, x, lambdas)
+    flops_launch = flops_of(*shared)
     pair_s = float(np.mean(pair_ms)) / 1e3
     achieved = flops_launch / pair_s / 1e12
-    flops_single = float(np.mean([c * FLOPS_PER_PAIR + lj * FLOPS_PER_LJ_PAIR for c, lj in counts]))
+    flops_single = float(np.mean([flops_of(*c) for c in counts]))
     achieved_single = flops_single / (float(np.mean(pair_ms_single)) / 1e3) / 1e12
+    peaks = measured_peaks()
+    hbm_peak = float(peaks.get("hbm_gbs", 6650.0))
+    hbm = hbm_roofline(
+        N, K, {k: float(np.median(v)) for k, v in st.items()}, tiles, items, hbm_peak
+    )
+
+    # FP64 pair arithmetic (unbound_impl(np.float64)): the same 12-window call
+    impl64 = nb.unbound_impl(np.float64)
+    ms64 = timed(lambda: one_step(impl64), steps=max(3, args.steps // 4))
+    value64 = max(3, args.steps // 4) * N_WINDOWS * world / (ms64 / 1e3)
+    f64_fixed = [t[6].cpu().numpy().view(np.uint64) for t in (o_dx, o_dp, o_dl, o_u)]
+    del impl64
+    errors = None
+    if rank == 0:
+        errors = output_errors(s, x, p, float(lambdas[6]), {"f32": f32_fixed, "f64": f64_fixed})
 
     # end to end through the C-ABI host entry (pinned host buffers, copies inside)
     hx = torch.as_tensor(x).pin_memory().numpy()
@@ -428,7 +589,8 @@ def run_tmnb(args, world, rank, local):
     h2d = hx.nbytes + hp.nbytes + hb.nbytes + hl.nbytes
     d2h = sum(o.nbytes for o in outs)
 
-    launches_per_step = 8  # check/prepare, 5 rebuild-path kernels (early exit unless rebuilding), pair, finalize
+    # check/prepare, 5 rebuild-chain kernels (returning at once unless rebuilding), dep tiles, pair, finalize
+    launches_per_step = 9
     result = {
         "metric": "nonbonded evals/s at 22,840 atoms (u, du_dx, du_dp, du_dl; 12 lambda windows per step)",
         "value": value,
@@ -443,15 +605,16 @@ def run_tmnb(args, world, rank, local):
         "dtype": "f32 pair arithmetic, int64 fixed-point accumulation",
         "data": "synthetic (seeded water + ligand box; DHFR needs OpenMM)",
         "config": {
-            "workload": "water_ligand_22840: 7,600 waters + 40-atom ligand, 6.1 nm box, cutoff 1.2, beta 2.0, 12 lambda windows in one multi-window call",
+            "workload": "water_ligand_22840: 7,600 waters + 40-atom ligand, 6.1 nm box, 12 lambda windows per call",
             "atoms": N,
             "exclusions": int(n_excl),
-            "pairs_in_cutoff_per_eval": int(np.mean([c for c, _ in counts])),
+            "pairs_in_cutoff_per_eval": int(np.mean([c[0] for c in counts])),
             "nblist_tiles": tiles,
             "nblist_items": items,
             "l2": "flushed before every timed step (256 MiB write)",
             "parallelism": f"replicas x{world}",
-            "pairs_per_multi_window_launch": int(shared_pairs),
+            "pairs_per_multi_window_launch": int(shared[0]),
+            "errors_vs_fp64_oracle": errors,
         },
         "e2e": {"value": e2e_value, "unit": "evals/s", "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
         "gpu_launches": launches_per_step * args.steps,
@@ -462,14 +625,18 @@ def run_tmnb(args, world, rank, local):
             "unit": "TFLOP/s",
             "frac": achieved / peak.value,
             # dram__bytes_read.sum + dram__bytes_write.sum of one launch of this kernel on
-            # this workload (ncu --set full capture, k_pair_12windows_water_ligand_22840.md
-            # under profiles/): the working set stays in L2, DRAM is not the bound
+            # this workload (ncu capture, k_pair_12windows_water_ligand_22840.md under
+            # profiles/): the working set stays in L2, DRAM is not the bound
             "traffic": PAIR_LAUNCH_DRAM_BYTES,
             "traffic_unit": "bytes per launch",
             "kernel": "k_pair (full variant, 12 windows in one launch)",
             "pair_kernel_ms": float(np.mean(pair_ms)),
             "flops_per_launch": float(flops_launch),
-            "peak_source": "measured by tmnb_probe_fp32_peak (FMA chains) on this GPU",
+            "flops_per_pair": {"plain": FLOPS_PER_PAIR, "lj_extra": FLOPS_PER_LJ_PAIR,
+                               "lambda_dependent_extra": FLOPS_PER_ALCH_PAIR},
+            "peak_source": "FP32 FMA throughput measured by tmnb_probe_fp32_peak on this GPU",
+            "hbm": {"peak_gbs": hbm_peak, "peak_source": "hbm_gbs of MEASURED_PEAKS.json (copy bandwidth)",
+                    "stages": hbm},
         },
         "single_window_calls": {
             "value": seq_value,
@@ -478,6 +645,12 @@ def run_tmnb(args, world, rank, local):
             "pair_kernel_ms": float(np.mean(pair_ms_single)),
             "achieved_tflops": achieved_single,
             "note": "the same 12 windows as 12 tmnb_potential_execute_device calls",
+        },
+        "fp64": {
+            "value": value64,
+            "unit": "evals/s",
+            "ms_per_step": ms64 / max(3, args.steps // 4),
+            "note": "the same 12-window call through unbound_impl(np.float64) (FP64 pair arithmetic)",
         },
     }
     try:
@@ -504,6 +677,44 @@ def run_tmnb(args, world, rank, local):
     clk.__exit__()
     result["clocks"] = clk.summary()
     return result
+
+
+def summary(res):
+    """The headline numbers of every form, flat, for the end of the JSON line."""
+    def get(d, *ks):
+        for k in ks:
+            if not isinstance(d, dict) or k not in d:
+                return None
+            d = d[k]
+        return d
+
+    err = get(res, "config", "errors_vs_fp64_oracle") or {}
+    out = {
+        "evals_per_s_12_windows": res.get("value"),
+        "evals_per_s_single_calls": get(res, "single_window_calls", "value"),
+        "evals_per_s_fp64_12_windows": get(res, "fp64", "value"),
+        "e2e_evals_per_s": get(res, "e2e", "value"),
+        "md_ns_per_day": get(res, "md", "ns_per_day"),
+        "pair_kernel_fp32_frac": get(res, "roofline", "frac"),
+        "batch_eval_speedup_vs_512_plain": get(res, "batch", "speedup_vs_plain"),
+        "batch_md_speedup_vs_512_plain": get(res, "batch", "md", "speedup_vs_plain_evals"),
+        "serve_throughput_rps": get(res, "serve", "throughput_requests_per_s"),
+        "serve_eval_p50_ms": None,
+        "serve_eval_p99_ms": None,
+        "serve_md_p50_s": get(res, "serve", "latency_md", "p50_s"),
+        "serve_md_p99_s": get(res, "serve", "latency_md", "p99_s"),
+        "grad_ms": get(res, "grad", "ms_per_loss_gradient"),
+    }
+    p50 = get(res, "serve", "latency_eval", "p50_s")
+    p99 = get(res, "serve", "latency_eval", "p99_s")
+    out["serve_eval_p50_ms"] = None if p50 is None else p50 * 1e3
+    out["serve_eval_p99_ms"] = None if p99 is None else p99 * 1e3
+    for prec in ("f32", "f64"):
+        for k, v in (err.get(prec) or {}).items():
+            out[f"err_{prec}_{k}"] = v
+    for name, v in (get(res, "roofline", "hbm", "stages") or {}).items():
+        out[f"hbm_frac_{name.split(' ')[0]}"] = v["frac"]
+    return out
 
 
 MD_STEPS = 10000
@@ -746,24 +957,33 @@ def run_batch_form():
 
 
 SERVE_RATE = 200.0  # requests/s
-SERVE_SECONDS = 3.0  # arrival window of the bounded sample
+SERVE_SECONDS = 60.0  # arrival window of the serving stream
+SERVE_COMPARE_SECONDS = 3.0  # prefix of the stream served both ways for the sequential comparison
 SERVE_MD_STEPS = 1000
+SERVE_SIZE_LEVELS = 64  # distinct system sizes (log-spaced on [500, 50000]) the stream draws from
 
 
 def serve_workload(seed=SEED + 11, seconds=SERVE_SECONDS):
     """Poisson arrivals at 200/s; 70 % single evaluations, 30 % 1,000-step
-    Langevin segments; sizes log-uniform on [500, 50,000] atoms; lambda U(0, 1)."""
+    Langevin segments; sizes log-uniform on [500, 50,000] atoms (drawn from 64
+    log-spaced levels, so that the stream's systems are built once each);
+    lambda U(0, 1)."""
     from timemachine_b200 import testsystems
     from timemachine_b200.serve import Request
 
     rng = np.random.default_rng(seed)
+    levels = np.exp(np.linspace(np.log(500), np.log(50000), SERVE_SIZE_LEVELS)).astype(int)
+    built = {}
     t, reqs = 0.0, []
     while True:
         t += rng.exponential(1.0 / SERVE_RATE)
         if t > seconds:
             break
         n = int(np.exp(rng.uniform(np.log(500), np.log(50000))))
-        s = testsystems.system_of_size(n, seed=int(rng.integers(1 << 30)))
+        n = int(levels[np.argmin(np.abs(np.log(levels) - np.log(n)))])
+        if n not in built:
+            built[n] = testsystems.system_of_size(n, seed=int(rng.integers(1 << 30)))
+        s = built[n]
         kind = "md" if rng.uniform() < 0.3 else "eval"
         reqs.append(
             Request(
@@ -777,39 +997,56 @@ def serve_workload(seed=SEED + 11, seconds=SERVE_SECONDS):
 
 
 def run_serve_form():
-    """Serving form: the request stream through the continuous-batching loop,
-    and the same stream through sequential plain calls on the same GPU."""
-    from timemachine_b200.serve import Server, latency_stats, run_sequential
-
+    """Serving form: the 60 s request stream of the serving workload through
+    the continuous-batching server; and its first 3 s both through the server
+    and through sequential plain calls on the same GPU (the comparison)."""
     import dataclasses
 
+    from timemachine_b200.serve import Server, latency_stats, run_sequential
+
     reqs = serve_workload()
-    fresh = [dataclasses.replace(r) for r in reqs]  # same stream, unserved, for the sequential run
+    md_atom_steps = sum(r.system.N * r.n_steps for r in reqs if r.kind == "md")
     server = Server(hbm_budget_bytes=150e9, md_chunk=50)
     t0 = time.perf_counter()
     done = server.run(reqs)
     wall = time.perf_counter() - t0
-    stats = latency_stats(done)
     evals = [r for r in done if r.kind == "eval"]
     mds = [r for r in done if r.kind == "md"]
+    # the comparison: the first seconds of the same stream, served both ways
+    prefix = [r for r in serve_workload(seconds=SERVE_COMPARE_SECONDS)]
+    fresh = [dataclasses.replace(r) for r in prefix]
+    s2 = Server(hbm_budget_bytes=150e9, md_chunk=50)
+    t1 = time.perf_counter()
+    done2 = s2.run(prefix)
+    wall2 = time.perf_counter() - t1
     seq = run_sequential(fresh)
     seq_wall = max(r.finished for r in seq) - min(r.arrival for r in seq)
-    seq_stats = latency_stats(seq)
     return {
         "workload": f"{len(reqs)} requests over {SERVE_SECONDS:.0f} s of Poisson arrivals at {SERVE_RATE:.0f}/s "
         f"({len(evals)} evaluations, {len(mds)} x {SERVE_MD_STEPS}-step MD segments), sizes log-uniform on "
-        "[500, 50000] atoms, lambda U(0,1), 150 GB HBM budget",
-        "latency": stats,
+        "[500, 50000] atoms (64 levels), lambda U(0,1), 150 GB HBM budget",
+        "latency": latency_stats(done),
         "latency_eval": latency_stats(evals) if evals else None,
         "latency_md": latency_stats(mds) if mds else None,
         "throughput_requests_per_s": len(done) / wall,
         "wall_s": wall,
-        "iterations": server.iterations,
+        "offered_requests_per_s": len(reqs) / SERVE_SECONDS,
+        "offered_md_atom_steps_per_s": md_atom_steps / SERVE_SECONDS,
+        "served_md_atom_steps_per_s": md_atom_steps / wall,
+        "capacity_note": "the stream offers more MD work than one B200 serves in 60 s when served_md_atom_steps_per_s "
+        "< offered_md_atom_steps_per_s; the backlog then sets the MD latencies, not the loop",
+        "eval_launches": server.ev.launched,
+        "md_launches": server.md.launched,
         "peak_device_bytes": server.peak_bytes,
-        "sequential_plain": {
-            "latency": seq_stats,
-            "throughput_requests_per_s": len(seq) / seq_wall,
-            "wall_s": seq_wall,
+        "compare_prefix": {
+            "requests": len(prefix),
+            "seconds_of_arrivals": SERVE_COMPARE_SECONDS,
+            "server": {"latency_eval": latency_stats([r for r in done2 if r.kind == "eval"]),
+                       "latency_md": latency_stats([r for r in done2 if r.kind == "md"]),
+                       "throughput_requests_per_s": len(done2) / wall2, "wall_s": wall2},
+            "sequential_plain": {"latency_eval": latency_stats([r for r in seq if r.kind == "eval"]),
+                                 "latency_md": latency_stats([r for r in seq if r.kind == "md"]),
+                                 "throughput_requests_per_s": len(seq) / seq_wall, "wall_s": seq_wall},
         },
         "timing": "host wall clock from each request's arrival to its result on the host (D2H included)",
     }
@@ -1107,6 +1344,8 @@ def main():
                 "sample": "2 single-window evaluations of the 22,840-atom box by the FP64 oracle (all host threads)",
             }
     if rank == 0 and res is not None:
+        if args.impl != "reference":
+            res["summary"] = summary(res)  # last key: the headline numbers of every form
         print(json.dumps(res))
     if world > 1:
         import torch.distributed as dist

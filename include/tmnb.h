@@ -298,9 +298,14 @@ tmnb_status tmnb_potential_copy_nblist(
     tmnb_potential *pot, void *stream, unsigned *perm, int *row_block_ntiles, unsigned *tile_cols);
 
 /* Instrumentation (no reference counterpart): CUDA events around every
- * pair-kernel launch on the launching stream, and the duration of the last
- * one (synchronises on its end event). */
+ * stage of a call on the launching stream, and the duration of the stage's
+ * last launch (synchronises on its end event). Stages: */
+#define TMNB_STAGE_PREPARE 0  /* rebuild check, box checks, staging (k_check_prepare) */
+#define TMNB_STAGE_REBUILD 1  /* neighbour-list rebuild chain (returns at once when none is due) */
+#define TMNB_STAGE_PAIR 2     /* pair kernel */
+#define TMNB_STAGE_FINALIZE 3 /* scatter into the caller's outputs and accumulator reset */
 tmnb_status tmnb_potential_enable_timing(tmnb_potential *pot, int on);
+tmnb_status tmnb_potential_last_stage_ms(tmnb_potential *pot, int stage, float *ms);
 tmnb_status tmnb_potential_last_pair_kernel_ms(tmnb_potential *pot, float *ms);
 
 /* Measured FP32 FMA throughput of the current device in TFLOP/s (the

@@ -126,6 +126,8 @@ def _declare(lib):
     lib.tmnb_potential_copy_nblist.restype = ctypes.c_int
     lib.tmnb_potential_enable_timing.argtypes = [vp, i]
     lib.tmnb_potential_last_pair_kernel_ms.argtypes = [vp, ctypes.POINTER(ctypes.c_float)]
+    lib.tmnb_potential_last_stage_ms.argtypes = [vp, i, ctypes.POINTER(ctypes.c_float)]
+    lib.tmnb_potential_last_stage_ms.restype = ctypes.c_int
     lib.tmnb_probe_fp32_peak.argtypes = [ctypes.POINTER(ctypes.c_double)]
     ull = ctypes.c_ulonglong
     lib.tmnb_context_create.argtypes = [i, vp, vp, vp, d, d, vp, vp, ull, i, vp, vp, vp, ctypes.POINTER(vp)]

@@ -575,10 +575,55 @@ struct BatchSystem {
     unsigned long long seed;
 };
 
+// A replica's device arena, allocated and freed in stream order on the
+// engine's stream (cudaMallocAsync / cudaFreeAsync from the device's default
+// memory pool). Unlike cudaFree, releasing it does not wait for the whole
+// device, so removing a finished replica does not stall on work that another
+// engine has in flight.
+struct StreamArena {
+    unsigned char *p = nullptr;
+    size_t n = 0;
+    cudaStream_t stream = nullptr;
+    StreamArena() = default;
+    StreamArena(const StreamArena &) = delete;
+    StreamArena &operator=(const StreamArena &) = delete;
+    ~StreamArena() { release(); }
+    void release() {
+        if (p) {
+            cudaFreeAsync(p, stream);
+        }
+        p = nullptr;
+        n = 0;
+    }
+    void alloc(size_t count, cudaStream_t s) {
+        release();
+        stream = s;
+        CK(cudaMallocAsync(reinterpret_cast<void **>(&p), count, s));
+        n = count;
+    }
+};
+
+// Host-to-device copy into a device buffer that grows by doubling, on `s`
+// (a buffer only reallocates, with its device-wide cudaFree, when it grows).
+template <typename T> void upload_on(DevBuf<T> &b, const T *h, size_t n, cudaStream_t s) {
+    if (b.n < n) {
+        b.alloc(std::max(n, 2 * b.n));
+    }
+    CK(cudaMemcpyAsync(b.p, h, n * sizeof(T), cudaMemcpyHostToDevice, s));
+}
+
 class BatchEngine {
   public:
     BatchEngine() {
         CK(cudaStreamCreateWithFlags(&stream_, cudaStreamNonBlocking));
+        // keep freed arenas in the pool for reuse instead of returning them
+        // to the driver at every synchronisation
+        int dev = 0;
+        CK(cudaGetDevice(&dev));
+        cudaMemPool_t pool;
+        CK(cudaDeviceGetDefaultMemPool(&pool, dev));
+        unsigned long long keep = ~0ULL;
+        CK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
         BPairTable<0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 14, 15>::fill(pair_kernels_);
         counter_.alloc(1);
     }
@@ -756,7 +801,8 @@ class BatchEngine {
         default:
             throw Error(TMNB_ERR_INVALID_ARGUMENT, "unknown state selector");
         }
-        CK(cudaMemcpy(out, src, bytes, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpyAsync(out, src, bytes, cudaMemcpyDeviceToHost, stream_));
+        CK(cudaStreamSynchronize(stream_));
     }
 
     // Overwrites replica `id`'s coordinates (0), velocities (1) or box (2).
@@ -769,7 +815,8 @@ class BatchEngine {
         const Rep &r = s.rep;
         const size_t n = which == 2 ? 9 : 3 * (size_t)r.N;
         double *dst = which == 0 ? r.x : (which == 1 ? r.v : r.box);
-        CK(cudaMemcpy(dst, in, n * 8, cudaMemcpyHostToDevice));
+        CK(cudaMemcpyAsync(dst, in, n * 8, cudaMemcpyHostToDevice, stream_));
+        CK(cudaStreamSynchronize(stream_));
     }
 
     // Sticky device error of replica `id` (0: none); cleared when read.
@@ -777,10 +824,12 @@ class BatchEngine {
         Slot &s = slot(id);
         CK(cudaStreamSynchronize(stream_));
         int e = 0;
-        CK(cudaMemcpy(&e, &s.rep.state->error, sizeof(int), cudaMemcpyDeviceToHost));
+        CK(cudaMemcpyAsync(&e, &s.rep.state->error, sizeof(int), cudaMemcpyDeviceToHost, stream_));
+        CK(cudaStreamSynchronize(stream_));
         if (e) {
             const int z = 0;
-            CK(cudaMemcpy(&s.rep.state->error, &z, sizeof(int), cudaMemcpyHostToDevice));
+            CK(cudaMemcpyAsync(&s.rep.state->error, &z, sizeof(int), cudaMemcpyHostToDevice, stream_));
+            CK(cudaStreamSynchronize(stream_));
         }
         return e;
     }
@@ -789,7 +838,8 @@ class BatchEngine {
         Slot &s = slot(id);
         CK(cudaStreamSynchronize(stream_));
         DevState st;
-        CK(cudaMemcpy(&st, s.rep.state, sizeof(st), cudaMemcpyDeviceToHost));
+        CK(cudaMemcpyAsync(&st, s.rep.state, sizeof(st), cudaMemcpyDeviceToHost, stream_));
+        CK(cudaStreamSynchronize(stream_));
         if (tiles) {
             *tiles = (int)st.total_tiles;
         }
@@ -817,7 +867,7 @@ class BatchEngine {
     struct Slot {
         BatchSystem sys; // pointers into the host copies below
         bool has_md = false;
-        DevBuf<unsigned char> arena;
+        StreamArena arena;
         Rep rep;
         std::vector<double> h_x, h_v, h_box, h_p, h_scales, h_bparams, h_aparams, h_cbs, h_ccs;
         std::vector<int> h_plane, h_offset, h_pairs, h_bonds, h_angles;
@@ -914,8 +964,8 @@ class BatchEngine {
 
     void allocate(Slot &slot, const BatchSystem &s) {
         const Layout L = layout(s.N, s.M, s.B, s.A);
-        slot.arena.alloc(L.total);
-        CK(cudaMemset(slot.arena.p, 0, L.total));
+        slot.arena.alloc(L.total, stream_);
+        CK(cudaMemsetAsync(slot.arena.p, 0, L.total, stream_));
         unsigned char *b = slot.arena.p;
         Rep &r = slot.rep;
         r.N = s.N;
@@ -972,29 +1022,29 @@ class BatchEngine {
         r.md_step = reinterpret_cast<unsigned long long *>(b + L.md_step);
         r.state = reinterpret_cast<DevState *>(b + L.state);
         const size_t N = s.N;
-        CK(cudaMemcpy(r.x, s.x, 24 * N, cudaMemcpyHostToDevice));
+        CK(cudaMemcpyAsync(r.x, s.x, 24 * N, cudaMemcpyHostToDevice, stream_));
         if (s.v) {
-            CK(cudaMemcpy(r.v, s.v, 24 * N, cudaMemcpyHostToDevice));
+            CK(cudaMemcpyAsync(r.v, s.v, 24 * N, cudaMemcpyHostToDevice, stream_));
         }
-        CK(cudaMemcpy(r.box, s.box, 72, cudaMemcpyHostToDevice));
-        CK(cudaMemcpy((void *)r.p, s.params, 24 * N, cudaMemcpyHostToDevice));
-        CK(cudaMemcpy((void *)r.plane, s.plane, 4 * N, cudaMemcpyHostToDevice));
-        CK(cudaMemcpy((void *)r.offset, s.offset, 4 * N, cudaMemcpyHostToDevice));
+        CK(cudaMemcpyAsync(r.box, s.box, 72, cudaMemcpyHostToDevice, stream_));
+        CK(cudaMemcpyAsync((void *)r.p, s.params, 24 * N, cudaMemcpyHostToDevice, stream_));
+        CK(cudaMemcpyAsync((void *)r.plane, s.plane, 4 * N, cudaMemcpyHostToDevice, stream_));
+        CK(cudaMemcpyAsync((void *)r.offset, s.offset, 4 * N, cudaMemcpyHostToDevice, stream_));
         if (s.M > 0) {
-            CK(cudaMemcpy((void *)r.pair_idxs, s.pair_idxs, 8 * (size_t)s.M, cudaMemcpyHostToDevice));
-            CK(cudaMemcpy((void *)r.scales, s.scales, 16 * (size_t)s.M, cudaMemcpyHostToDevice));
+            CK(cudaMemcpyAsync((void *)r.pair_idxs, s.pair_idxs, 8 * (size_t)s.M, cudaMemcpyHostToDevice, stream_));
+            CK(cudaMemcpyAsync((void *)r.scales, s.scales, 16 * (size_t)s.M, cudaMemcpyHostToDevice, stream_));
         }
         if (s.B > 0) {
-            CK(cudaMemcpy((void *)r.bond_idxs, s.bond_idxs, 8 * (size_t)s.B, cudaMemcpyHostToDevice));
-            CK(cudaMemcpy((void *)r.bond_params, s.bond_params, 16 * (size_t)s.B, cudaMemcpyHostToDevice));
+            CK(cudaMemcpyAsync((void *)r.bond_idxs, s.bond_idxs, 8 * (size_t)s.B, cudaMemcpyHostToDevice, stream_));
+            CK(cudaMemcpyAsync((void *)r.bond_params, s.bond_params, 16 * (size_t)s.B, cudaMemcpyHostToDevice, stream_));
         }
         if (s.A > 0) {
-            CK(cudaMemcpy((void *)r.angle_idxs, s.angle_idxs, 12 * (size_t)s.A, cudaMemcpyHostToDevice));
-            CK(cudaMemcpy((void *)r.angle_params, s.angle_params, 16 * (size_t)s.A, cudaMemcpyHostToDevice));
+            CK(cudaMemcpyAsync((void *)r.angle_idxs, s.angle_idxs, 12 * (size_t)s.A, cudaMemcpyHostToDevice, stream_));
+            CK(cudaMemcpyAsync((void *)r.angle_params, s.angle_params, 16 * (size_t)s.A, cudaMemcpyHostToDevice, stream_));
         }
         if (s.cbs && s.ccs) {
-            CK(cudaMemcpy((void *)r.cbs, s.cbs, 8 * N, cudaMemcpyHostToDevice));
-            CK(cudaMemcpy((void *)r.ccs, s.ccs, 8 * N, cudaMemcpyHostToDevice));
+            CK(cudaMemcpyAsync((void *)r.cbs, s.cbs, 8 * N, cudaMemcpyHostToDevice, stream_));
+            CK(cudaMemcpyAsync((void *)r.ccs, s.ccs, 8 * N, cudaMemcpyHostToDevice, stream_));
         }
         // identity slot order until the first (forced) rebuild
         std::vector<unsigned> perm(N);
@@ -1003,11 +1053,13 @@ class BatchEngine {
             perm[k] = (unsigned)k;
             slot_of[k] = (int)k;
         }
-        CK(cudaMemcpy(r.perm, perm.data(), 4 * N, cudaMemcpyHostToDevice));
-        CK(cudaMemcpy(r.slot_of, slot_of.data(), 4 * N, cudaMemcpyHostToDevice));
+        CK(cudaMemcpyAsync(r.perm, perm.data(), 4 * N, cudaMemcpyHostToDevice, stream_));
+        CK(cudaMemcpyAsync(r.slot_of, slot_of.data(), 4 * N, cudaMemcpyHostToDevice, stream_));
         DevState st{};
         st.rebuild = 1;
-        CK(cudaMemcpy(r.state, &st, sizeof(st), cudaMemcpyHostToDevice));
+        CK(cudaMemcpyAsync(r.state, &st, sizeof(st), cudaMemcpyHostToDevice, stream_));
+        // the host staging (perm, slot_of, st) is local: finish the copies here
+        CK(cudaStreamSynchronize(stream_));
     }
 
     // New tuning: re-lay the replica out (arena sizes depend on the chunk and
@@ -1017,16 +1069,18 @@ class BatchEngine {
         const int N = slot.rep.N;
         std::vector<double> x(3 * (size_t)N), v(3 * (size_t)N), box(9);
         unsigned long long step = 0;
-        CK(cudaMemcpy(x.data(), slot.rep.x, 24 * (size_t)N, cudaMemcpyDeviceToHost));
-        CK(cudaMemcpy(v.data(), slot.rep.v, 24 * (size_t)N, cudaMemcpyDeviceToHost));
-        CK(cudaMemcpy(box.data(), slot.rep.box, 72, cudaMemcpyDeviceToHost));
-        CK(cudaMemcpy(&step, slot.rep.md_step, 8, cudaMemcpyDeviceToHost));
+        CK(cudaMemcpyAsync(x.data(), slot.rep.x, 24 * (size_t)N, cudaMemcpyDeviceToHost, stream_));
+        CK(cudaMemcpyAsync(v.data(), slot.rep.v, 24 * (size_t)N, cudaMemcpyDeviceToHost, stream_));
+        CK(cudaMemcpyAsync(box.data(), slot.rep.box, 72, cudaMemcpyDeviceToHost, stream_));
+        CK(cudaMemcpyAsync(&step, slot.rep.md_step, 8, cudaMemcpyDeviceToHost, stream_));
+        CK(cudaStreamSynchronize(stream_));
         BatchSystem s = slot.sys;
         s.x = x.data();
         s.v = v.data();
         s.box = box.data();
         allocate(slot, s);
-        CK(cudaMemcpy(slot.rep.md_step, &step, 8, cudaMemcpyHostToDevice));
+        CK(cudaMemcpyAsync(slot.rep.md_step, &step, 8, cudaMemcpyHostToDevice, stream_));
+        CK(cudaStreamSynchronize(stream_));
     }
 
     Slot &slot(int id) {
@@ -1073,17 +1127,18 @@ class BatchEngine {
         n_bmap_ = (int)bmap.size();
         n_amap_ = (int)amap.size();
         if (R_ > 0) {
-            table_.upload(table.data(), table.size());
-            ablk_.upload(ablk.data(), ablk.size());
-            rbmap_.upload(rbmap.data(), rbmap.size());
-            gmap_.upload(gmap.data(), gmap.size());
+            upload_on(table_, table.data(), table.size(), stream_);
+            upload_on(ablk_, ablk.data(), ablk.size(), stream_);
+            upload_on(rbmap_, rbmap.data(), rbmap.size(), stream_);
+            upload_on(gmap_, gmap.data(), gmap.size(), stream_);
             if (n_bmap_) {
-                bmap_.upload(bmap.data(), bmap.size());
+                upload_on(bmap_, bmap.data(), bmap.size(), stream_);
             }
             if (n_amap_) {
-                amap_.upload(amap.data(), amap.size());
+                upload_on(amap_, amap.data(), amap.size(), stream_);
             }
-            prefix_.alloc(R_ + 1);
+            prefix_.ensure(R_ + 1);
+            CK(cudaStreamSynchronize(stream_)); // the host tables above are local
         }
         table_dirty_ = false;
     }

@@ -208,33 +208,60 @@ class NonbondedPotential : public PotentialBase {
 
     ~NonbondedPotential() {
         if (timing_) {
-            cudaEventDestroy(ev_pair_[0]);
-            cudaEventDestroy(ev_pair_[1]);
+            for (auto &e : ev_) {
+                cudaEventDestroy(e[0]);
+                cudaEventDestroy(e[1]);
+            }
         }
     }
 
-    // CUDA events around every pair-kernel launch (on the launching stream).
+    // CUDA events around every stage of a call (on the launching stream):
+    // TMNB_STAGE_PREPARE (k_check_prepare), _REBUILD (the five rebuild-chain
+    // kernels, which return at once when no rebuild is due), _PAIR (k_pair),
+    // _FINALIZE (k_finalize and the accumulator memset).
     void enable_timing(bool on) {
         if (on && !timing_) {
-            CK(cudaEventCreate(&ev_pair_[0]));
-            CK(cudaEventCreate(&ev_pair_[1]));
+            for (auto &e : ev_) {
+                CK(cudaEventCreate(&e[0]));
+                CK(cudaEventCreate(&e[1]));
+            }
         } else if (!on && timing_) {
-            CK(cudaEventDestroy(ev_pair_[0]));
-            CK(cudaEventDestroy(ev_pair_[1]));
+            for (auto &e : ev_) {
+                CK(cudaEventDestroy(e[0]));
+                CK(cudaEventDestroy(e[1]));
+            }
         }
         timing_ = on;
-        pair_timed_ = false;
+        for (bool &t : timed_) {
+            t = false;
+        }
     }
 
-    float last_pair_ms() {
-        if (!timing_ || !pair_timed_) {
-            throw Error(TMNB_ERR_INVALID_ARGUMENT, "no timed pair-kernel launch (enable timing first)");
+    void stage_begin(int stage, cudaStream_t stream) {
+        if (timing_) {
+            CK(cudaEventRecord(ev_[stage][0], stream));
         }
-        CK(cudaEventSynchronize(ev_pair_[1]));
+    }
+    void stage_end(int stage, cudaStream_t stream) {
+        if (timing_) {
+            CK(cudaEventRecord(ev_[stage][1], stream));
+            timed_[stage] = true;
+        }
+    }
+
+    float last_stage_ms(int stage) {
+        if (stage < 0 || stage >= N_STAGES) {
+            throw Error(TMNB_ERR_INVALID_ARGUMENT, "unknown stage");
+        }
+        if (!timing_ || !timed_[stage]) {
+            throw Error(TMNB_ERR_INVALID_ARGUMENT, "no timed launch of this stage (enable timing first)");
+        }
+        CK(cudaEventSynchronize(ev_[stage][1]));
         float ms = 0.f;
-        CK(cudaEventElapsedTime(&ms, ev_pair_[0], ev_pair_[1]));
+        CK(cudaEventElapsedTime(&ms, ev_[stage][0], ev_[stage][1]));
         return ms;
     }
+    float last_pair_ms() { return last_stage_ms(TMNB_STAGE_PAIR); }
 
     static int current_device() {
         int d = 0;
@@ -478,12 +505,16 @@ class NonbondedPotential : public PotentialBase {
 
         const int tpb = 256;
         const int sgrid = std::max(1, std::min((S_ + tpb - 1) / tpb, 8 * num_sms()));
+        stage_begin(TMNB_STAGE_PREPARE, stream);
         launch_dependent(
             k_check_prepare, dim3(sgrid), dim3(tpb), 0, stream, pa, (const unsigned *)perm_.p,
             (const double *)(has_nblist_ ? nb_x_.p : nullptr), (const double *)nb_box_.p, state_.p);
         CK(cudaPeekAtLastError());
+        stage_end(TMNB_STAGE_PREPARE, stream);
         if (has_nblist_) {
+            stage_begin(TMNB_STAGE_REBUILD, stream);
             record_rebuild_chain(d_x, d_box, pa, sgrid, tpb, stream, K);
+            stage_end(TMNB_STAGE_REBUILD, stream);
         }
 
         const int kidx = (d_du_dp ? 1 : 0) | (d_du_dl ? 2 : 0) | (d_du_dx ? 4 : 0) | (d_u ? 8 : 0);
@@ -528,15 +559,10 @@ class NonbondedPotential : public PotentialBase {
             const PairKernels &table = kernels_[row_table(rows_)];
             pair_kernel_t k = K > 1 ? table.multi[kidx] : table.single[kidx];
             const size_t smem = 0;
-            if (timing_) {
-                CK(cudaEventRecord(ev_pair_[0], stream));
-            }
+            stage_begin(TMNB_STAGE_PAIR, stream);
             launch_dependent(k, dim3(pair_grid(k, smem)), dim3(128), smem, stream, a);
             CK(cudaPeekAtLastError());
-            if (timing_) {
-                CK(cudaEventRecord(ev_pair_[1], stream));
-                pair_timed_ = true;
-            }
+            stage_end(TMNB_STAGE_PAIR, stream);
 
             FinalizeArgs fa;
             fa.N = N_;
@@ -564,6 +590,7 @@ class NonbondedPotential : public PotentialBase {
             fa.state = state_.p;
             const size_t fin_threads = (size_t)S_ * K;
             const int fgrid = (int)std::max<size_t>(1, std::min<size_t>((fin_threads + tpb - 1) / tpb, 16 * (size_t)num_sms()));
+            stage_begin(TMNB_STAGE_FINALIZE, stream);
             launch_dependent(k_finalize, dim3(fgrid), dim3(tpb), 0, stream, fa);
             CK(cudaPeekAtLastError());
             // Zero the accumulator blocks k_finalize read (one coalesced memset;
@@ -572,6 +599,7 @@ class NonbondedPotential : public PotentialBase {
             // arrays of the block are the only ones written.
             const size_t used = (kidx == 4 && K == 1) ? 3 * (size_t)S_ : acc_block_elems() * (K > 1 ? 1 + K : 1);
             CK(cudaMemsetAsync(acc_.p, 0, used * sizeof(unsigned long long), stream));
+            stage_end(TMNB_STAGE_FINALIZE, stream);
         }
     }
 
@@ -853,9 +881,10 @@ class NonbondedPotential : public PotentialBase {
     PairKernels kernels_[3] = {};
 
     // pair-kernel timing
+    static constexpr int N_STAGES = 4;
     bool timing_ = false;
-    bool pair_timed_ = false;
-    cudaEvent_t ev_pair_[2] = {nullptr, nullptr};
+    bool timed_[N_STAGES] = {};
+    cudaEvent_t ev_[N_STAGES][2] = {};
 
 };
 
@@ -1387,6 +1416,17 @@ tmnb_status tmnb_potential_last_pair_kernel_ms(tmnb_potential *pot, float *ms) {
         return TMNB_ERR_INVALID_ARGUMENT;
     }
     return tmb::guarded([&] { *ms = as_nb(pot)->last_pair_ms(); });
+}
+
+tmnb_status tmnb_potential_last_stage_ms(tmnb_potential *pot, int stage, float *ms) {
+    if (tmnb_status s = check_handle(pot)) {
+        return s;
+    }
+    if (!ms) {
+        tmb::g_last_error = "null argument";
+        return TMNB_ERR_INVALID_ARGUMENT;
+    }
+    return tmb::guarded([&] { *ms = as_nb(pot)->last_stage_ms(stage); });
 }
 
 tmnb_status tmnb_probe_fp32_peak(double *tflops) {

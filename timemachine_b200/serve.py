@@ -1,14 +1,23 @@
 """Serving loop: continuous batching of energy/force and short-MD requests.
 
-Requests of different atom counts arrive over time. The loop keeps each
-admitted request's coordinates, velocities, box and neighbour list resident
-on the device (one replica of a ReplicaBatch), admits waiting requests as
-device memory frees up (admission by HBM footprint against a budget), and
-serves every admitted request together: each loop iteration launches one
-batched evaluation of the waiting energy/force requests and one batched chunk
-of MD steps of the running segments, on two streams, so their work overlaps
-on the device. Requests that arrive while others are on the GPU join at the
-next iteration.
+Requests of different atom counts arrive over time. Each admitted request's
+coordinates, velocities, box and neighbour list stay resident on the device
+(one replica of a ReplicaBatch); admission is by HBM footprint against a
+budget. Two engines serve the two request kinds on their own CUDA streams:
+
+- the evaluation engine runs one batched evaluation of every evaluation
+  request admitted since its last batch;
+- the MD engine advances every running segment by chunks of Langevin steps
+  (one CUDA-graph-replayed chunk while its membership is unchanged).
+
+The loop never waits on the device. It polls a CUDA event per engine: when an
+engine's launch has completed it collects that engine's finished requests,
+admits the requests that arrived meanwhile (membership changes only while the
+engine is idle) and launches the engine again, so evaluations are answered as
+soon as their batch ends -- they do not wait for an MD chunk -- and the two
+engines' work overlaps on the device. Replica arenas are allocated and freed
+in stream order, so a finished request's release does not wait for the
+other engine.
 
 A request's result does not depend on what else is being served: each replica
 is an independent system with integer (fixed-point) accumulation, so it is
@@ -50,98 +59,168 @@ def _terms(system, name):
     return 0 if a is None else len(a)
 
 
-class Server:
-    def __init__(self, hbm_budget_bytes=150e9, md_chunk=50, tuning=None):
-        self.budget = float(hbm_budget_bytes)
-        self.md_chunk = int(md_chunk)
-        self.eval_engine = ReplicaBatch()
-        self.md_engine = ReplicaBatch()
+class _Engine:
+    """One ReplicaBatch with its stream, its in-flight launch and its requests."""
+
+    def __init__(self, tuning):
+        import torch
+
+        self.batch = ReplicaBatch()
         if tuning:
-            self.eval_engine.set_tuning(**tuning)
-            self.md_engine.set_tuning(**tuning)
-        self.waiting = []
-        self.active_eval = []
-        self.active_md = []
+            self.batch.set_tuning(**tuning)
+        self.stream = torch.cuda.ExternalStream(self.batch.stream)
+        self.event = None  # completion event of the launch in flight
+        self.running = []  # requests in the launch in flight (or resident between launches)
+        self.launched = 0
+
+    def idle(self):
+        return self.event is None or self.event.query()
+
+    def mark(self):
+        import torch
+
+        self.event = torch.cuda.Event()
+        self.event.record(self.stream)
+        self.launched += 1
+
+
+class Server:
+    """hbm_budget_bytes: device bytes all resident requests may hold.
+    md_budget_fraction: the share of it MD segments may hold, so that
+    evaluation requests always find room (they are short-lived).
+    md_max_atoms: resident MD atoms at most (FIFO admission beyond): an MD
+    chunk then takes bounded time, and under a backlog the earlier segments
+    finish first instead of all advancing together."""
+
+    def __init__(self, hbm_budget_bytes=150e9, md_chunk=50, tuning=None, md_graphs=True,
+                 md_budget_fraction=0.8, md_max_atoms=4_000_000):
+        self.budget = float(hbm_budget_bytes)
+        self.md_budget = self.budget * float(md_budget_fraction)
+        self.md_max_atoms = int(md_max_atoms)
+        self.md_chunk = int(md_chunk)
+        self.md_graphs = md_graphs
+        self.ev = _Engine(tuning)
+        self.md = _Engine(tuning)
+        self.waiting = []  # arrived or future requests, not yet admitted
         self.done = []
         self.iterations = 0
         self.peak_bytes = 0
+        self.md_chunk_steps = []  # steps of each MD launch
+
+    # kept for callers of the earlier interface
+    @property
+    def eval_engine(self):
+        return self.ev.batch
+
+    @property
+    def md_engine(self):
+        return self.md.batch
 
     def footprint(self, req):
         s = req.system
-        return self.eval_engine.footprint(
-            s.N, len(s.exclusion_idxs), _terms(s, "bond_idxs"), _terms(s, "angle_idxs")
-        )
+        return self.ev.batch.footprint(s.N, len(s.exclusion_idxs), _terms(s, "bond_idxs"), _terms(s, "angle_idxs"))
 
     def bytes_in_use(self):
-        return self.eval_engine.bytes_in_use() + self.md_engine.bytes_in_use()
+        return self.ev.batch.bytes_in_use() + self.md.batch.bytes_in_use()
 
     def submit(self, req):
         self.waiting.append(req)
 
-    def _admit(self, now):
-        """FIFO admission of arrived requests while the HBM budget allows."""
+    def _admit(self, kind, engine, now):
+        """FIFO admission of arrived requests of one kind into an idle engine
+        while the HBM budget allows (a request that does not fit blocks the
+        later ones of its kind, keeping arrival order). MD segments are held
+        to their share of the budget and to md_max_atoms resident atoms."""
         used = self.bytes_in_use()
-        keep = []
-        blocked = False
+        md_used = self.md.batch.bytes_in_use()
+        md_atoms = sum(r.system.N for r in self.md.running)
+        keep, blocked = [], False
         for req in self.waiting:
-            if blocked or req.arrival > now:
+            if req.kind != kind or blocked or req.arrival > now:
                 keep.append(req)
                 continue
             need = self.footprint(req)
-            if used + need > self.budget:
-                if need > self.budget:
-                    raise RuntimeError(f"request {req.rid} needs {need} bytes, above the HBM budget")
-                blocked = True  # keep arrival order
+            if need > self.budget:
+                raise RuntimeError(f"request {req.rid} needs {need} bytes, above the HBM budget")
+            over = used + need > self.budget
+            if kind == "md" and md_used > 0:  # an MD segment alone is always admissible
+                over = over or md_used + need > self.md_budget or md_atoms + req.system.N > self.md_max_atoms
+            if over:
+                blocked = True
                 keep.append(req)
                 continue
-            if req.kind == "eval":
-                req._replica = self.eval_engine.add(req.system, req.lam)
-                self.active_eval.append(req)
+            if kind == "md":
+                md_used += need
+                md_atoms += req.system.N
+            if kind == "eval":
+                req._replica = engine.batch.add(req.system, req.lam)
             else:
-                req._replica = self.md_engine.add(req.system, req.lam, v=req.v0, md=req.md, seed=req.seed)
-                self.active_md.append(req)
+                req._replica = engine.batch.add(req.system, req.lam, v=req.v0, md=req.md, seed=req.seed)
             req.admitted = time.perf_counter()
+            engine.running.append(req)
             used += need
         self.waiting = keep
         self.peak_bytes = max(self.peak_bytes, used)
 
-    def step(self):
-        """One loop iteration: admit, launch both engines, collect completions."""
-        self._admit(time.perf_counter())
-        evals = list(self.active_eval)
-        if evals:
-            self.eval_engine.evaluate()
-        n_md = 0
-        if self.active_md:
-            n_md = min(self.md_chunk, min(r.n_steps - r.steps_done for r in self.active_md))
-            self.md_engine.md(n_md, chunk=n_md, use_graph=False)
-        if evals:
-            self.eval_engine.synchronize()
-            for req in evals:
-                req.result = self.eval_engine.result_fixed(req._replica)
+    def _service_eval(self, now):
+        e = self.ev
+        if not e.idle():
+            return False
+        if e.running:  # the batch in flight has finished: answer it
+            for req in e.running:
+                req.result = e.batch.result_fixed(req._replica)
                 req.finished = time.perf_counter()
-                self.eval_engine.remove(req._replica)
+                e.batch.remove(req._replica)
                 self.done.append(req)
-            self.active_eval = []
-        if n_md:
-            self.md_engine.synchronize()
+            e.running = []
+            e.event = None
+        self._admit("eval", e, now)
+        if e.running:
+            e.batch.evaluate()
+            e.mark()
+            return True
+        return False
+
+    def _service_md(self, now):
+        e = self.md
+        if not e.idle():
+            return False
+        if e.event is not None:  # the chunk in flight has finished
             still = []
-            for req in self.active_md:
-                req.steps_done += n_md
+            for req in e.running:
+                req.steps_done += e.last_chunk
                 if req.steps_done >= req.n_steps:
-                    req.result = (self.md_engine.get_x(req._replica), self.md_engine.get_v(req._replica))
+                    req.result = (e.batch.get_x(req._replica), e.batch.get_v(req._replica))
                     req.finished = time.perf_counter()
-                    self.md_engine.remove(req._replica)
+                    e.batch.remove(req._replica)
                     self.done.append(req)
                 else:
                     still.append(req)
-            self.active_md = still
+            e.running = still
+            e.event = None
+        self._admit("md", e, now)
+        if e.running:
+            n = min(self.md_chunk, min(r.n_steps - r.steps_done for r in e.running))
+            e.batch.md(n, chunk=n, use_graph=self.md_graphs)
+            e.last_chunk = n
+            self.md_chunk_steps.append(n)
+            e.mark()
+            return True
+        return False
+
+    def step(self):
+        """One pass of the loop: service each idle engine (collect, admit,
+        launch). Returns True when something was launched."""
+        now = time.perf_counter()
+        a = self._service_eval(now)
+        b = self._service_md(now)
         self.iterations += 1
+        return a or b
 
     def busy(self):
-        return bool(self.waiting or self.active_eval or self.active_md)
+        return bool(self.waiting or self.ev.running or self.md.running)
 
-    def run(self, requests, t0=None):
+    def run(self, requests, t0=None, poll_s=2e-4):
         """Serves `requests` (arrival times in seconds relative to t0, default
         now) until all are done; returns them in completion order. A request's
         latency is finished - arrival (both absolute after this call)."""
@@ -150,13 +229,12 @@ class Server:
             r.arrival = t0 + r.arrival
             self.submit(r)
         while self.busy():
-            if not (self.active_eval or self.active_md):
+            launched = self.step()
+            if not launched:
+                # nothing to do until a launch completes or a request arrives
                 now = time.perf_counter()
-                nxt = min(r.arrival for r in self.waiting)
-                if nxt > now:
-                    time.sleep(min(nxt - now, 0.01))
-                    continue
-            self.step()
+                nxt = min((r.arrival for r in self.waiting), default=now + poll_s)
+                time.sleep(max(0.0, min(poll_s, nxt - now)))
         return self.done
 
 
