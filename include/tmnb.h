@@ -391,6 +391,17 @@ tmnb_status tmnb_context_set_x(tmnb_context *ctx, const double *in);
 tmnb_status tmnb_context_set_v(tmnb_context *ctx, const double *in);
 tmnb_status tmnb_context_set_box(tmnb_context *ctx, const double *in);
 tmnb_status tmnb_context_barostat_stats(tmnb_context *ctx, int *accepted, int *attempted, double *volume_scale);
+/* MonteCarloBarostat::set_pressure / set_interval
+ * (timemachine/cpp/src/barostat.cu:386-397, bound in wrap_kernels.cpp):
+ * the pressure in bar; a new interval restarts the move counter. */
+tmnb_status tmnb_context_barostat_set_pressure(tmnb_context *ctx, double pressure_bar);
+tmnb_status tmnb_context_barostat_set_interval(tmnb_context *ctx, int interval);
+/* The last barostat move (inspection, no reference counterpart):
+ * values[8] = rand0, rand1, proposal volume scale, volume delta, length
+ * scale, accepted (1/0), volume scale after adaptation, pressure
+ * (kJ/mol/nm^3); energies[2] = fixed-point total energy before the move and
+ * at the trial coordinates. */
+tmnb_status tmnb_context_barostat_last_move(tmnb_context *ctx, double *values, unsigned long long *energies);
 tmnb_status tmnb_context_destroy(tmnb_context *ctx);
 
 /*

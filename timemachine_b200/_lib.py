@@ -137,6 +137,9 @@ def _declare(lib):
     for nm in ["get_x", "get_v", "get_box", "set_x", "set_v", "set_box"]:
         getattr(lib, "tmnb_context_" + nm).argtypes = [vp, vp]
     lib.tmnb_context_barostat_stats.argtypes = [vp, c_int_p, c_int_p, c_double_p]
+    lib.tmnb_context_barostat_set_pressure.argtypes = [vp, d]
+    lib.tmnb_context_barostat_set_interval.argtypes = [vp, i]
+    lib.tmnb_context_barostat_last_move.argtypes = [vp, vp, vp]
     lib.tmnb_context_destroy.argtypes = [vp]
     lib.tmnb_harmonic_bond_create.argtypes = [i, i, vp, vp, vp, ctypes.POINTER(vp)]
     lib.tmnb_harmonic_angle_create.argtypes = [i, i, vp, vp, vp, ctypes.POINTER(vp)]

@@ -43,6 +43,10 @@ struct MDState {
     int accepted;
     int total_accepted;
     int total_attempted;
+    // the last move, as proposed and decided (inspection)
+    double proposal_scale;                // volume scale the proposal used
+    unsigned long long last_u_before;     // fixed-point total energy before the move
+    unsigned long long last_u_after;      // and at the trial coordinates
 };
 
 __global__ void k_langevin(
@@ -147,6 +151,7 @@ __global__ void k_baro_propose(
         if (st->volume_scale == 0) {
             st->volume_scale = 0.01 * volume;
         }
+        st->proposal_scale = st->volume_scale;
         const double delta_volume = st->volume_scale * 2 * (st->rand0 - 0.5);
         const double new_volume = volume + delta_volume;
         st->volume_delta = delta_volume;
@@ -227,6 +232,8 @@ __global__ void k_baro_decide(
         init_u += part0[w];
         final_u += part1[w];
     }
+    st->last_u_before = init_u;
+    st->last_u_after = final_u;
     const double volume = box[0] * box[4] * box[8];
     const double new_volume = volume + st->volume_delta;
     const double energy_delta = static_cast<double>(static_cast<long long>(final_u - init_u)) / FX_EXPONENT;
@@ -620,6 +627,47 @@ class Context {
         CK(cudaMemcpy(b.p, in, b.n * sizeof(double), cudaMemcpyHostToDevice));
     }
 
+    // MonteCarloBarostat::set_pressure (timemachine/cpp/src/barostat.cu:386-389)
+    void set_barostat_pressure(double pressure_bar) {
+        if (!has_baro_) {
+            throw Error(TMNB_ERR_INVALID_ARGUMENT, "no barostat");
+        }
+        baro_pressure_ = pressure_bar * AVOGADRO * 1e-25;
+        invalidate_graphs(); // the captured moves hold the old pressure
+    }
+
+    // MonteCarloBarostat::set_interval: the move counter restarts
+    // (timemachine/cpp/src/barostat.cu:391-397)
+    void set_barostat_interval(int interval) {
+        if (!has_baro_) {
+            throw Error(TMNB_ERR_INVALID_ARGUMENT, "no barostat");
+        }
+        if (interval <= 0) {
+            throw Error(TMNB_ERR_INVALID_ARGUMENT, "Barostat interval must be greater than 0");
+        }
+        baro_interval_ = interval;
+        baro_step_ = 0;
+    }
+
+    // The last move: rand0, rand1, the proposal's volume scale, volume delta,
+    // length scale, energies before and after (fixed point, as int64 bit
+    // patterns), accepted (1/0), and the volume scale after the adaptation.
+    void barostat_last_move(double *out, unsigned long long *u) {
+        CK(cudaStreamSynchronize(stream_));
+        MDState st;
+        CK(cudaMemcpy(&st, st_.p, sizeof(st), cudaMemcpyDeviceToHost));
+        out[0] = st.rand0;
+        out[1] = st.rand1;
+        out[2] = st.proposal_scale;
+        out[3] = st.volume_delta;
+        out[4] = st.length_scale;
+        out[5] = st.accepted;
+        out[6] = st.volume_scale;
+        out[7] = baro_pressure_;
+        u[0] = st.last_u_before;
+        u[1] = st.last_u_after;
+    }
+
     void barostat_stats(int *accepted, int *attempted, double *volume_scale) {
         CK(cudaStreamSynchronize(stream_));
         MDState s;
@@ -861,6 +909,31 @@ tmnb_status tmnb_context_barostat_stats(tmnb_context *ctx, int *accepted, int *a
         return s;
     }
     return tmb::guarded([&] { ctx->impl->barostat_stats(accepted, attempted, volume_scale); });
+}
+
+tmnb_status tmnb_context_barostat_set_pressure(tmnb_context *ctx, double pressure_bar) {
+    if (tmnb_status s = check_ctx(ctx)) {
+        return s;
+    }
+    return tmb::guarded([&] { ctx->impl->set_barostat_pressure(pressure_bar); });
+}
+
+tmnb_status tmnb_context_barostat_set_interval(tmnb_context *ctx, int interval) {
+    if (tmnb_status s = check_ctx(ctx)) {
+        return s;
+    }
+    return tmb::guarded([&] { ctx->impl->set_barostat_interval(interval); });
+}
+
+tmnb_status tmnb_context_barostat_last_move(tmnb_context *ctx, double *values, unsigned long long *energies) {
+    if (tmnb_status s = check_ctx(ctx)) {
+        return s;
+    }
+    if (!values || !energies) {
+        tmb::g_last_error = "null argument";
+        return TMNB_ERR_INVALID_ARGUMENT;
+    }
+    return tmb::guarded([&] { ctx->impl->barostat_last_move(values, energies); });
 }
 
 tmnb_status tmnb_context_destroy(tmnb_context *ctx) {

@@ -90,67 +90,89 @@ struct PrepareArgs {
     SlotArrays slots;
 };
 
-// Stage one atom into its slot, for every window k, with the transforms of
-// window k: w = cutoff*(plane + offset*f_w), dw/dlambda = offset*g_w*cutoff
+// Staging of one atom for window k, with the transforms of window k:
+// w = cutoff*(plane + offset*f_w), dw/dlambda = offset*g_w*cutoff
 // (timemachine/cpp/src/kernels/k_lambda_transformer_jit.cuh:25-55);
 // interpolated parameters p = (1-f) p0 + f p1 and dp/dlambda = g (p1 - p0)
-// per parameter column (same file :57-98). The atom is lambda-dependent when
-// its offset is nonzero, its end states differ, or any window stages values
-// other than window 0's: pairs of lambda-independent atoms give the same
-// per-pair values in every window, bit for bit.
-__device__ __forceinline__ void prepare_slot(const PrepareArgs &a, int s, int atom) {
+// per parameter column (same file :57-98). v[0..5] receives the staged
+// parameters and their lambda derivatives in FP64.
+__device__ __forceinline__ void window_values(const PrepareArgs &a, int atom, int k, double &w, double &dw_dl,
+                                              double (&v)[6]) {
     const int plane = a.plane[atom];
     const int offset = a.offset[atom];
-    const double *xa = a.x + 3 * (size_t)atom;
-    const double x0 = xa[0], x1 = xa[1], x2 = xa[2];
-    const float fx = (float)x0, fy = (float)x1, fz = (float)x2;
+    const LambdaWindow &L = a.lam[k];
+    w = (plane + offset * L.f_w) * a.cutoff;
+    dw_dl = offset * L.g_w * a.cutoff;
     const double *p0 = a.p + 3 * (size_t)atom;
-    const double q0 = p0[0], s0 = p0[1], e0 = p0[2];
-    double q1 = q0, s1 = s0, e1 = e0;
-    bool dep = offset != 0;
+    v[0] = p0[0];
+    v[1] = p0[1];
+    v[2] = p0[2];
+    v[3] = v[4] = v[5] = 0.0;
     if (a.interpolated) {
         const double *p1 = a.p + 3 * ((size_t)a.N + atom);
-        q1 = p1[0];
-        s1 = p1[1];
-        e1 = p1[2];
-        dep = dep || q0 != q1 || s0 != s1 || e0 != e1;
+        v[0] = (1 - L.f_q) * p0[0] + L.f_q * p1[0];
+        v[1] = (1 - L.f_s) * p0[1] + L.f_s * p1[1];
+        v[2] = (1 - L.f_e) * p0[2] + L.f_e * p1[2];
+        v[3] = L.g_q * (p1[0] - p0[0]);
+        v[4] = L.g_s * (p1[1] - p0[1]);
+        v[5] = L.g_e * (p1[2] - p0[2]);
     }
-    double first[6] = {0, 0, 0, 0, 0, 0};
-    for (int k = 0; k < a.K; k++) {
-        const LambdaWindow &L = a.lam[k];
-        const double w = (plane + offset * L.f_w) * a.cutoff;
-        const double dw_dl = offset * L.g_w * a.cutoff;
-        double v[6] = {q0, s0, e0, 0.0, 0.0, 0.0};
+}
+
+__device__ __forceinline__ void stage_window(const PrepareArgs &a, int s, int atom, int k) {
+    double w, dw_dl, v[6];
+    window_values(a, atom, k, w, dw_dl, v);
+    const double *xa = a.x + 3 * (size_t)atom;
+    const size_t o = (size_t)k * a.S + s;
+    a.slots.posw[o] = make_float4((float)xa[0], (float)xa[1], (float)xa[2], (float)w);
+    a.slots.prm[o] = make_float4((float)v[0], (float)v[1], (float)v[2], (float)dw_dl);
+    if (a.interpolated) {
+        a.slots.dprm[o] = make_float4((float)v[3], (float)v[4], (float)v[5], 0.0f);
+    }
+    if (a.slots.posw64 != nullptr) {
+        a.slots.posw64[o] = make_double4(xa[0], xa[1], xa[2], w);
+        a.slots.prm64[o] = make_double4(v[0], v[1], v[2], dw_dl);
         if (a.interpolated) {
-            v[0] = (1 - L.f_q) * q0 + L.f_q * q1;
-            v[1] = (1 - L.f_s) * s0 + L.f_s * s1;
-            v[2] = (1 - L.f_e) * e0 + L.f_e * e1;
-            v[3] = L.g_q * (q1 - q0);
-            v[4] = L.g_s * (s1 - s0);
-            v[5] = L.g_e * (e1 - e0);
+            a.slots.dprm64[o] = make_double4(v[3], v[4], v[5], 0.0);
         }
-        const size_t o = (size_t)k * a.S + s;
-        a.slots.posw[o] = make_float4(fx, fy, fz, (float)w);
-        a.slots.prm[o] = make_float4((float)v[0], (float)v[1], (float)v[2], (float)dw_dl);
-        if (a.interpolated) {
-            a.slots.dprm[o] = make_float4((float)v[3], (float)v[4], (float)v[5], 0.0f);
-        }
-        if (a.slots.posw64 != nullptr) {
-            a.slots.posw64[o] = make_double4(x0, x1, x2, w);
-            a.slots.prm64[o] = make_double4(v[0], v[1], v[2], dw_dl);
-            if (a.interpolated) {
-                a.slots.dprm64[o] = make_double4(v[3], v[4], v[5], 0.0);
-            }
-        }
+    }
+}
+
+// An atom is lambda-dependent when its offset is nonzero, its end states
+// differ, or any window stages parameter values other than window 0's: pairs
+// of lambda-independent atoms give the same per-pair values in every window,
+// bit for bit.
+__device__ __forceinline__ bool lambda_dependent(const PrepareArgs &a, int atom) {
+    if (a.offset[atom] != 0) {
+        return true;
+    }
+    if (!a.interpolated) {
+        return false;
+    }
+    const double *p0 = a.p + 3 * (size_t)atom;
+    const double *p1 = a.p + 3 * ((size_t)a.N + atom);
+    if (p0[0] != p1[0] || p0[1] != p1[1] || p0[2] != p1[2]) {
+        return true;
+    }
+    double w, dw_dl, first[6], v[6];
+    window_values(a, atom, 0, w, dw_dl, first);
+    for (int k = 1; k < a.K; k++) {
+        window_values(a, atom, k, w, dw_dl, v);
         for (int c = 0; c < 6; c++) {
-            if (k == 0) {
-                first[c] = v[c];
-            } else if (v[c] != first[c]) {
-                dep = true;
+            if (v[c] != first[c]) {
+                return true;
             }
         }
     }
-    a.slots.lamdep[s] = dep ? 1 : 0;
+    return false;
+}
+
+// Stage one atom into its slot for every window and record its lambda dependence.
+__device__ __forceinline__ void prepare_slot(const PrepareArgs &a, int s, int atom) {
+    for (int k = 0; k < a.K; k++) {
+        stage_window(a, s, atom, k);
+    }
+    a.slots.lamdep[s] = lambda_dependent(a, atom) ? 1 : 0;
 }
 
 // ---------------------------------------------------------------------------
@@ -191,9 +213,19 @@ static __global__ void k_check_prepare(
             }
         }
     }
+    // one thread per (window, slot), slots fastest: the K windows' staging
+    // stores spread over the grid; the window-0 thread of a slot also takes
+    // the rebuild test and the slot's lambda dependence
     const double half_pad2 = 0.25 * a.padding * a.padding;
-    for (int s = tid; s < a.S; s += gridDim.x * blockDim.x) {
+    const size_t total = (size_t)a.S * (size_t)a.K;
+    for (size_t t = tid; t < total; t += (size_t)gridDim.x * blockDim.x) {
+        const int k = (int)(t / (size_t)a.S);
+        const int s = (int)(t - (size_t)k * a.S);
         const int atom = perm[s];
+        stage_window(a, s, atom, k);
+        if (k != 0) {
+            continue;
+        }
         if (nb_x != nullptr) {
             const double *xn = a.x + 3 * (size_t)atom;
             const double *xo = nb_x + 3 * (size_t)atom;
@@ -204,9 +236,9 @@ static __global__ void k_check_prepare(
                 state->rebuild = 1; // benign race: every writer stores 1
             }
         }
-        const unsigned char dep_before = a.slots.lamdep[s];
-        prepare_slot(a, s, atom);
-        if (a.slots.lamdep[s] != dep_before) {
+        const unsigned char dep = lambda_dependent(a, atom) ? 1 : 0;
+        if (a.slots.lamdep[s] != dep) {
+            a.slots.lamdep[s] = dep;
             // the lambda-dependent tiles change with it (benign race: every writer stores the same)
             state->dep_dirty = 1;
             state->n_dep = 0;

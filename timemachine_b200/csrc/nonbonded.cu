@@ -505,9 +505,12 @@ class NonbondedPotential : public PotentialBase {
 
         const int tpb = 256;
         const int sgrid = std::max(1, std::min((S_ + tpb - 1) / tpb, 8 * num_sms()));
+        // k_check_prepare: one thread per (window, slot)
+        const int pgrid = (int)std::max<size_t>(
+            1, std::min<size_t>(((size_t)S_ * K + tpb - 1) / tpb, 8 * (size_t)num_sms()));
         stage_begin(TMNB_STAGE_PREPARE, stream);
         launch_dependent(
-            k_check_prepare, dim3(sgrid), dim3(tpb), 0, stream, pa, (const unsigned *)perm_.p,
+            k_check_prepare, dim3(pgrid), dim3(tpb), 0, stream, pa, (const unsigned *)perm_.p,
             (const double *)(has_nblist_ ? nb_x_.p : nullptr), (const double *)nb_box_.p, state_.p);
         CK(cudaPeekAtLastError());
         stage_end(TMNB_STAGE_PREPARE, stream);

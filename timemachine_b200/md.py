@@ -52,9 +52,33 @@ class MonteCarloBarostat:
         self.group_idxs = group_idxs
         self.interval = interval
         self.seed = seed
+        self._contexts = []  # contexts driving this barostat (weak references)
 
     def impl(self, bound_potentials=None):
         return self
+
+    def _live(self):
+        out = []
+        for ref in self._contexts:
+            c = ref()
+            if c is not None and getattr(c, "_h", None):
+                out.append(c)
+        return out
+
+    def set_pressure(self, pressure):
+        """custom_ops.MonteCarloBarostat.set_pressure (bar)."""
+        self.pressure = pressure
+        for c in self._live():
+            _lib.check(c._lib.tmnb_context_barostat_set_pressure(c._h, float(pressure)))
+
+    def set_interval(self, interval):
+        """custom_ops.MonteCarloBarostat.set_interval: restarts the move counter."""
+        self.interval = interval
+        for c in self._live():
+            _lib.check(c._lib.tmnb_context_barostat_set_interval(c._h, int(interval)))
+
+    def get_interval(self):
+        return self.interval
 
     def group_of(self):
         g = np.full(self.N, -1, dtype=np.int32)
@@ -103,6 +127,9 @@ class Context:
         )
         self._h = h
         if barostat is not None:
+            import weakref
+
+            barostat._contexts.append(weakref.ref(self))
             g = barostat.group_of()
             _lib.check(
                 self._lib.tmnb_context_set_barostat(
@@ -185,6 +212,20 @@ class Context:
     def set_box(self, box):
         box = np.ascontiguousarray(box, dtype=np.float64)
         _lib.check(self._lib.tmnb_context_set_box(self._h, _p(box)))
+
+    def barostat_last_move(self):
+        """The last barostat move: dict of rand0, rand1, proposal_scale,
+        volume_delta, length_scale, accepted, volume_scale (after adaptation),
+        pressure (kJ/mol/nm^3), u_before / u_after (fixed point, uint64)."""
+        vals = np.zeros(8)
+        us = np.zeros(2, dtype=np.uint64)
+        _lib.check(self._lib.tmnb_context_barostat_last_move(self._h, _p(vals), _p(us)))
+        keys = ["rand0", "rand1", "proposal_scale", "volume_delta", "length_scale", "accepted", "volume_scale",
+                "pressure"]
+        out = dict(zip(keys, vals.tolist()))
+        out["accepted"] = bool(out["accepted"])
+        out["u_before"], out["u_after"] = np.uint64(us[0]), np.uint64(us[1])
+        return out
 
     def barostat_stats(self):
         a, t, vs = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_double()
