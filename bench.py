@@ -119,6 +119,8 @@ def parse():
         "the command profiled by ncu for the committed kernel summaries",
     )
     ap.add_argument("--profile-outputs", default="all", choices=["all", "du_dx", "u"])
+    ap.add_argument("--profile-precision", default="f32", choices=["f32", "f64"],
+                    help="pair arithmetic of the windows/single profile modes")
     ap.add_argument(
         "--profile-mode",
         default="windows",
@@ -181,7 +183,7 @@ def run_profile(args, local):
 
     s, x, p, lambdas = build_workload(0)
     impl = P.Nonbonded(s.exclusion_idxs, s.scales, s.lambda_plane_idxs, s.lambda_offset_idxs, s.beta, s.cutoff)
-    impl = impl.unbound_impl(np.float32)
+    impl = impl.unbound_impl(np.float64 if args.profile_precision == "f64" else np.float32)
     dev = torch.device("cuda", local)
     dx = torch.as_tensor(x, device=dev)
     dp = torch.as_tensor(p, device=dev).reshape(-1)
