@@ -557,6 +557,11 @@ tmnb_status tmnb_batch_stats(tmnb_batch *b, int id, int *tiles, int *items, int 
 /* The batch's CUDA stream (every batch call is ordered on it), e.g. to record
  * events around tmnb_batch_evaluate / tmnb_batch_md. */
 tmnb_status tmnb_batch_stream(tmnb_batch *b, void **stream);
+/* Scheduling priority of the batch's stream (CUDA stream priority, clamped to
+ * the device's range; lower numbers are scheduled first when blocks of
+ * several streams wait for SMs). Waits for the batch's work; its stream
+ * handle changes. */
+tmnb_status tmnb_batch_set_priority(tmnb_batch *b, int priority);
 int tmnb_batch_size(const tmnb_batch *b);
 
 /* Largest N accepted by tmnb_pair_list_execute_static (3.16 MiB of static

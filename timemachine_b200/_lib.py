@@ -174,6 +174,8 @@ def _declare(lib):
     lib.tmnb_batch_error.argtypes = [vp, i, c_int_p]
     lib.tmnb_batch_stats.argtypes = [vp, i, c_int_p, c_int_p, c_int_p]
     lib.tmnb_batch_stream.argtypes = [vp, ctypes.POINTER(vp)]
+    lib.tmnb_batch_set_priority.argtypes = [vp, i]
+    lib.tmnb_batch_set_priority.restype = ctypes.c_int
     lib.tmnb_batch_size.argtypes = [vp]
     lib.tmnb_batch_size.restype = ctypes.c_int
     lib.tmnb_potential_num_params.argtypes = [vp]

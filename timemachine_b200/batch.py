@@ -40,11 +40,15 @@ def _terms(system, name, width):
 
 
 class ReplicaBatch:
-    def __init__(self):
+    def __init__(self, priority=None):
+        """priority: CUDA stream priority of the batch's stream (lower numbers
+        first; None: the default priority)."""
         self._lib = _lib.lib()
         h = ctypes.c_void_p()
         _lib.check(self._lib.tmnb_batch_create(ctypes.byref(h)))
         self._h = h
+        if priority is not None:
+            _lib.check(self._lib.tmnb_batch_set_priority(self._h, int(priority)))
         self._n = {}
         self.tuning = {"chunk": 4, "padding": 0.1, "grid_bits_offset": 0, "pair_ctas_per_sm": 0, "rows": 16}
 

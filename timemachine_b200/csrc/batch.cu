@@ -854,6 +854,26 @@ class BatchEngine {
     int size() const { return (int)reps_.size(); }
     cudaStream_t stream() const { return stream_; }
 
+    // Scheduling priority of the batch's stream (cudaStreamCreateWithPriority;
+    // lower numbers run first where blocks of several streams wait for SMs).
+    // The stream is replaced after the work on it finished; captured graphs
+    // are dropped.
+    void set_priority(int priority) {
+        int least = 0, greatest = 0;
+        CK(cudaDeviceGetStreamPriorityRange(&least, &greatest));
+        priority = std::max(greatest, std::min(least, priority));
+        CK(cudaStreamSynchronize(stream_));
+        drop_graphs();
+        cudaStream_t s = nullptr;
+        CK(cudaStreamCreateWithPriority(&s, cudaStreamNonBlocking, priority));
+        // arenas were allocated in order on the old stream: it has finished
+        for (auto &kv : reps_) {
+            kv.second->arena.stream = s;
+        }
+        CK(cudaStreamDestroy(stream_));
+        stream_ = s;
+    }
+
   private:
     struct Layout {
         size_t x, v, box, p, plane, offset, pairs, scales, bonds, bparams, angles, aparams, cbs, ccs;
@@ -1269,6 +1289,13 @@ tmnb_status tmnb_batch_create(tmnb_batch **out) {
         b->impl = std::make_unique<tmb::BatchEngine>();
         *out = b.release();
     });
+}
+
+tmnb_status tmnb_batch_set_priority(tmnb_batch *b, int priority) {
+    if (!b) {
+        return null_argument();
+    }
+    return tmb::guarded([&] { b->impl->set_priority(priority); });
 }
 
 tmnb_status tmnb_batch_destroy(tmnb_batch *b) {

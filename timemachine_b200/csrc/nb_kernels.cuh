@@ -1556,10 +1556,11 @@ static __global__ void k_dep_tiles(DepArgs a, DevState *state) {
 template <typename Real, bool U, bool DX, bool DL, bool DP, bool INTERP, bool MULTI, int RG = TILE>
 // Occupancy, measured on B200: all four outputs at 6 CTAs/SM (80 registers,
 // no spills; 12-window call -3.5 % against 5), forces only at 8 (64). FP64
-// variants are left to the compiler.
+// variants at 5 (96 registers, a few spilled words): the 12-window call
+// took 0.407 ms against 0.455 ms at the compiler's 154 registers (3 CTAs).
 __global__ void __launch_bounds__(
     128,
-    sizeof(Real) != 4 ? 1 : ((U && DX && DL && DP && !INTERP) ? 6 : ((DX && !U && !DL && !DP) ? 8 : 1)))
+    sizeof(Real) != 4 ? 5 : ((U && DX && DL && DP && !INTERP) ? 6 : ((DX && !U && !DL && !DP) ? 8 : 1)))
     k_pair(PairArgs a) {
     grid_dependency_wait();
     if (a.state->error) {

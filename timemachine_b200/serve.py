@@ -62,10 +62,10 @@ def _terms(system, name):
 class _Engine:
     """One ReplicaBatch with its stream, its in-flight launch and its requests."""
 
-    def __init__(self, tuning):
+    def __init__(self, tuning, priority=None):
         import torch
 
-        self.batch = ReplicaBatch()
+        self.batch = ReplicaBatch(priority=priority)
         if tuning:
             self.batch.set_tuning(**tuning)
         self.stream = torch.cuda.ExternalStream(self.batch.stream)
@@ -99,7 +99,10 @@ class Server:
         self.md_max_atoms = int(md_max_atoms)
         self.md_chunk = int(md_chunk)
         self.md_graphs = md_graphs
-        self.ev = _Engine(tuning)
+        # evaluations are short and latency-bound: their stream gets the
+        # highest scheduling priority, so their blocks go first whenever the
+        # MD chunk's kernels free an SM
+        self.ev = _Engine(tuning, priority=-1000)
         self.md = _Engine(tuning)
         self.waiting = []  # arrived or future requests, not yet admitted
         self.done = []
