@@ -272,3 +272,80 @@ def test_near_coincident_exclusions_bitexact_vs_reference(precision):
             np.testing.assert_array_equal(a[k], b[k])
     else:
         compare(decode(b, params.shape), decode(a, params.shape), 1e-8, 1e-9, "coincident f64")
+
+
+def _np_decode(fixed, p_shape):
+    from timemachine_b200.fixed_point import du_dp_fixed_to_float, fixed_to_float, sum_fixed
+
+    dx, dp, dl, u = fixed
+    return fixed_to_float(dx), du_dp_fixed_to_float(dp).reshape(p_shape), fixed_to_float(sum_fixed(dl)), \
+        fixed_to_float(sum_fixed(u))
+
+
+@pytest.mark.parametrize("interpolated", [False, True])
+def test_f64_pair_list_and_group_vs_oracle(interpolated):
+    """The FP64 kernels of the other potentials of the path: the negated pair
+    list (exclusions) and the interaction group, plain and interpolated,
+    within the reference's FP64 tolerance of the oracle."""
+    from oracle.nonbonded_oracle import interaction_group_oracle, pair_list_oracle
+
+    rng = np.random.default_rng(77 + int(interpolated))
+    c = small_water_case(rng, 400)
+    N = c["x"].shape[0]
+    params = c["params"]
+    if interpolated:
+        params = np.concatenate([params, params * rng.uniform(0.5, 1.5, size=params.shape)])
+    x, p, box = f32_round(c["x"]), f32_round(params), c["box"]
+    lam = 0.35
+    cls = P.NonbondedPairListNegatedInterpolated if interpolated else P.NonbondedPairListNegated
+    pl = cls(c["exclusion_idxs"], c["scales"], c["plane"], c["offset"], 2.0, 1.0).unbound_impl(np.float64)
+    test = pl.execute(x, p, box, lam)
+    rx, rp, rl, ru = pair_list_oracle(x, p, box, lam, c["plane"], c["offset"], 2.0, 1.0, c["exclusion_idxs"],
+                                      c["scales"], interpolated)
+    compare((-rx, -rp, -rl, -ru), test, 1e-8, 1e-8, "pair list")
+    rows = rng.choice(N, size=37, replace=False).astype(np.int32)
+    gcls = P.NonbondedInteractionGroupInterpolated if interpolated else P.NonbondedInteractionGroup
+    g = gcls(rows, c["plane"], c["offset"], 2.0, 1.1).unbound_impl(np.float64)
+    test = g.execute(x, p, box, lam)
+    ref = interaction_group_oracle(x, p, box, lam, c["plane"], c["offset"], 2.0, 1.1, rows, interpolated)
+    compare(ref, test, 1e-8, 1e-8, "group")
+
+
+@needs_ref
+@pytest.mark.parametrize("interpolated", [False, True])
+def test_f64_group_vs_reference_f64_kernel(interpolated):
+    from timemachine_b200 import testsystems
+
+    rng = np.random.default_rng(91)
+    s = testsystems.build_system(700, 3.0, seed=21, n_ligand=24)
+    rows = np.flatnonzero(s.lambda_offset_idxs != 0).astype(np.int32)
+    params = s.params
+    if interpolated:
+        params = np.concatenate([params, params * rng.uniform(0.8, 1.2, size=params.shape)])
+    x, p = f32_round(s.x), f32_round(params)
+    gcls = P.NonbondedInteractionGroupInterpolated if interpolated else P.NonbondedInteractionGroup
+    mine = gcls(rows, s.lambda_plane_idxs, s.lambda_offset_idxs, s.beta, s.cutoff).unbound_impl(np.float64)
+    ref = refgpu.RefInteractionGroup(rows, s.lambda_plane_idxs, s.lambda_offset_idxs, s.beta, s.cutoff,
+                                     interpolated, precision=64)
+    for lam in [0.0, 0.4]:
+        a = mine._execute_fixed(x, p, s.box, lam, True, True, True, True)
+        b = ref.execute_host_fixed(x, p, s.box, lam)
+        compare(_np_decode(b, p.shape), _np_decode(a, p.shape), 1e-8, 1e-9, f"group lambda={lam}")
+
+
+def test_lambda_transforms_on_the_interaction_group():
+    """The group forwards the transform expressions too (its constructor's
+    last four arguments), checked against the oracle with the same transforms."""
+    from oracle.nonbonded_oracle import interaction_group_oracle
+
+    c, qlj = _advanced_case()
+    x, p = f32_round(c["x"]), f32_round(qlj)
+    box = np.eye(3) * 3.0
+    rows = np.arange(0, 36, 3, dtype=np.int32)
+    g = P.NonbondedInteractionGroupInterpolated(rows, c["plane"], c["offset"], 2.0, 1.0,
+                                                *TRANSFORM_EXPRS).unbound_impl(np.float64)
+    for lam in [0.1, 0.6]:
+        test = g.execute(x, p, box, lam)
+        ref = interaction_group_oracle(x, p, box, lam, c["plane"], c["offset"], 2.0, 1.0, rows, True,
+                                       transforms=TRANSFORM_FNS)
+        compare(ref, test, 1e-8, 1e-11, f"lambda={lam}", 1e-11)
