@@ -124,10 +124,10 @@ def parse():
     ap.add_argument(
         "--profile-mode",
         default="windows",
-        choices=["windows", "single", "md", "batch", "grad"],
+        choices=["windows", "single", "md", "batch", "batch_md", "grad"],
         help="windows: one 12-window call per step; single: one single-window call per step (cycling lambdas); "
         "md: Langevin steps of the MD workload (graph-replayed); batch: evaluations of 64 replicas (the first 8 "
-        "systems of the batching mix x 8 windows); grad: loss gradients of the differentiation workload on 4 frames",
+        "systems of the batching mix x 8 windows); batch_md: batched Langevin steps of the same 64 replicas; grad: loss gradients of the differentiation workload on 4 frames",
     )
     ap.add_argument(
         "--forms",
@@ -158,18 +158,23 @@ def run_profile(args, local):
         ctx.multiple_steps(np.full(args.profile, MD_LAMBDA))
         print(json.dumps({"profile_md_steps": args.profile}))
         return
-    if args.profile_mode == "batch":
+    if args.profile_mode in ("batch", "batch_md"):
         from timemachine_b200.batch import ReplicaBatch
 
         systems, lambdas = batch_workload()
         b = ReplicaBatch()
+        rng = np.random.default_rng(SEED + 5)
         for k, s in enumerate(systems[:8]):
             for w, lam in enumerate(lambdas):
-                b.add(s, lam, seed=1000 * k + w)
+                b.add(s, lam, v=_mb_velocities(rng, s, BATCH_MD["temperature"]), md=BATCH_MD, seed=1000 * k + w)
         for _ in range(args.profile):
-            b.evaluate()
+            if args.profile_mode == "batch":
+                b.evaluate()
+            else:
+                b.md(1, chunk=1, use_graph=False)
         b.synchronize()
-        print(json.dumps({"profile_batch_evaluations": args.profile, "replicas": len(b)}))
+        print(json.dumps({"profile_batch_" + ("evaluations" if args.profile_mode == "batch" else "md_steps"):
+                          args.profile, "replicas": len(b)}))
         return
     if args.profile_mode == "grad":
         loss_and_grads = grad_workload(n_frames=4)[0]
