@@ -345,7 +345,11 @@ __device__ __forceinline__ PairArgs pair_args(const Rep &r) {
 
 // Persistent pair kernel over every replica's work units.
 template <bool U, bool DX, bool DL, bool DP, int RG>
-__global__ void __launch_bounds__(128, (DX && !U && !DL && !DP) ? 8 : 5) k_b_pair(const Rep *__restrict__ reps, int R, const int *__restrict__ prefix, int *counter) {
+__global__ void __launch_bounds__(
+    128, (DX && !U && !DL && !DP) ? (TMNB_PACKED_FORCES && RG == 16 ? TMNB_PACKED_FORCES_CTAS : 8) : 5)
+    k_b_pair(const Rep *__restrict__ reps, int R, const int *__restrict__ prefix, int *counter) {
+    // forces-only evaluations of 16-row tiles take the packed sweep, as in k_pair
+    constexpr bool PACKED = TMNB_PACKED_FORCES && RG == 16 && DX && !U && !DL && !DP;
     const int lane = threadIdx.x & 31;
     const int total = prefix[R];
     for (;;) {
@@ -388,6 +392,18 @@ __global__ void __launch_bounds__(128, (DX && !U && !DL && !DP) ? 8 : 5) k_b_pai
             continue;
         }
         const int4 it = r.items[local];
+        if constexpr (PACKED) {
+            const unsigned ia = (unsigned)(it.x * RG + (lane & 7));
+            RowForces A, B;
+            for (int t = 0; t < it.z; t++) {
+                const long long tile = (long long)it.y + t;
+                const unsigned j = r.tile_cols[tile * TILE + lane];
+                tile_forces_p2(a, lane, S, ia, j, 0, a.acc, box_x, box_y, box_z, inv_box_x, inv_box_y, inv_box_z,
+                               cutoff_squared, beta, A, B);
+            }
+            flush_forces_p2(a.acc, ia, S, A, B);
+            continue;
+        }
         const unsigned i = (unsigned)(it.x * RG + (lane & (RG - 1)));
         unsigned long long gi_x = 0, gi_y = 0, gi_z = 0, g_qi = 0, g_sigi = 0, g_epsi = 0, du_dl = 0, energy = 0;
         for (int t = 0; t < it.z; t++) {
