@@ -217,7 +217,7 @@ __global__ void k_b_bounds(const Rep *__restrict__ reps, const int2 *__restrict_
     block_bounds_warp(r.N, m.y, r.box, r.posw, r.bb_ctr, r.bb_ext);
 }
 
-__global__ void __launch_bounds__(TB_WARPS * 32) k_b_tiles(const Rep *__restrict__ reps, const int2 *__restrict__ gmap) {
+__global__ void __launch_bounds__(TB_WARPS * 32, TMNB_TB_CTAS) k_b_tiles(const Rep *__restrict__ reps, const int2 *__restrict__ gmap) {
     const int2 m = gmap[blockIdx.x]; // (replica, row group)
     const Rep &r = reps[m.x];
     if (!r.state->rebuild || r.state->error) {

@@ -648,9 +648,18 @@ __host__ __device__ __forceinline__ long long tile_base(const TileArgs &a, int g
 }
 
 constexpr int TB_WARPS = 8;
+// Tile-build CTAs per SM the compiler must fit (40 registers). The packed row
+// tests left to the compiler take 57 registers (4 CTAs/SM): measured on B200,
+// one rebuild 87.3 us with the scalar tests, 90.0 us packed at 57 registers,
+// 81.3 us packed at 40.
+#ifndef TMNB_TB_CTAS
+#define TMNB_TB_CTAS 6
+#endif
 
 __device__ __forceinline__ void build_tiles_cta(const TileArgs &a, const int rb, DevState *state) {
     __shared__ float4 row_pos[TILE];
+    // the same positions as x, y, z arrays: element pair m holds rows 2m, 2m + 1
+    __shared__ __align__(8) float row_x[TILE], row_y[TILE], row_z[TILE];
     __shared__ float4 row_box[2]; // the row group's box: centre, half-extent
     __shared__ unsigned buf[TB_WARPS][2 * TILE];
     __shared__ unsigned rem[TB_WARPS * TILE];
@@ -714,6 +723,9 @@ __device__ __forceinline__ void build_tiles_cta(const TileArgs &a, const int rb,
         p.y = rc.y + wrap_delta(p.y - rc.y, Ly, iLy);
         p.z = rc.z + wrap_delta(p.z - rc.z, Lz, iLz);
         row_pos[threadIdx.x] = p;
+        row_x[threadIdx.x] = p.x;
+        row_y[threadIdx.x] = p.y;
+        row_z[threadIdx.x] = p.z;
     }
     if (threadIdx.x == 0) {
         tile_count = 0;
@@ -777,15 +789,20 @@ __device__ __forceinline__ void build_tiles_cta(const TileArgs &a, const int rb,
             bool hit = false;
             if (__any_sync(FULL_MASK, need)) {
                 if (shifted) {
-                    const float qx = rc.x + wx, qy = rc.y + wy, qz = rc.z + wz;
+                    // two rows per packed FP32x2 test (rows past row_n sit at
+                    // the centre and are masked)
+                    const float2 qx = f2(rc.x + wx), qy = f2(rc.y + wy), qz = f2(rc.z + wz);
+                    const float2 *rx2 = reinterpret_cast<const float2 *>(row_x);
+                    const float2 *ry2 = reinterpret_cast<const float2 *>(row_y);
+                    const float2 *rz2 = reinterpret_cast<const float2 *>(row_z);
                     for (int r0 = 0; r0 < row_n; r0 += 8) {
 #pragma unroll
-                        for (int r = r0; r < r0 + 8; r++) {
-                            const float4 pi = row_pos[r]; // rows past row_n sit at the centre and are masked below
-                            const float dx = pi.x - qx;
-                            const float dy = pi.y - qy;
-                            const float dz = pi.z - qz;
-                            hit |= (r < row_n) && (dx * dx + dy * dy + dz * dz < r2);
+                        for (int r = r0; r < r0 + 8; r += 2) {
+                            const float2 dx = fsub2(rx2[r >> 1], qx);
+                            const float2 dy = fsub2(ry2[r >> 1], qy);
+                            const float2 dz = fsub2(rz2[r >> 1], qz);
+                            const float2 d2 = ffma2(dz, dz, ffma2(dy, dy, fmul2(dx, dx)));
+                            hit |= ((r < row_n) && (d2.x < r2)) || ((r + 1 < row_n) && (d2.y < r2));
                         }
                         if (__all_sync(FULL_MASK, hit || !need)) {
                             break;
@@ -917,7 +934,7 @@ __device__ __forceinline__ void build_tiles_cta(const TileArgs &a, const int rb,
     }
 }
 
-static __global__ void __launch_bounds__(TB_WARPS * 32) k_build_tiles(TileArgs a, DevState *state) {
+static __global__ void __launch_bounds__(TB_WARPS * 32, TMNB_TB_CTAS) k_build_tiles(TileArgs a, DevState *state) {
     grid_dependency_wait();
     if (!state->rebuild || state->error) {
         return;
@@ -1531,49 +1548,12 @@ __device__ __forceinline__ void flush_row_rg(
 // about half the FP32 instructions, and one column rotation for two pairs.
 // The transcendental steps (rsqrt, exp, the IEEE reciprocal) and the
 // fixed-point conversions stay per component, and the row and column forces
-// of a pair are converted once, as in pair_terms. The packed operations are
-// inline PTX: an asm statement is never contracted, so a product followed by
-// a sum keeps both roundings. (The all-outputs variants keep the one-row
+// of a pair are converted once, as in pair_terms. The packed operations
+// (fmul2 and the others, nb_pair_math.cuh) are inline PTX, so a product
+// followed by a sum keeps both roundings. (The all-outputs variants keep the one-row
 // sweep: with two rows per lane they need 127 registers, 4 CTAs/SM, and the
 // 12-window call measured 2 % slower.)
 // ---------------------------------------------------------------------------
-__device__ __forceinline__ float2 f2(float v) { return make_float2(v, v); }
-__device__ __forceinline__ float2 fmul2(float2 a, float2 b) {
-    float2 r;
-    asm("{\n\t.reg .b64 ra, rb, rd;\n\tmov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
-        "mul.rn.f32x2 rd, ra, rb;\n\tmov.b64 {%0, %1}, rd;\n\t}"
-        : "=f"(r.x), "=f"(r.y)
-        : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
-    return r;
-}
-__device__ __forceinline__ float2 fadd2(float2 a, float2 b) {
-    float2 r;
-    asm("{\n\t.reg .b64 ra, rb, rd;\n\tmov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
-        "add.rn.f32x2 rd, ra, rb;\n\tmov.b64 {%0, %1}, rd;\n\t}"
-        : "=f"(r.x), "=f"(r.y)
-        : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
-    return r;
-}
-__device__ __forceinline__ float2 fsub2(float2 a, float2 b) {
-    float2 r;
-    asm("{\n\t.reg .b64 ra, rb, rd;\n\tmov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
-        "sub.rn.f32x2 rd, ra, rb;\n\tmov.b64 {%0, %1}, rd;\n\t}"
-        : "=f"(r.x), "=f"(r.y)
-        : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y));
-    return r;
-}
-__device__ __forceinline__ float2 ffma2(float2 a, float2 b, float2 c) {
-    float2 r;
-    asm("{\n\t.reg .b64 ra, rb, rc, rd;\n\tmov.b64 ra, {%2, %3};\n\tmov.b64 rb, {%4, %5};\n\t"
-        "mov.b64 rc, {%6, %7};\n\tfma.rn.f32x2 rd, ra, rb, rc;\n\tmov.b64 {%0, %1}, rd;\n\t}"
-        : "=f"(r.x), "=f"(r.y)
-        : "f"(a.x), "f"(a.y), "f"(b.x), "f"(b.y), "f"(c.x), "f"(c.y));
-    return r;
-}
-__device__ __forceinline__ float2 madd2(float2 a, float2 b, float2 c, int fused) {
-    return fused ? ffma2(a, b, c) : fadd2(fmul2(a, b), c);
-}
-
 // min_image of nb_pair_math.cuh per component; neg_box = -box.
 __device__ __forceinline__ float2 min_image2(float2 delta, float2 neg_box, float2 inv_box) {
     const float2 magic = f2(12582912.0f); // round_half_even of nb_pair_math.cuh
