@@ -217,42 +217,14 @@ __global__ void k_b_bounds(const Rep *__restrict__ reps, const int2 *__restrict_
     block_bounds_warp(r.N, m.y, r.box, r.posw, r.bb_ctr, r.bb_ext);
 }
 
-__global__ void __launch_bounds__(TB_WARPS * 32, TMNB_TB_CTAS) k_b_tiles(const Rep *__restrict__ reps, const int2 *__restrict__ gmap) {
-    const int2 m = gmap[blockIdx.x]; // (replica, row group)
-    const Rep &r = reps[m.x];
-    if (!r.state->rebuild || r.state->error) {
-        return;
-    }
-    TileArgs ta;
-    ta.S = r.N;
-    ta.RB = r.RB;
-    ta.rows = r.rows;
-    ta.group = 0;
-    ta.row_end = r.N;
-    ta.col_begin = 0;
-    ta.n_row_blocks = r.NG;
-    ta.cb_first = 0;
-    ta.radius = (float)(r.cutoff + r.padding + 1e-5);
-    ta.box = r.box;
-    ta.posw = r.posw;
-    ta.prm = r.prm;
-    ta.bb_ctr = r.bb_ctr;
-    ta.bb_ext = r.bb_ext;
-    ta.tile_cols = r.tile_cols;
-    ta.rb_ntiles = r.rb_ntiles;
-    ta.items = r.items;
-    ta.chunk = r.chunk;
-    build_tiles_cta(ta, m.y, r.state);
-}
-
-// Exclusive prefix over replicas of their work units (tile items + chunks of
-// 32 scaled pairs); replicas with an error contribute none. One CTA.
-__global__ void k_b_units(const Rep *__restrict__ reps, int R, int *__restrict__ prefix, int *__restrict__ counter) {
+// Exclusive prefix over replicas of count(replica) into prefix[0..R-1], the
+// total into prefix[R]. One CTA.
+template <typename Count>
+__device__ __forceinline__ void replica_prefix(int R, int *__restrict__ prefix, Count count) {
     __shared__ int warp_sums[32];
     __shared__ int carry;
     if (threadIdx.x == 0) {
         carry = 0;
-        *counter = 0;
     }
     __syncthreads();
     const int lane = threadIdx.x & 31;
@@ -260,11 +232,7 @@ __global__ void k_b_units(const Rep *__restrict__ reps, int R, int *__restrict__
     const int nwarps = blockDim.x >> 5;
     for (int base = 0; base < R; base += blockDim.x) {
         const int q = base + threadIdx.x;
-        int v = 0;
-        if (q < R) {
-            const Rep &r = reps[q];
-            v = r.state->error ? 0 : r.state->n_items + (r.M + TILE - 1) / TILE;
-        }
+        const int v = q < R ? count(q) : 0;
         int incl = v;
         for (int o = 1; o < 32; o <<= 1) {
             const int n = __shfl_up_sync(FULL_MASK, incl, o);
@@ -301,6 +269,89 @@ __global__ void k_b_units(const Rep *__restrict__ reps, int R, int *__restrict__
     if (threadIdx.x == 0) {
         prefix[R] = carry;
     }
+}
+
+// Last replica q with prefix[q] <= unit (replicas without units are skipped).
+__device__ __forceinline__ int replica_of(const int *__restrict__ prefix, int R, int unit) {
+    int lo = 0, hi = R - 1;
+    while (lo < hi) {
+        const int mid = (lo + hi + 1) >> 1;
+        if (prefix[mid] <= unit) {
+            lo = mid;
+        } else {
+            hi = mid - 1;
+        }
+    }
+    return lo;
+}
+
+// Persistent over the row groups of the replicas that rebuild this step (the
+// prefix of k_b_tile_units), claimed one at a time from a counter: a step in
+// which few replicas rebuild launches a few CTAs per SM instead of one CTA per
+// row group of every replica.
+__global__ void __launch_bounds__(TB_WARPS * 32, TMNB_TB_CTAS)
+    k_b_tiles(const Rep *__restrict__ reps, int R, const int *__restrict__ tprefix, int *__restrict__ tcounter) {
+    const int total = tprefix[R];
+    __shared__ int next;
+    for (;;) {
+        __syncthreads(); // the previous row group's shared state is no longer read
+        if (threadIdx.x == 0) {
+            next = atomicAdd(tcounter, 1); // row groups are claimed dynamically: their costs differ
+        }
+        __syncthreads();
+        const int u = next;
+        if (u >= total) {
+            break;
+        }
+        const int q = replica_of(tprefix, R, u);
+        const Rep &r = reps[q];
+        TileArgs ta;
+        ta.S = r.N;
+        ta.RB = r.RB;
+        ta.rows = r.rows;
+        ta.group = 0;
+        ta.row_end = r.N;
+        ta.col_begin = 0;
+        ta.n_row_blocks = r.NG;
+        ta.cb_first = 0;
+        ta.radius = (float)(r.cutoff + r.padding + 1e-5);
+        ta.box = r.box;
+        ta.posw = r.posw;
+        ta.prm = r.prm;
+        ta.bb_ctr = r.bb_ctr;
+        ta.bb_ext = r.bb_ext;
+        ta.tile_cols = r.tile_cols;
+        ta.rb_ntiles = r.rb_ntiles;
+        ta.items = r.items;
+        ta.chunk = r.chunk;
+        build_tiles_cta(ta, u - tprefix[q], r.state);
+    }
+}
+
+// Exclusive prefix over replicas of their work units (tile items + chunks of
+// 32 scaled pairs); replicas with an error contribute none. One CTA.
+__global__ void k_b_units(const Rep *__restrict__ reps, int R, int *__restrict__ prefix, int *__restrict__ counter) {
+    if (threadIdx.x == 0) {
+        *counter = 0;
+    }
+    replica_prefix(R, prefix, [&](int q) {
+        const Rep &r = reps[q];
+        return r.state->error ? 0 : r.state->n_items + (r.M + TILE - 1) / TILE;
+    });
+}
+
+// Exclusive prefix over replicas of the row groups whose lists this step
+// rebuilds (none for a replica without the rebuild flag or with an error).
+// One CTA.
+__global__ void k_b_tile_units(const Rep *__restrict__ reps, int R, int *__restrict__ tprefix,
+                               int *__restrict__ tcounter) {
+    if (threadIdx.x == 0) {
+        *tcounter = 0;
+    }
+    replica_prefix(R, tprefix, [&](int q) {
+        const Rep &r = reps[q];
+        return (r.state->rebuild && !r.state->error) ? r.NG : 0;
+    });
 }
 
 __device__ __forceinline__ PairArgs pair_args(const Rep &r) {
@@ -361,19 +412,10 @@ __global__ void __launch_bounds__(
         if (unit >= total) {
             break;
         }
-        // replica of the unit: last q with prefix[q] <= unit
-        int lo = 0, hi = R - 1;
-        while (lo < hi) {
-            const int mid = (lo + hi + 1) >> 1;
-            if (prefix[mid] <= unit) {
-                lo = mid;
-            } else {
-                hi = mid - 1;
-            }
-        }
-        const Rep &r = reps[lo];
+        const int q = replica_of(prefix, R, unit);
+        const Rep &r = reps[q];
         const PairArgs a = pair_args(r);
-        const int local = unit - prefix[lo];
+        const int local = unit - prefix[q];
         const float box_x = (float)r.box[0], box_y = (float)r.box[4], box_z = (float)r.box[8];
         const float inv_box_x = 1 / box_x, inv_box_y = 1 / box_y, inv_box_z = 1 / box_z;
         const float real_cutoff = (float)r.cutoff;
@@ -642,6 +684,7 @@ class BatchEngine {
         CK(cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep));
         BPairTable<0, 1, 2, 3, 4, 5, 6, 7, 8, 9, 10, 11, 12, 13, 14, 15>::fill(pair_kernels_);
         counter_.alloc(1);
+        tcounter_.alloc(1);
     }
     ~BatchEngine() {
         drop_graphs();
@@ -1134,7 +1177,8 @@ class BatchEngine {
         CK(cudaStreamSynchronize(stream_));
         drop_graphs();
         std::vector<Rep> table;
-        std::vector<int2> ablk, rbmap, gmap, bmap, amap;
+        std::vector<int2> ablk, rbmap, bmap, amap;
+        int n_groups = 0; // row groups of all replicas
         int q = 0;
         for (auto &kv : reps_) {
             const Rep &r = kv.second->rep;
@@ -1145,9 +1189,7 @@ class BatchEngine {
             for (int rb = 0; rb < r.RB; rb++) {
                 rbmap.push_back(make_int2(q, rb));
             }
-            for (int g = 0; g < r.NG; g++) {
-                gmap.push_back(make_int2(q, g));
-            }
+            n_groups += r.NG;
             for (int b0 = 0; b0 < r.n_bonds; b0 += TERM_BLOCK) {
                 bmap.push_back(make_int2(q, b0));
             }
@@ -1159,14 +1201,13 @@ class BatchEngine {
         R_ = q;
         n_ablk_ = (int)ablk.size();
         n_rb_ = (int)rbmap.size();
-        n_gmap_ = (int)gmap.size();
+        n_groups_ = n_groups;
         n_bmap_ = (int)bmap.size();
         n_amap_ = (int)amap.size();
         if (R_ > 0) {
             upload_on(table_, table.data(), table.size(), stream_);
             upload_on(ablk_, ablk.data(), ablk.size(), stream_);
             upload_on(rbmap_, rbmap.data(), rbmap.size(), stream_);
-            upload_on(gmap_, gmap.data(), gmap.size(), stream_);
             if (n_bmap_) {
                 upload_on(bmap_, bmap.data(), bmap.size(), stream_);
             }
@@ -1174,12 +1215,21 @@ class BatchEngine {
                 upload_on(amap_, amap.data(), amap.size(), stream_);
             }
             prefix_.ensure(R_ + 1);
+            tprefix_.ensure(R_ + 1);
             CK(cudaStreamSynchronize(stream_)); // the host tables above are local
         }
         table_dirty_ = false;
     }
 
     bpair_t pair_kernel(int flags) const { return pair_kernels_[rows_ == 32 ? 0 : (rows_ == 16 ? 1 : 2)][flags]; }
+
+    // persistent tile-build CTAs: as many as are resident at once, and never
+    // more than the row groups of all replicas
+    int tiles_grid() {
+        int per_sm = 0;
+        CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_b_tiles, TB_WARPS * 32, 0));
+        return std::max(1, std::min(std::max(1, per_sm) * num_sms(), n_groups_));
+    }
 
     int pair_grid(int flags) {
         int per_sm = 0;
@@ -1197,7 +1247,8 @@ class BatchEngine {
         k_b_scan<<<R_, 1024, 0, stream_>>>(table_.p);
         k_b_scatter<<<n_ablk_, ATOM_BLOCK, 0, stream_>>>(table_.p, ablk_.p);
         k_b_bounds<<<(n_rb_ * 32 + 255) / 256, 256, 0, stream_>>>(table_.p, rbmap_.p, n_rb_);
-        k_b_tiles<<<n_gmap_, TB_WARPS * 32, 0, stream_>>>(table_.p, gmap_.p);
+        k_b_tile_units<<<1, 1024, 0, stream_>>>(table_.p, R_, tprefix_.p, tcounter_.p);
+        k_b_tiles<<<tiles_grid(), TB_WARPS * 32, 0, stream_>>>(table_.p, R_, tprefix_.p, tcounter_.p);
         k_b_units<<<1, 1024, 0, stream_>>>(table_.p, R_, prefix_.p, counter_.p);
         pair_kernel(flags)<<<pair_grid(flags), 128, 0, stream_>>>(table_.p, R_, prefix_.p, counter_.p);
         k_b_finalize<<<n_ablk_, ATOM_BLOCK, 0, stream_>>>(table_.p, ablk_.p, flags);
@@ -1260,10 +1311,10 @@ class BatchEngine {
     std::map<int, std::unique_ptr<Slot>> reps_;
     int next_id_ = 0;
     bool table_dirty_ = true;
-    int R_ = 0, n_ablk_ = 0, n_rb_ = 0, n_gmap_ = 0, n_bmap_ = 0, n_amap_ = 0;
+    int R_ = 0, n_ablk_ = 0, n_rb_ = 0, n_groups_ = 0, n_bmap_ = 0, n_amap_ = 0;
     DevBuf<Rep> table_;
-    DevBuf<int2> ablk_, rbmap_, gmap_, bmap_, amap_;
-    DevBuf<int> prefix_, counter_;
+    DevBuf<int2> ablk_, rbmap_, bmap_, amap_;
+    DevBuf<int> prefix_, counter_, tprefix_, tcounter_;
     bpair_t pair_kernels_[3][16];
     int rows_ = 16; // slots per row group of every replica's tile list
     std::map<int, cudaGraphExec_t> graphs_;
