@@ -659,7 +659,9 @@ constexpr int TB_WARPS = 8;
 __device__ __forceinline__ void build_tiles_cta(const TileArgs &a, const int rb, DevState *state) {
     __shared__ float4 row_pos[TILE];
     // the same positions as x, y, z arrays: element pair m holds rows 2m, 2m + 1
-    __shared__ __align__(8) float row_x[TILE], row_y[TILE], row_z[TILE];
+    __shared__ __align__(8) float row_x[TILE];
+    __shared__ __align__(8) float row_y[TILE];
+    __shared__ __align__(8) float row_z[TILE];
     __shared__ float4 row_box[2]; // the row group's box: centre, half-extent
     __shared__ unsigned buf[TB_WARPS][2 * TILE];
     __shared__ unsigned rem[TB_WARPS * TILE];
