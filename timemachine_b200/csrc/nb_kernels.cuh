@@ -42,6 +42,12 @@ constexpr int TILE = 32;
 #ifndef TMNB_PACKED_FORCES_CTAS
 #define TMNB_PACKED_FORCES_CTAS 6
 #endif
+// The one-row sweep evaluates the independent x / y steps of a pair (minimum
+// image, force components) and the paired charge / epsilon derivatives in
+// the two components of packed FP32x2 operations.
+#ifndef TMNB_PACKED_SCALAR
+#define TMNB_PACKED_SCALAR 1
+#endif
 
 // Sticky device-side state of one potential instance.
 struct DevState {
@@ -1089,8 +1095,15 @@ __device__ __forceinline__ void pair_terms(
             const unsigned long long gs = to_fixed(sig_grad, FX_EXPONENT_SIG);
             g_sigi += gs;
             g_sigj += gs;
-            g_epsi += to_fixed(fmul(eps_grad, eps_j), FX_EXPONENT_EPS);
-            g_epsj += to_fixed(fmul(eps_grad, eps_i), FX_EXPONENT_EPS);
+            if constexpr (TMNB_PACKED_SCALAR && sizeof(Real) == 4) {
+                const float2 ge = fmul2(fmul2(f2(eps_grad), make_float2(eps_j, eps_i)),
+                                        f2(static_cast<float>(FX_EXPONENT_EPS)));
+                g_epsi += fixed_round(ge.x);
+                g_epsj += fixed_round(ge.y);
+            } else {
+                g_epsi += to_fixed(fmul(eps_grad, eps_j), FX_EXPONENT_EPS);
+                g_epsj += to_fixed(fmul(eps_grad, eps_i), FX_EXPONENT_EPS);
+            }
         }
         if (DL && ALCH && INTERP) {
             real_du_dl = ffma(sig_grad, fadd(dsig_dl_i, dsig_dl_j), real_du_dl);
@@ -1102,8 +1115,15 @@ __device__ __forceinline__ void pair_terms(
         // odd) except where the conversion saturates (|y| >= 2^63) or y is NaN;
         // those lanes add the difference afterwards.
         const Real ex = static_cast<Real>(FX_EXPONENT);
-        const Real yx = fmul(fmul(prefactor, delta_x), ex);
-        const Real yy = fmul(fmul(prefactor, delta_y), ex);
+        Real yx, yy;
+        if constexpr (TMNB_PACKED_SCALAR && sizeof(Real) == 4) {
+            const float2 yxy = fmul2(fmul2(f2(prefactor), make_float2(delta_x, delta_y)), f2(ex));
+            yx = yxy.x;
+            yy = yxy.y;
+        } else {
+            yx = fmul(fmul(prefactor, delta_x), ex);
+            yy = fmul(fmul(prefactor, delta_y), ex);
+        }
         const Real yz = fmul(fmul(prefactor, delta_z), ex);
         const unsigned long long fx = fixed_round(yx);
         const unsigned long long fy = fixed_round(yy);
@@ -1121,8 +1141,15 @@ __device__ __forceinline__ void pair_terms(
         }
     }
     if (DP) {
-        g_qi += to_fixed(fmul(fmul(qj, inv_d), erfc_bd), FX_EXPONENT);
-        g_qj += to_fixed(fmul(fmul(qi, inv_d), erfc_bd), FX_EXPONENT);
+        if constexpr (TMNB_PACKED_SCALAR && sizeof(Real) == 4) {
+            const float2 gq = fmul2(fmul2(fmul2(make_float2(qj, qi), f2(inv_d)), f2(erfc_bd)),
+                                    f2(static_cast<float>(FX_EXPONENT)));
+            g_qi += fixed_round(gq.x);
+            g_qj += fixed_round(gq.y);
+        } else {
+            g_qi += to_fixed(fmul(fmul(qj, inv_d), erfc_bd), FX_EXPONENT);
+            g_qj += to_fixed(fmul(fmul(qi, inv_d), erfc_bd), FX_EXPONENT);
+        }
     }
     if (DL && ALCH) {
         real_du_dl = ffma(fmul(delta_w, prefactor), fsub(dw_dl_i, dw_dl_j), real_du_dl);
@@ -1202,12 +1229,19 @@ __device__ __forceinline__ void sweep_tile(
     constexpr int UNROLL = (DX && !U && !DL && !DP) ? 4 : 1;
 #pragma unroll UNROLL
     for (int round = 0; round < RG; round++) {
-        Real delta_x = fsub(ci_x, cj_x);
-        Real delta_y = fsub(ci_y, cj_y);
-        Real delta_z = fsub(ci_z, cj_z);
-        delta_x = min_image(delta_x, box_x, inv_box_x);
-        delta_y = min_image(delta_y, box_y, inv_box_y);
-        delta_z = min_image(delta_z, box_z, inv_box_z);
+        Real delta_x, delta_y;
+        if constexpr (TMNB_PACKED_SCALAR && sizeof(Real) == 4) {
+            // x and y in the two components of one packed operation each
+            const float2 dxy = min_image2(
+                fsub2(make_float2(ci_x, ci_y), make_float2(cj_x, cj_y)), make_float2(-box_x, -box_y),
+                make_float2(inv_box_x, inv_box_y));
+            delta_x = dxy.x;
+            delta_y = dxy.y;
+        } else {
+            delta_x = min_image(fsub(ci_x, cj_x), box_x, inv_box_x);
+            delta_y = min_image(fsub(ci_y, cj_y), box_y, inv_box_y);
+        }
+        const Real delta_z = min_image(fsub(ci_z, cj_z), box_z, inv_box_z);
         Real d2 = dist2(delta_x, delta_y, delta_z);
         Real delta_w;
         if (ALCH) {
@@ -1556,17 +1590,6 @@ __device__ __forceinline__ void flush_row_rg(
 // sweep: with two rows per lane they need 127 registers, 4 CTAs/SM, and the
 // 12-window call measured 2 % slower.)
 // ---------------------------------------------------------------------------
-// min_image of nb_pair_math.cuh per component; neg_box = -box.
-__device__ __forceinline__ float2 min_image2(float2 delta, float2 neg_box, float2 inv_box) {
-    const float2 magic = f2(12582912.0f); // round_half_even of nb_pair_math.cuh
-    const float2 n = fsub2(fadd2(fmul2(delta, inv_box), magic), magic);
-#if TMNB_DAG_MINIMG
-    return ffma2(neg_box, n, delta);
-#else
-    return fadd2(delta, fmul2(neg_box, n));
-#endif
-}
-
 struct RowForces {
     unsigned long long x = 0, y = 0, z = 0;
 };

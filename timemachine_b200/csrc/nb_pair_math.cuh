@@ -207,6 +207,17 @@ template <typename Real> __device__ __forceinline__ Real add_w2(Real d2, Real dw
 #endif
 }
 
+// min_image per component; neg_box = -box.
+__device__ __forceinline__ float2 min_image2(float2 delta, float2 neg_box, float2 inv_box) {
+    const float2 magic = f2(12582912.0f); // round_half_even
+    const float2 n = fsub2(fadd2(fmul2(delta, inv_box), magic), magic);
+#if TMNB_DAG_MINIMG
+    return ffma2(neg_box, n, delta);
+#else
+    return fadd2(delta, fmul2(neg_box, n));
+#endif
+}
+
 template <typename Real> __device__ __forceinline__ Real madd(Real a, Real b, Real c, int fused) {
     return fused ? ffma(a, b, c) : fadd(fmul(a, b), c);
 }
