@@ -90,10 +90,14 @@ class Server:
     evaluation requests always find room (they are short-lived).
     md_max_atoms: resident MD atoms at most (FIFO admission beyond): an MD
     chunk then takes bounded time, and under a backlog the earlier segments
-    finish first instead of all advancing together."""
+    finish first instead of all advancing together.
+    md_pair_ctas_per_sm: CTAs per SM of the MD engine's persistent pair
+    kernel (0: as many as fit). Its CTAs hold their SM slots for the whole
+    kernel, so a cap below the fit leaves slots on every SM for the
+    evaluation engine's kernels."""
 
     def __init__(self, hbm_budget_bytes=150e9, md_chunk=50, tuning=None, md_graphs=True,
-                 md_budget_fraction=0.8, md_max_atoms=4_000_000):
+                 md_budget_fraction=0.8, md_max_atoms=4_000_000, md_pair_ctas_per_sm=0):
         self.budget = float(hbm_budget_bytes)
         self.md_budget = self.budget * float(md_budget_fraction)
         self.md_max_atoms = int(md_max_atoms)
@@ -103,7 +107,10 @@ class Server:
         # highest scheduling priority, so their blocks go first whenever the
         # MD chunk's kernels free an SM
         self.ev = _Engine(tuning, priority=-1000)
-        self.md = _Engine(tuning)
+        md_tuning = dict(tuning or {})
+        if md_pair_ctas_per_sm:
+            md_tuning["pair_ctas_per_sm"] = int(md_pair_ctas_per_sm)
+        self.md = _Engine(md_tuning)
         self.waiting = []  # arrived or future requests, not yet admitted
         self.done = []
         self.iterations = 0
