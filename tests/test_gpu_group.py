@@ -153,3 +153,6 @@ def test_bitexact_against_reference_build(rng, interpolated):
         np.testing.assert_array_equal(mine[1], theirs[1].reshape(mine[1].shape), err_msg=f"du_dp lambda={lam}")
         assert mine[2].sum(dtype=np.uint64) == theirs[2].sum(dtype=np.uint64)
         assert mine[3].sum(dtype=np.uint64) == theirs[3].sum(dtype=np.uint64)
+        # forces only: the packed two-rows-per-lane sweep, with the group's rows ending mid row group
+        forces = g._execute_fixed(s.x, params, s.box, lam, True, False, False, False)
+        np.testing.assert_array_equal(forces[0], theirs[0], err_msg=f"forces-only du_dx lambda={lam}")
