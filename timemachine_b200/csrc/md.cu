@@ -471,20 +471,26 @@ class Context {
         CK(cudaPeekAtLastError());
     }
 
-    cudaGraphExec_t graph_for(int kind, double lambda, unsigned long long *dl_out) {
-        const auto key = std::make_tuple(kind, lambda, (const void *)dl_out);
+    // kind 0: one step (du_dl into dl_out if given); 1: the barostat move;
+    // 2: `steps` steps.
+    cudaGraphExec_t graph_for(int kind, double lambda, unsigned long long *dl_out, int steps = 1) {
+        const auto key = std::make_tuple(kind, lambda, (const void *)dl_out, steps);
         auto it = graphs_.find(key);
         if (it != graphs_.end()) {
             return it->second;
         }
         cudaGraph_t g;
-        if (kind == 0 && bps_.size() > 1) {
+        if (kind != 1 && bps_.size() > 1) {
             ensure_branches(bps_.size() - 1); // created outside the capture
         }
         CK(cudaStreamBeginCapture(stream_, cudaStreamCaptureModeRelaxed));
         try {
             if (kind == 0) {
                 record_step(lambda, dl_out, true);
+            } else if (kind == 2) {
+                for (int k = 0; k < steps; k++) {
+                    record_step(lambda, nullptr, true);
+                }
             } else {
                 record_barostat(lambda);
             }
@@ -523,11 +529,29 @@ class Context {
             CK(cudaMemcpyAsync(&st_.p->dl_slot, &zero, sizeof(int), cudaMemcpyHostToDevice, stream_));
         }
         int frame = 0;
-        for (int i = 1; i <= n_steps; i++) {
+        const bool store_x = x_interval > 0 && x_out_host;
+        for (int i = 1; i <= n_steps;) {
             const double lam = lambdas[i - 1];
             unsigned long long *dl_slot_base = (dl_interval > 0 && i % dl_interval == 0) ? dl_dev.p : nullptr;
-            advance(lam, dl_slot_base, use_graphs);
-            if (x_interval > 0 && i % x_interval == 0 && x_out_host) {
+            // Replayed steps run in chunks of up to MAX_GRAPH_STEPS steps per
+            // graph: the same lambda, no du_dl store inside, frames and the
+            // barostat move only after the chunk's last step.
+            int L = 1;
+            if (use_graphs && !dl_slot_base) {
+                const int baro_left = has_baro_ ? baro_interval_ - (int)(baro_step_ % baro_interval_) : MAX_GRAPH_STEPS;
+                while (L < MAX_GRAPH_STEPS && L < baro_left && i + L <= n_steps && lambdas[i + L - 1] == lam &&
+                       !(dl_interval > 0 && (i + L) % dl_interval == 0) && !(store_x && (i + L - 1) % x_interval == 0)) {
+                    L++;
+                }
+            }
+            if (L > 1) {
+                CK(cudaGraphLaunch(graph_for(2, lam, nullptr, L), stream_));
+                barostat_after(lam, L, use_graphs);
+            } else {
+                advance(lam, dl_slot_base, use_graphs);
+            }
+            i += L;
+            if (store_x && (i - 1) % x_interval == 0) {
                 store_frame(frame, x_out_host, box_out_host);
                 frame++;
             }
@@ -694,8 +718,14 @@ class Context {
         } else {
             record_step(lam, dl_slot_base);
         }
+        barostat_after(lam, 1, use_graphs);
+    }
+
+    // The barostat's step count after `steps` integrator steps, and its move
+    // when the count reaches the interval.
+    void barostat_after(double lam, int steps, bool use_graphs) {
         if (has_baro_) {
-            baro_step_++;
+            baro_step_ += steps;
             if (baro_step_ % baro_interval_ == 0) {
                 if (use_graphs) {
                     CK(cudaGraphLaunch(graph_for(1, lam, nullptr), stream_));
@@ -737,7 +767,8 @@ class Context {
     DevBuf<MDState> st_;
     std::vector<std::unique_ptr<BoundPot>> bps_;
     cudaStream_t stream_ = nullptr;
-    std::map<std::tuple<int, double, const void *>, cudaGraphExec_t> graphs_;
+    std::map<std::tuple<int, double, const void *, int>, cudaGraphExec_t> graphs_;
+    static constexpr int MAX_GRAPH_STEPS = 25; // steps captured in one graph at most
     std::vector<cudaStream_t> side_;
     std::vector<cudaEvent_t> join_ev_;
     cudaEvent_t fork_ev_ = nullptr;
