@@ -605,8 +605,24 @@ class Context {
             CK(cudaMemsetAsync(u_win.p, 0, u_win.n * sizeof(unsigned long long), stream_));
         }
         int frame = 0;
-        for (int i = 1; i <= n_steps; i++) {
-            advance(lambda, nullptr, use_graphs);
+        for (int i = 1; i <= n_steps;) {
+            // replayed steps in chunks (as in multiple_steps) that end at the
+            // next frame, energy sample or barostat move
+            int L = 1;
+            if (use_graphs) {
+                const int baro_left = has_baro_ ? baro_interval_ - (int)(baro_step_ % baro_interval_) : MAX_GRAPH_STEPS;
+                while (L < MAX_GRAPH_STEPS && L < baro_left && i + L <= n_steps && (i + L - 1) % x_interval != 0 &&
+                       (i + L - 1) % u_interval != 0) {
+                    L++;
+                }
+            }
+            if (L > 1) {
+                CK(cudaGraphLaunch(graph_for(2, lambda, nullptr, L), stream_));
+                barostat_after(lambda, L, use_graphs);
+            } else {
+                advance(lambda, nullptr, use_graphs);
+            }
+            i += L - 1; // the chunk's last step
             if (i % x_interval == 0 && x_out_host) {
                 store_frame(frame, x_out_host, box_out_host);
                 frame++;
@@ -624,6 +640,7 @@ class Context {
                     CK(cudaPeekAtLastError());
                 }
             }
+            i++;
         }
         if (n_u > 0 && K > 0 && u_out_host) {
             std::vector<unsigned long long> h((size_t)n_u * K);
