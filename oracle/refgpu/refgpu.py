@@ -1,4 +1,4 @@
-"""ctypes wrapper of the reference timemachine CUDA build (TEST/BASELINE INFRASTRUCTURE).
+"""ctypes wrapper of the reference timemachine CUDA build (TEST INFRASTRUCTURE; also timed by the reference arm of bench.py).
 
 Loads oracle/_ref/libtmref.so (built from the reference sources by
 oracle/refgpu/Makefile) for the bit-exact parity tests and for bench.py's

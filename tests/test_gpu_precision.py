@@ -26,7 +26,7 @@ pytestmark = pytest.mark.gpu
 
 needs_ref = pytest.mark.skipif(not refgpu.available(), reason="reference CUDA build (oracle/_ref) not present")
 
-# north-star force bar for the FP64 path against the FP64 oracle
+# force bar (1e-5, relative to max(|F|, 1)) of the FP64 path against the FP64 oracle
 FORCE_BAR_F64 = 1e-5
 
 
