@@ -98,6 +98,23 @@ def test_rebuild_cadence_graph_and_eager_agree(n_waters, edge, dt):
         assert r[4] == ref[4]
 
 
+def test_multi_step_graphs_with_frames_equal_eager():
+    """Graph replay runs the steps between frames, du_dl samples and barostat
+    moves as one captured graph per run (intervals 10, 7 and 25 do not line
+    up); the frames, du_dl samples and final state equal eager steps bit for
+    bit."""
+    s = testsystems.build_system(500, 2.9, seed=13, n_ligand=10)
+    lam = np.full(100, 0.4)
+    runs = []
+    for use_graphs in (True, False):
+        ctx, _ = _context(s, use_graphs, dt=2.0e-3, barostat_interval=25)
+        dl, xs, boxes = ctx.multiple_steps(lam, store_du_dl_interval=7, store_x_interval=10)
+        runs.append((dl, xs, boxes, ctx.get_x_t(), ctx.get_v_t(), ctx.get_box()))
+    assert runs[0][1].shape == (10, s.N, 3)
+    for a, b in zip(runs[0], runs[1]):
+        np.testing.assert_array_equal(a, b)
+
+
 def test_single_step_follows_baoab_update():
     """Zero temperature (no noise): x1, v1 equal the BAOAB update of
     timemachine/cpp/src/integrator.cu:37-69 with the potential's forces."""
