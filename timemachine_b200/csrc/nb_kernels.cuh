@@ -1586,9 +1586,9 @@ __device__ __forceinline__ void flush_row_rg(
 // fixed-point conversions stay per component, and the row and column forces
 // of a pair are converted once, as in pair_terms. The packed operations
 // (fmul2 and the others, nb_pair_math.cuh) are inline PTX, so a product
-// followed by a sum keeps both roundings. (The all-outputs variants keep the one-row
-// sweep: with two rows per lane they need 127 registers, 4 CTAs/SM, and the
-// 12-window call measured 2 % slower.)
+// followed by a sum keeps both roundings. (The all-outputs variants keep the
+// one-row sweep: with two rows per lane they need 127 registers, 4 CTAs/SM,
+// and the 12-window call measured 2 % slower.)
 // ---------------------------------------------------------------------------
 struct RowForces {
     unsigned long long x = 0, y = 0, z = 0;
