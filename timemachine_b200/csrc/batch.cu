@@ -440,10 +440,10 @@ __global__ void __launch_bounds__(
             for (int t = 0; t < it.z; t++) {
                 const long long tile = (long long)it.y + t;
                 const unsigned j = r.tile_cols[tile * TILE + lane];
-                tile_forces_p2(a, lane, S, ia, j, 0, a.acc, box_x, box_y, box_z, inv_box_x, inv_box_y, inv_box_z,
+                tile_forces_p2<U, DX>(a, lane, S, ia, j, 0, a.acc, box_x, box_y, box_z, inv_box_x, inv_box_y, inv_box_z,
                                cutoff_squared, beta, A, B);
             }
-            flush_forces_p2(a.acc, ia, S, A, B);
+            flush_forces_p2<U, DX>(a.acc, ia, S, A, B);
             continue;
         }
         const unsigned i = (unsigned)(it.x * RG + (lane & (RG - 1)));

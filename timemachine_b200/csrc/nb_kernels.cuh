@@ -42,6 +42,11 @@ constexpr int TILE = 32;
 #ifndef TMNB_PACKED_FORCES_CTAS
 #define TMNB_PACKED_FORCES_CTAS 6
 #endif
+// Energy-only FP32 evaluations of 16-row tiles (the barostat's) use the same
+// packed sweep.
+#ifndef TMNB_PACKED_ENERGY
+#define TMNB_PACKED_ENERGY 1
+#endif
 // The one-row sweep evaluates the independent x / y steps of a pair (minimum
 // image, force components) and the paired charge / epsilon derivatives in
 // the two components of packed FP32x2 operations.
@@ -1590,11 +1595,13 @@ __device__ __forceinline__ void flush_row_rg(
 // one-row sweep: with two rows per lane they need 127 registers, 4 CTAs/SM,
 // and the 12-window call measured 2 % slower.)
 // ---------------------------------------------------------------------------
+// Row accumulators of the packed sweep: forces and energy.
 struct RowForces {
-    unsigned long long x = 0, y = 0, z = 0;
+    unsigned long long x = 0, y = 0, z = 0, u = 0;
 };
 
-template <bool ALCH, bool CHECK>
+// U: energy; DX: forces (one of them or both).
+template <bool U, bool DX, bool ALCH, bool CHECK>
 __device__ __forceinline__ void sweep_forces_p2(
     const int lane,
     const unsigned S,
@@ -1665,15 +1672,23 @@ __device__ __forceinline__ void sweep_forces_p2(
             poly = madd2(poly, t, f2(-0.284496736f), TMNB_DAG_POLY);
             poly = madd2(poly, t, f2(0.254829592f), TMNB_DAG_POLY);
             const float2 pt = fmul2(poly, t);
-            const float2 cbd = fmul2(f2(static_cast<float>(1.128379167095512595889238330988549829708)), bd);
+            const float2 erfc_bd = fmul2(pt, e);
+            float2 pre = f2(0.0f);
+            if (DX) {
+                const float2 cbd = fmul2(f2(static_cast<float>(1.128379167095512595889238330988549829708)), bd);
 #if TMNB_DAG_ERF == 1
-            const float2 s = ffma2(cbd, e, fmul2(pt, e));
+                const float2 s = ffma2(cbd, e, erfc_bd);
 #elif TMNB_DAG_ERF == 0
-            const float2 s = fadd2(fmul2(cbd, e), fmul2(pt, e));
+                const float2 s = fadd2(fmul2(cbd, e), erfc_bd);
 #else
-            const float2 s = ffma2(pt, e, fmul2(cbd, e));
+                const float2 s = ffma2(pt, e, fmul2(cbd, e));
 #endif
-            float2 pre = fmul2(qij_inv, fmul2(make_float2(-inv_d2.x, -inv_d2.y), s));
+                pre = fmul2(qij_inv, fmul2(make_float2(-inv_d2.x, -inv_d2.y), s));
+            }
+            float2 u = f2(0.0f);
+            if (U) {
+                u = fmul2(qij_inv, erfc_bd);
+            }
             // Lennard-Jones where both atoms carry epsilon (per pair)
             const bool lj_a = eps_i.x != 0 && eps_j != 0;
             const bool lj_b = eps_i.y != 0 && eps_j != 0;
@@ -1684,22 +1699,50 @@ __device__ __forceinline__ void sweep_forces_p2(
                 const float2 s2 = fmul2(s1, s1);
                 const float2 s4 = fmul2(s2, s2);
                 const float2 s6 = fmul2(s4, s2);
-                const float2 ljx = fmul2(eps_ij, fmul2(s6, inv_d2));
-                const float2 ljy = madd2(s6, f2(48.0f), f2(-24.0f), TMNB_DAG_LJP);
+                if (DX) {
+                    const float2 ljx = fmul2(eps_ij, fmul2(s6, inv_d2));
+                    const float2 ljy = madd2(s6, f2(48.0f), f2(-24.0f), TMNB_DAG_LJP);
 #if TMNB_DAG_PRE == 1
-                const float2 pre_lj = ffma2(make_float2(-ljx.x, -ljx.y), ljy, pre);
+                    const float2 pre_lj = ffma2(make_float2(-ljx.x, -ljx.y), ljy, pre);
 #elif TMNB_DAG_PRE == 0
-                const float2 pre_lj = fsub2(pre, fmul2(ljx, ljy));
+                    const float2 pre_lj = fsub2(pre, fmul2(ljx, ljy));
 #else
 #error "TMNB_DAG_PRE == 2 has no packed form"
 #endif
-                pre = make_float2(lj_a ? pre_lj.x : pre.x, lj_b ? pre_lj.y : pre.y);
+                    pre = make_float2(lj_a ? pre_lj.x : pre.x, lj_b ? pre_lj.y : pre.y);
+                }
+                if (U) {
+                    // lennard_jones of nb_pair_math.cuh: A = (4 eps_ij)(s6 - 1), u += A s6
+#if TMNB_DAG_S6M1
+                    const float2 s6m1 = ffma2(s4, s2, f2(-1.0f));
+#else
+                    const float2 s6m1 = fsub2(s6, f2(1.0f));
+#endif
+                    const float2 Acoef = fmul2(fmul2(f2(4.0f), eps_ij), s6m1);
+#if TMNB_DAG_U == 1
+                    const float2 u_lj = ffma2(Acoef, s6, u);
+#elif TMNB_DAG_U == 0
+                    const float2 u_lj = fadd2(u, fmul2(Acoef, s6));
+#else
+                    const float2 u_lj = ffma2(qij_inv, erfc_bd, fmul2(Acoef, s6));
+#endif
+                    u = make_float2(lj_a ? u_lj.x : u.x, lj_b ? u_lj.y : u.y);
+                }
+            }
+            if (U) {
+                const float2 yu = fmul2(u, f2(static_cast<float>(FX_EXPONENT)));
+                if (in_a) {
+                    A.u += fixed_round(yu.x);
+                }
+                if (in_b) {
+                    B.u += fixed_round(yu.y);
+                }
             }
             const float2 ex = f2(static_cast<float>(FX_EXPONENT));
             const float2 yx = fmul2(fmul2(pre, dx), ex);
             const float2 yy = fmul2(fmul2(pre, dy), ex);
             const float2 yz = fmul2(fmul2(pre, dz), ex);
-            if (in_a) {
+            if (DX && in_a) {
                 const unsigned long long fx = fixed_round(yx.x), fy = fixed_round(yy.x), fz = fixed_round(yz.x);
                 A.x += fx;
                 A.y += fy;
@@ -1713,7 +1756,7 @@ __device__ __forceinline__ void sweep_forces_p2(
                     gj_z += fixed_round(-yz.x) + fz;
                 }
             }
-            if (in_b) {
+            if (DX && in_b) {
                 const unsigned long long fx = fixed_round(yx.y), fy = fixed_round(yy.y), fz = fixed_round(yz.y);
                 B.x += fx;
                 B.y += fy;
@@ -1740,14 +1783,17 @@ __device__ __forceinline__ void sweep_forces_p2(
         if (ALCH) {
             cj_w = __shfl_sync(FULL_MASK, cj_w, src);
         }
-        gj_x = __shfl_sync(FULL_MASK, gj_x, src);
-        gj_y = __shfl_sync(FULL_MASK, gj_y, src);
-        gj_z = __shfl_sync(FULL_MASK, gj_z, src);
+        if (DX) {
+            gj_x = __shfl_sync(FULL_MASK, gj_x, src);
+            gj_y = __shfl_sync(FULL_MASK, gj_y, src);
+            gj_z = __shfl_sync(FULL_MASK, gj_z, src);
+        }
     }
 }
 
-// One 16-row tile of a forces-only evaluation, window `window`: the lane's
-// rows ia and ia + 8 against column slot j.
+// One 16-row tile of a forces and / or energy evaluation (U, DX), window
+// `window`: the lane's rows ia and ia + 8 against column slot j.
+template <bool U, bool DX>
 __device__ __forceinline__ void tile_forces_p2(
     const PairArgs &a,
     const int lane,
@@ -1778,9 +1824,9 @@ __device__ __forceinline__ void tile_forces_p2(
     const float4 prb = b_ok ? a.prm[wo + ib] : make_float4(0.f, 0.f, 0.f, 0.f);
     const float4 pwj = col_ok ? a.posw[wo + j] : make_float4(nan, nan, nan, 0.f);
     const float4 prj = col_ok ? a.prm[wo + j] : make_float4(0.f, 0.f, 0.f, 0.f);
-    // Forces depend on the parameters' lambda derivatives only through w: a
-    // tile whose w are all zero adds dw*dw = 0 exactly, so it skips the 4th
-    // dimension whatever the interpolated parameters do.
+    // Forces and energies depend on the parameters' lambda derivatives only
+    // through w: a tile whose w are all zero adds dw*dw = 0 exactly, so it
+    // skips the 4th dimension whatever the interpolated parameters do.
     const bool alch = __any_sync(FULL_MASK, pwa.w != 0.f || pwb.w != 0.f || pwj.w != 0.f);
     const unsigned ia_eff = a_ok ? ia : 0xffffffffu;
     const unsigned ib_eff = b_ok ? ib : 0xffffffffu;
@@ -1788,7 +1834,7 @@ __device__ __forceinline__ void tile_forces_p2(
     const bool check = __any_sync(FULL_MASK, col_ok && j < row_first + 16);
     unsigned long long gj_x = 0, gj_y = 0, gj_z = 0;
 #define TMB_SWEEP_P2(ALCH_, CHECK_)                                                                                    \
-    sweep_forces_p2<ALCH_, CHECK_>(                                                                                     \
+    sweep_forces_p2<U, DX, ALCH_, CHECK_>(                                                                              \
         lane, S, ia_eff, ib_eff, j, make_float2(pwa.x, pwb.x), make_float2(pwa.y, pwb.y), make_float2(pwa.z, pwb.z),   \
         make_float2(pwa.w, pwb.w), make_float2(pra.x, prb.x), make_float2(pra.y, prb.y), make_float2(pra.z, prb.z),   \
         pwj.x, pwj.y, pwj.z, pwj.w, prj.x, prj.y, prj.z, f2(-box_x), f2(-box_y), f2(-box_z), f2(inv_box_x),           \
@@ -1807,7 +1853,7 @@ __device__ __forceinline__ void tile_forces_p2(
         }
     }
 #undef TMB_SWEEP_P2
-    if (col_ok) {
+    if (DX && col_ok) {
         red_add(acc_out.x + j, gj_x);
         red_add(acc_out.y + j, gj_y);
         red_add(acc_out.z + j, gj_z);
@@ -1816,29 +1862,46 @@ __device__ __forceinline__ void tile_forces_p2(
 
 // Row sums of a packed sweep: the four lanes holding rows ia / ia + 8
 // (lanes l, l^8, l^16, l^24) combine, and lanes 0-7 flush.
+template <bool U, bool DX>
 __device__ __forceinline__ void flush_forces_p2(const Accum &acc_out, unsigned ia, unsigned row_end, RowForces A,
                                                 RowForces B) {
 #pragma unroll
     for (int o = 8; o < TILE; o <<= 1) {
-        A.x += __shfl_xor_sync(FULL_MASK, A.x, o);
-        A.y += __shfl_xor_sync(FULL_MASK, A.y, o);
-        A.z += __shfl_xor_sync(FULL_MASK, A.z, o);
-        B.x += __shfl_xor_sync(FULL_MASK, B.x, o);
-        B.y += __shfl_xor_sync(FULL_MASK, B.y, o);
-        B.z += __shfl_xor_sync(FULL_MASK, B.z, o);
+        if (DX) {
+            A.x += __shfl_xor_sync(FULL_MASK, A.x, o);
+            A.y += __shfl_xor_sync(FULL_MASK, A.y, o);
+            A.z += __shfl_xor_sync(FULL_MASK, A.z, o);
+            B.x += __shfl_xor_sync(FULL_MASK, B.x, o);
+            B.y += __shfl_xor_sync(FULL_MASK, B.y, o);
+            B.z += __shfl_xor_sync(FULL_MASK, B.z, o);
+        }
+        if (U) {
+            A.u += __shfl_xor_sync(FULL_MASK, A.u, o);
+            B.u += __shfl_xor_sync(FULL_MASK, B.u, o);
+        }
     }
     if ((threadIdx.x & (TILE - 1)) >= 8) {
         return;
     }
     if (ia < row_end) {
-        red_add(acc_out.x + ia, A.x);
-        red_add(acc_out.y + ia, A.y);
-        red_add(acc_out.z + ia, A.z);
+        if (DX) {
+            red_add(acc_out.x + ia, A.x);
+            red_add(acc_out.y + ia, A.y);
+            red_add(acc_out.z + ia, A.z);
+        }
+        if (U) {
+            red_add(acc_out.u + ia, A.u);
+        }
     }
     if (ia + 8 < row_end) {
-        red_add(acc_out.x + ia + 8, B.x);
-        red_add(acc_out.y + ia + 8, B.y);
-        red_add(acc_out.z + ia + 8, B.z);
+        if (DX) {
+            red_add(acc_out.x + ia + 8, B.x);
+            red_add(acc_out.y + ia + 8, B.y);
+            red_add(acc_out.z + ia + 8, B.z);
+        }
+        if (U) {
+            red_add(acc_out.u + ia + 8, B.u);
+        }
     }
 }
 
@@ -1888,18 +1951,33 @@ static __global__ void k_dep_tiles(DepArgs a, DevState *state) {
 // MULTI (K > 1 windows): the tile items skip lambda-dependent tiles and add
 // into the shared accumulator block; each (tile, window) unit adds into the
 // window's block; a lambda-dependent scaled pair is evaluated for every window.
+// CTAs per SM the compiler must fit for each pair-kernel variant (its
+// register budget): measured on B200, see the kernel below.
+template <typename Real, bool U, bool DX, bool DL, bool DP, bool INTERP, int RG>
+constexpr int pair_min_ctas() {
+    if (sizeof(Real) != 4) {
+        return 5;
+    }
+    if (U && DX && DL && DP && !INTERP) {
+        return 6;
+    }
+    if (DX && !U && !DL && !DP) {
+        return (TMNB_PACKED_FORCES && RG == 16) ? TMNB_PACKED_FORCES_CTAS : 8;
+    }
+    if (U && !DX && !DL && !DP && TMNB_PACKED_FORCES && TMNB_PACKED_ENERGY && RG == 16) {
+        return TMNB_PACKED_FORCES_CTAS;
+    }
+    return 1;
+}
+
 template <typename Real, bool U, bool DX, bool DL, bool DP, bool INTERP, bool MULTI, int RG = TILE>
 // Occupancy, measured on B200: all four outputs at 6 CTAs/SM (80 registers,
-// no spills; 12-window call -3.5 % against 5), forces only at 8 (64). FP64
+// no spills; 12-window call -3.5 % against 5); forces only or energy only
+// with the packed two-rows sweep at 6 (80), forces only with 8 or 32 rows per
+// tile at 8 (64). FP64
 // variants at 5 (96 registers, a few spilled words): the 12-window call
 // took 0.407 ms against 0.455 ms at the compiler's 154 registers (3 CTAs).
-__global__ void __launch_bounds__(
-    128,
-    sizeof(Real) != 4 ? 5
-                      : ((U && DX && DL && DP && !INTERP) ? 6
-                                                          : ((DX && !U && !DL && !DP) ? (TMNB_PACKED_FORCES && RG == 16 ? TMNB_PACKED_FORCES_CTAS : 8)
-                                                                                      : 1)))
-    k_pair(PairArgs a) {
+__global__ void __launch_bounds__(128, (pair_min_ctas<Real, U, DX, DL, DP, INTERP, RG>())) k_pair(PairArgs a) {
     grid_dependency_wait();
     if (a.state->error) {
         return;
@@ -1923,7 +2001,8 @@ __global__ void __launch_bounds__(
     const int n_tiles_units = n_items + n_dep_units;
     const int n_total = n_tiles_units + (a.M + TILE - 1) / TILE;
     // forces-only FP32 evaluations of 16-row tiles take the packed sweep
-    constexpr bool PACKED = TMNB_PACKED_FORCES && sizeof(Real) == 4 && RG == 16 && DX && !U && !DL && !DP;
+    constexpr bool PACKED =
+        TMNB_PACKED_FORCES && sizeof(Real) == 4 && RG == 16 && !DL && !DP && ((DX && !U) || (U && !DX && TMNB_PACKED_ENERGY));
 
     for (;;) {
         int item = 0;
@@ -1965,9 +2044,9 @@ __global__ void __launch_bounds__(
                 const unsigned j = a.tile_cols[(long long)dt.y * TILE + lane];
                 const Accum wk = acc_block(a.acc, a.acc_block, 1 + k);
                 RowForces A, B;
-                tile_forces_p2(a, lane, S, ia, j, k, wk, box_x, box_y, box_z, inv_box_x, inv_box_y, inv_box_z,
+                tile_forces_p2<U, DX>(a, lane, S, ia, j, k, wk, box_x, box_y, box_z, inv_box_x, inv_box_y, inv_box_z,
                                cutoff_squared, beta, A, B);
-                flush_forces_p2(wk, ia, (unsigned)a.row_end, A, B);
+                flush_forces_p2<U, DX>(wk, ia, (unsigned)a.row_end, A, B);
                 continue;
             }
             const int4 it = a.items[item];
@@ -1981,10 +2060,10 @@ __global__ void __launch_bounds__(
                 if (MULTI && __any_sync(FULL_MASK, row_dep || (j < S && a.lamdep[j]))) {
                     continue; // evaluated per window by the (tile, window) units
                 }
-                tile_forces_p2(a, lane, S, ia, j, 0, a.acc, box_x, box_y, box_z, inv_box_x, inv_box_y, inv_box_z,
+                tile_forces_p2<U, DX>(a, lane, S, ia, j, 0, a.acc, box_x, box_y, box_z, inv_box_x, inv_box_y, inv_box_z,
                                cutoff_squared, beta, A, B);
             }
-            flush_forces_p2(a.acc, ia, (unsigned)a.row_end, A, B);
+            flush_forces_p2<U, DX>(a.acc, ia, (unsigned)a.row_end, A, B);
             continue;
         }
         if (MULTI && item >= n_items) {
