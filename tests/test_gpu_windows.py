@@ -67,6 +67,9 @@ def test_interpolated_windows_equal_single_window(name):
     ).unbound_impl(np.float32)
     lams = np.array([0.0, float(g["lam"]), 0.33, 0.5, 1.0])
     _assert_windows_equal(impl, g["x"], g["params"], g["box"], lams)
+    # forces only and energy only: the packed two-rows sweep, per-window units included
+    _assert_windows_equal(impl, g["x"], g["params"], g["box"], lams, (True, False, False, False))
+    _assert_windows_equal(impl, g["x"], g["params"], g["box"], lams, (False, False, False, True))
 
 
 def test_windows_follow_changed_lambda_dependence_without_rebuild():
