@@ -885,7 +885,7 @@ def run_batch_form():
         repeats=1,
         candidates=[
             dict(chunk=c, padding=p, grid_bits_offset=0, pair_ctas_per_sm=0, rows=r)
-            for r in (8, 16, 32) for c in (1, 2, 4, 8) for p in (0.06, 0.1)
+            for r in (8, 16, 32) for c in (8, 16, 32, 64, 128) for p in (0.06, 0.1)
         ],
     )
     t_eval = timed(lambda: b.evaluate(), 3)
@@ -963,7 +963,7 @@ def run_batch_form():
         repeats=1,
         candidates=[
             dict(chunk=c, padding=p, grid_bits_offset=0, pair_ctas_per_sm=0, rows=r)
-            for r in (8, 16, 32) for c in (1, 2, 4, 8) for p in (0.06, 0.1)
+            for r in (8, 16, 32) for c in (8, 16, 32, 64, 128) for p in (0.06, 0.1)
         ],
     )
     t_md = timed(lambda: b.md(BATCH_CHUNK, chunk=BATCH_CHUNK, use_graph=True), 1)
