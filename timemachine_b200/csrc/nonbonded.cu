@@ -24,6 +24,11 @@
 #include <string>
 #include <vector>
 
+// Tiles per work item of lists built by single-window calls.
+#ifndef TMNB_SINGLE_CHUNK
+#define TMNB_SINGLE_CHUNK 2
+#endif
+
 namespace tmb {
 
 enum class Kind { AllPairs, PairList, Nonbonded, Group };
@@ -640,10 +645,11 @@ class NonbondedPotential : public PotentialBase {
         ta.tile_cols = tile_cols_.p;
         ta.rb_ntiles = rb_ntiles_.p;
         ta.items = items_.p;
-        // tiles per work item, measured on B200 at 22,840 atoms: one for a
-        // single window (a finer tail: -8 % per MD step, -10 % per call), four
-        // for several windows (fewer row flushes: -3 %)
-        ta.chunk = K > 1 ? 4 : 1;
+        // tiles per work item, measured on B200 at 22,840 atoms: two for a
+        // single window with the packed forces sweep (MD step 125.7 -> 121.3
+        // us against one; one had been -8 % against four with the one-row
+        // sweep), four for several windows (fewer row flushes: -3 %)
+        ta.chunk = K > 1 ? 4 : TMNB_SINGLE_CHUNK;
         const DevState *cst = state_.p;
         launch_dependent(k_bin_keys, dim3(sgrid), dim3(tpb), 0, stream, sa, cst);
         launch_dependent(k_bin_scan, dim3(1), dim3(1024), 0, stream, sa, state_.p);
