@@ -28,6 +28,10 @@
 #ifndef TMNB_SINGLE_CHUNK
 #define TMNB_SINGLE_CHUNK 2
 #endif
+// Tiles per work item of lists built by multi-window calls.
+#ifndef TMNB_MULTI_CHUNK
+#define TMNB_MULTI_CHUNK 4
+#endif
 
 namespace tmb {
 
@@ -649,7 +653,7 @@ class NonbondedPotential : public PotentialBase {
         // single window with the packed forces sweep (MD step 125.7 -> 121.3
         // us against one; one had been -8 % against four with the one-row
         // sweep), four for several windows (fewer row flushes: -3 %)
-        ta.chunk = K > 1 ? 4 : TMNB_SINGLE_CHUNK;
+        ta.chunk = K > 1 ? TMNB_MULTI_CHUNK : TMNB_SINGLE_CHUNK;
         const DevState *cst = state_.p;
         launch_dependent(k_bin_keys, dim3(sgrid), dim3(tpb), 0, stream, sa, cst);
         launch_dependent(k_bin_scan, dim3(1), dim3(1024), 0, stream, sa, state_.p);
