@@ -66,9 +66,11 @@ __global__ void k_langevin(
         s_step = st->step;
     }
     __syncthreads();
-    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    // two threads per atom (halves of its Philox draws and components)
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = t >> 1;
     if (i < N) {
-        langevin_atom(i, s_step, key, ca, cbs[i], ccs[i], dt, x, v, du_dx);
+        langevin_atom_half(i, t & 1, s_step, key, ca, cbs[i], ccs[i], dt, x, v, du_dx);
     }
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -445,7 +447,7 @@ class Context {
         }
         const int tpb = 128;
         launch_dependent(
-            k_langevin, dim3((N_ + tpb - 1) / tpb), dim3(tpb), 0, stream_, N_, ca_, (const double *)cbs_.p,
+            k_langevin, dim3((2 * N_ + tpb - 1) / tpb), dim3(tpb), 0, stream_, N_, ca_, (const double *)cbs_.p,
             (const double *)ccs_.p, dt_, x_.p, v_.p, du_dx_.p, key_, st_.p);
         CK(cudaPeekAtLastError());
     }

@@ -39,6 +39,26 @@ __device__ __forceinline__ double2 normal2(unsigned a, unsigned b, unsigned c, u
     return make_double2(r * co, r * s);
 }
 
+// One component's update with its noise; the force accumulator is zeroed for
+// the next step.
+__device__ __forceinline__ void langevin_dim(
+    int k,
+    double noise,
+    double ca,
+    double cb,
+    double cc,
+    double dt,
+    double *__restrict__ x,
+    double *__restrict__ v,
+    unsigned long long *__restrict__ du_dx) {
+    const double force = static_cast<double>(static_cast<long long>(du_dx[k])) / FX_EXPONENT;
+    const double v_mid = v[k] + cb * force;
+    const double v_new = ca * v_mid + cc * noise;
+    v[k] = v_new;
+    x[k] += 0.5 * dt * (v_mid + v_new);
+    du_dx[k] = 0; // the next step accumulates from zero
+}
+
 // One atom's update: v_mid = v + cb * F, v' = ca * v_mid + cc * noise,
 // x' = x + dt/2 * (v_mid + v'); the force accumulator is zeroed for the next
 // step. Noise: Philox keyed by `key`, counter (atom, step).
@@ -60,13 +80,32 @@ __device__ __forceinline__ void langevin_atom(
     const double noise[3] = {n01.x, n01.y, n23.x};
 #pragma unroll
     for (int d = 0; d < 3; d++) {
-        const int k = 3 * i + d;
-        const double force = static_cast<double>(static_cast<long long>(du_dx[k])) / FX_EXPONENT;
-        const double v_mid = v[k] + cb * force;
-        const double v_new = ca * v_mid + cc * noise[d];
-        v[k] = v_new;
-        x[k] += 0.5 * dt * (v_mid + v_new);
-        du_dx[k] = 0; // the next step accumulates from zero
+        langevin_dim(3 * i + d, noise[d], ca, cb, cc, dt, x, v, du_dx);
+    }
+}
+
+// The same update split over two threads: half 0 draws the first Philox
+// block and updates x and y, half 1 the second block and z (the same numbers
+// and arithmetic per component as langevin_atom).
+__device__ __forceinline__ void langevin_atom_half(
+    int i,
+    int half,
+    unsigned long long step,
+    uint2 key,
+    double ca,
+    double cb,
+    double cc,
+    double dt,
+    double *__restrict__ x,
+    double *__restrict__ v,
+    unsigned long long *__restrict__ du_dx) {
+    const uint4 r = philox4x32_10(make_uint4((unsigned)i, (unsigned)step, (unsigned)(step >> 32), (unsigned)half), key);
+    const double2 n = normal2(r.x, r.y, r.z, r.w);
+    if (half == 0) {
+        langevin_dim(3 * i + 0, n.x, ca, cb, cc, dt, x, v, du_dx);
+        langevin_dim(3 * i + 1, n.y, ca, cb, cc, dt, x, v, du_dx);
+    } else {
+        langevin_dim(3 * i + 2, n.x, ca, cb, cc, dt, x, v, du_dx);
     }
 }
 
