@@ -66,6 +66,7 @@ struct DevState {
     int n_dep;            // lambda-dependent tiles listed by k_dep_tiles (multi-window calls)
     int dep_dirty;        // 1: the list of lambda-dependent tiles must be redone (rebuild, or lamdep changed)
     int items_chunk;      // tiles per work item in the list of the last rebuild
+    int item_count;       // work items reserved so far by the rebuild in progress (0 between rebuilds)
 };
 
 // Error codes written into DevState::error (mirrored in include/tmnb.h).
@@ -878,13 +879,25 @@ __device__ __forceinline__ void build_tiles_cta(const TileArgs &a, const int rb,
                                 (unsigned)S, a.prm);
         }
         __syncwarp();
+        const int total = tile_count + (n + TILE - 1) / TILE;
+        // the group's work items, at a range reserved from the list's
+        // counter (items are in any order: the pair kernel schedules them
+        // dynamically and its sums do not depend on the order)
+        const int ni = (total + a.chunk - 1) / a.chunk;
+        int first_item = 0;
         if (lane == 0) {
-            const int total = tile_count + (n + TILE - 1) / TILE;
             a.rb_ntiles[rb] = total;
             atomicAdd(&state->total_tiles, (unsigned)total);
+            first_item = atomicAdd(&state->item_count, ni);
+        }
+        first_item = __shfl_sync(FULL_MASK, first_item, 0);
+        const long long first_tile = tile_base(a, rb);
+        for (int c = lane; c < ni; c += TILE) {
+            const int first = c * a.chunk;
+            a.items[first_item + c] = make_int4(rb, (int)(first_tile + first), min(a.chunk, total - first), 0);
         }
     }
-    // the last CTA to finish builds the work-item list
+    // the last CTA to finish publishes the list
     __threadfence();
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -895,49 +908,10 @@ __device__ __forceinline__ void build_tiles_cta(const TileArgs &a, const int rb,
     if (!is_last) {
         return;
     }
-    __threadfence();
-    __shared__ int carry;
-    __shared__ int wsum[TB_WARPS];
     if (threadIdx.x == 0) {
-        carry = 0;
-    }
-    __syncthreads();
-    for (int base = 0; base < a.n_row_blocks; base += blockDim.x) {
-        const int r = base + threadIdx.x;
-        const int nt = r < a.n_row_blocks ? *((volatile int *)&a.rb_ntiles[r]) : 0;
-        const int ni = (nt + a.chunk - 1) / a.chunk;
-        int incl = ni;
-        for (int o = 1; o < 32; o <<= 1) {
-            const int n = __shfl_up_sync(FULL_MASK, incl, o);
-            if (lane >= o) {
-                incl += n;
-            }
-        }
-        if (lane == 31) {
-            wsum[warp] = incl;
-        }
-        __syncthreads();
-        int wprefix = 0;
-        for (int w = 0; w < warp; w++) {
-            wprefix += wsum[w];
-        }
-        int pos = carry + wprefix + incl - ni;
-        for (int c = 0; c < ni; c++) {
-            const int first = c * a.chunk;
-            a.items[pos + c] = make_int4(r, (int)(tile_base(a, r) + first), min(a.chunk, nt - first), 0);
-        }
-        __syncthreads();
-        if (threadIdx.x == 0) {
-            int tot = 0;
-            for (int w = 0; w < TB_WARPS; w++) {
-                tot += wsum[w];
-            }
-            carry += tot;
-        }
-        __syncthreads();
-    }
-    if (threadIdx.x == 0) {
-        state->n_items = carry;
+        __threadfence();
+        state->n_items = *((volatile int *)&state->item_count);
+        state->item_count = 0;
         state->items_chunk = a.chunk;
         state->dep_dirty = 1; // the lambda-dependent tiles follow the new list
         state->n_dep = 0;
