@@ -380,9 +380,12 @@ __device__ __forceinline__ void bin_scan_cta(const SortArgs &a, DevState *state)
     const int lane = threadIdx.x & 31;
     const int wid = threadIdx.x >> 5;
     const int nwarps = blockDim.x >> 5;
-    for (int base = 0; base < NB; base += blockDim.x) {
-        const int b = base + threadIdx.x;
-        const int v = b < NB ? a.bin_count[b] : 0;
+    // four consecutive cells per thread (NB is a multiple of 64, the counts
+    // 256-byte aligned): a quarter of the passes and barriers
+    for (int base = 0; base < NB; base += 4 * (int)blockDim.x) {
+        const int b = base + 4 * (int)threadIdx.x;
+        const int4 c4 = b < NB ? *reinterpret_cast<const int4 *>(a.bin_count + b) : make_int4(0, 0, 0, 0);
+        const int v = c4.x + c4.y + c4.z + c4.w;
         int incl = v;
         for (int o = 1; o < 32; o <<= 1) {
             const int n = __shfl_up_sync(FULL_MASK, incl, o);
@@ -409,8 +412,9 @@ __device__ __forceinline__ void bin_scan_cta(const SortArgs &a, DevState *state)
         __syncthreads();
         const int warp_prefix = wid > 0 ? warp_sums[wid - 1] : 0;
         if (b < NB) {
-            a.bin_cursor[b] = carry + warp_prefix + incl - v;
-            a.bin_count[b] = 0;
+            const int e = carry + warp_prefix + incl - v;
+            *reinterpret_cast<int4 *>(a.bin_cursor + b) = make_int4(e, e + c4.x, e + c4.x + c4.y, e + c4.x + c4.y + c4.z);
+            *reinterpret_cast<int4 *>(a.bin_count + b) = make_int4(0, 0, 0, 0);
         }
         __syncthreads();
         if (threadIdx.x == 0) {
