@@ -616,8 +616,9 @@ static __global__ void k_block_bounds(
 // radius (minimum image, 3D). Kept atoms are packed 32 to a tile, so a tile is
 // rows x 32 pairs; smaller row groups sit in smaller regions and list fewer
 // out-of-range column atoms. The tiles of row group g occupy a fixed range
-// (tile_base) sized by the column blocks it can reach. The last CTA to finish
-// turns the per-group tile counts into work items of at most `chunk` tiles.
+// (tile_base) sized by the column blocks it can reach. Each group's CTA cuts
+// its tiles into work items of at most `chunk` tiles, written at a range it
+// reserves from a counter; the last CTA to finish publishes the item count.
 // (Same selection rule as timemachine/cpp/src/kernels/k_neighborlist.cuh:168-427,
 // which uses 32-atom row blocks.)
 // ---------------------------------------------------------------------------
