@@ -115,6 +115,31 @@ def test_multi_step_graphs_with_frames_equal_eager():
         np.testing.assert_array_equal(a, b)
 
 
+def test_fused_graph_steps_leave_the_potential_clean():
+    """Captured multi-step runs hand the nonbonded potential's coordinate
+    staging and force scatter to the integrator kernel. With the nonbonded
+    potential first in the list (recorded on the capture stream, not on a
+    forked branch) the trajectory equals eager steps bit for bit, and
+    afterwards the same potential evaluates exactly like a fresh instance (no
+    forces left in its accumulators, staging and work counter in order)."""
+    s = testsystems.build_system(500, 2.9, seed=17, n_ligand=10)
+    lam = np.full(60, 0.2)  # captured runs of 25, 25 and 10 steps
+    runs = []
+    for use_graphs in (True, False):
+        bps = _bound_potentials(s)[::-1]
+        intg = md.LangevinIntegrator(300.0, 2.0e-3, 1.0, s.masses, 31)
+        ctx = md.Context(s.x, _v0(s, 300.0, 31), s.box, intg, bps, use_graphs=use_graphs)
+        ctx.multiple_steps(lam)
+        x, box = ctx.get_x_t(), ctx.get_box()
+        runs.append((x, ctx.get_v_t(), bps[0].execute(x, box, 0.2)))
+    np.testing.assert_array_equal(runs[0][0], runs[1][0])
+    np.testing.assert_array_equal(runs[0][1], runs[1][1])
+    fresh = _bound_potentials(s)[2].execute(runs[0][0], s.box, 0.2)
+    for out in (runs[0][2], runs[1][2]):
+        for a, b in zip(out, fresh):
+            np.testing.assert_array_equal(a, b)
+
+
 def test_single_step_follows_baoab_update():
     """Zero temperature (no noise): x1, v1 equal the BAOAB update of
     timemachine/cpp/src/integrator.cu:37-69 with the potential's forces."""

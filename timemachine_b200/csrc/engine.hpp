@@ -98,6 +98,22 @@ inline int num_sms() {
 }
 
 // Device-level contract of a potential (timemachine/cpp/src/potential.hpp:51-62).
+// What an MD integrator kernel needs to take over a potential's per-step
+// coordinate staging and force scatter (single lambda window, forces only):
+// the slot order, the staged coordinates, the neighbour-list reference
+// coordinates and flags, and the slot-ordered fixed-point force accumulators.
+struct MDFusion {
+    const int *slot_of;      // [N] atom -> slot
+    float4 *posw;            // [S] staged x, y, z, w (the integrator writes x, y, z)
+    const double *nb_x;      // [N,3] coordinates at the last neighbour-list rebuild
+    double half_pad2;        // (padding / 2)^2
+    int *rebuild;            // set to 1 when an atom moved more than padding / 2
+    int *next_item;          // the pair kernel's work counter, reset for the next step
+    const int *error;        // nonzero: the potential failed, its forces are not added
+    unsigned long long *acc; // [3][S] slot-ordered fixed-point forces x, y, z
+    int S;
+};
+
 class PotentialBase {
   public:
     virtual ~PotentialBase() { release_host_stream(); }
@@ -125,6 +141,26 @@ class PotentialBase {
         for (int i = 0; i < P; i++) {
             out[i] = static_cast<double>(static_cast<long long>(du_dp[i])) / static_cast<double>(0x1000000000ULL);
         }
+    }
+
+    // MD integrator fusion: fills `f` and returns true when this potential can
+    // leave its forces in slot-ordered accumulators for the integrator kernel
+    // and take coordinates staged by it.
+    virtual bool md_fusion(MDFusion &f) {
+        (void)f;
+        return false;
+    }
+
+    // Forces of one MD step for a fused integrator (only when md_fusion() is
+    // true): the forces stay in MDFusion::acc, where the integrator kernel
+    // reads them; `prestaged` = the previous integrator kernel staged these
+    // coordinates, took the neighbour-list test and reset the work counter
+    // (same lambda, parameters and box as the previous call).
+    virtual void execute_md_fused(
+        int N, int P, const double *d_x, const double *d_p, const double *d_box, double lambda, bool prestaged,
+        cudaStream_t stream) {
+        (void)N, (void)P, (void)d_x, (void)d_p, (void)d_box, (void)lambda, (void)prestaged, (void)stream;
+        throw Error(TMNB_ERR_INTERNAL, "potential has no fused MD path");
     }
 
     // K lambda windows on the same coordinates and parameters; output k of

@@ -21,6 +21,16 @@
 #include <map>
 #include <vector>
 
+// Captured multi-step MD graphs hand the nonbonded potential's per-step
+// staging and force scatter to the integrator kernel (k_langevin_fused).
+#ifndef TMNB_MD_FUSE
+#define TMNB_MD_FUSE 1
+#endif
+// 1: k_langevin_fused clears the accumulators it read; 0: a memset after it.
+#ifndef TMNB_MD_FUSED_ZERO
+#define TMNB_MD_FUSED_ZERO 0
+#endif
+
 namespace tmb {
 
 namespace {
@@ -71,6 +81,87 @@ __global__ void k_langevin(
     const int i = t >> 1;
     if (i < N) {
         langevin_atom_half(i, t & 1, s_step, key, ca, cbs[i], ccs[i], dt, x, v, du_dx);
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        __threadfence();
+        if (atomicAdd(&st->done_blocks, 1u) == gridDim.x - 1) {
+            st->step += 1;
+            st->done_blocks = 0;
+        }
+    }
+}
+
+// The integrator step fused with a potential's per-step staging and force
+// scatter (MDFusion). Each atom's force adds the potential's slot-ordered
+// fixed-point accumulator (what k_finalize would have added; integer sums, so
+// the order does not matter), which is cleared for the next step here
+// (TMNB_MD_FUSED_ZERO) or by a memset after the kernel. With `stage_next` the
+// new coordinates are staged into the potential's slots and the
+// neighbour-list test of k_check_prepare is taken, so the next step's forces
+// start at the rebuild chain and the pair kernel.
+__global__ void k_langevin_fused(
+    int N,
+    double ca,
+    const double *__restrict__ cbs,
+    const double *__restrict__ ccs,
+    double dt,
+    double *__restrict__ x,
+    double *__restrict__ v,
+    unsigned long long *__restrict__ du_dx,
+    uint2 key,
+    MDState *st,
+    MDFusion f,
+    int stage_next) {
+    grid_dependency_wait();
+    __shared__ unsigned long long s_step;
+    if (threadIdx.x == 0) {
+        s_step = st->step;
+    }
+    __syncthreads();
+    // two threads per atom, as k_langevin: half 0 updates x and y, half 1 z
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int i = t >> 1;
+    const int half = t & 1;
+    const bool ok = *f.error == 0; // k_finalize adds nothing after an error
+    double c0 = 0.0, c1 = 0.0;     // the new coordinates: x, y (half 0) or z (half 1)
+    int s = 0;
+    if (i < N) {
+        s = f.slot_of[i];
+        const uint4 r = philox4x32_10(make_uint4((unsigned)i, (unsigned)s_step, (unsigned)(s_step >> 32), (unsigned)half), key);
+        const double2 n = normal2(r.x, r.y, r.z, r.w);
+        if (half == 0) {
+            const unsigned long long ax = f.acc[s];
+            const unsigned long long ay = f.acc[(size_t)f.S + s];
+            if (TMNB_MD_FUSED_ZERO) {
+                f.acc[s] = 0;
+                f.acc[(size_t)f.S + s] = 0;
+            }
+            c0 = langevin_dim(3 * i + 0, n.x, ca, cbs[i], ccs[i], dt, x, v, du_dx, ok ? ax : 0ull);
+            c1 = langevin_dim(3 * i + 1, n.y, ca, cbs[i], ccs[i], dt, x, v, du_dx, ok ? ay : 0ull);
+        } else {
+            const unsigned long long az = f.acc[2 * (size_t)f.S + s];
+            if (TMNB_MD_FUSED_ZERO) {
+                f.acc[2 * (size_t)f.S + s] = 0;
+            }
+            c0 = langevin_dim(3 * i + 2, n.x, ca, cbs[i], ccs[i], dt, x, v, du_dx, ok ? az : 0ull);
+        }
+    }
+    if (stage_next) {
+        // the pair of lanes (2m, 2m + 1) holds one atom; half 0 takes its z
+        const double z_new = __shfl_down_sync(0xffffffffu, c0, 1);
+        if (half == 0 && i < N) {
+            // the staged values of k_check_prepare: FP32 coordinates, w kept
+            *reinterpret_cast<float2 *>(f.posw + s) = make_float2((float)c0, (float)c1);
+            reinterpret_cast<float *>(f.posw + s)[2] = (float)z_new;
+            const double *xo = f.nb_x + 3 * (size_t)i;
+            if (moved_beyond_half_padding(c0 - xo[0], c1 - xo[1], z_new - xo[2], f.half_pad2)) {
+                *f.rebuild = 1; // benign race: every writer stores 1
+            }
+        }
+        if (t == 0) {
+            *f.next_item = 0;
+        }
     }
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -420,9 +511,26 @@ class Context {
     // on its own forked stream, so the captured graph runs the potentials
     // concurrently; they all add into du_dx / du_dl with integer atomics, so
     // the sums do not depend on the order.
-    void record_step(double lambda, unsigned long long *dl_out, bool branch = false) {
+    //
+    // With `fuse` (forces only), the first potential that offers it hands its
+    // coordinate staging and force scatter to the integrator kernel
+    // (k_langevin_fused): `prestaged` = the previous step's integrator kernel
+    // staged this step's coordinates, `stage_next` = this step's integrator
+    // kernel stages the next step's (same lambda, no barostat move between).
+    void record_step(
+        double lambda, unsigned long long *dl_out, bool branch = false, bool fuse = false, bool prestaged = false,
+        bool stage_next = false) {
         const size_t n = bps_.size();
         const bool fork = branch && n > 1;
+        MDFusion f{};
+        int fk = -1;
+        if (fuse && !dl_out) {
+            for (size_t k = 0; k < n && fk < 0; k++) {
+                if (bps_[k]->pot->md_fusion(f)) {
+                    fk = (int)k;
+                }
+            }
+        }
         if (fork) {
             ensure_branches(n - 1);
             CK(cudaEventRecord(fork_ev_, stream_));
@@ -434,9 +542,13 @@ class Context {
                 CK(cudaStreamWaitEvent(s, fork_ev_, 0));
             }
             BoundPot &b = *bps_[k];
-            b.pot->execute_device(
-                N_, b.P, x_.p, b.params.p, box_.p, lambda, du_dx_.p, nullptr, dl_out ? du_dl_buf_.p : nullptr,
-                nullptr, s);
+            if ((int)k == fk) {
+                b.pot->execute_md_fused(N_, b.P, x_.p, b.params.p, box_.p, lambda, prestaged, s);
+            } else {
+                b.pot->execute_device(
+                    N_, b.P, x_.p, b.params.p, box_.p, lambda, du_dx_.p, nullptr, dl_out ? du_dl_buf_.p : nullptr,
+                    nullptr, s);
+            }
             if (fork && k > 0) {
                 CK(cudaEventRecord(join_ev_[k - 1], s));
                 CK(cudaStreamWaitEvent(stream_, join_ev_[k - 1], 0));
@@ -446,6 +558,17 @@ class Context {
             k_reduce_dl<<<1, 1024, 0, stream_>>>(N_, du_dl_buf_.p, dl_out, st_.p);
         }
         const int tpb = 128;
+        if (fk >= 0) {
+            launch_dependent(
+                k_langevin_fused, dim3((2 * N_ + tpb - 1) / tpb), dim3(tpb), 0, stream_, N_, ca_,
+                (const double *)cbs_.p, (const double *)ccs_.p, dt_, x_.p, v_.p, du_dx_.p, key_, st_.p, f,
+                stage_next ? 1 : 0);
+            CK(cudaPeekAtLastError());
+            if (!TMNB_MD_FUSED_ZERO) {
+                CK(cudaMemsetAsync(f.acc, 0, 3 * (size_t)f.S * sizeof(unsigned long long), stream_));
+            }
+            return;
+        }
         launch_dependent(
             k_langevin, dim3((2 * N_ + tpb - 1) / tpb), dim3(tpb), 0, stream_, N_, ca_, (const double *)cbs_.p,
             (const double *)ccs_.p, dt_, x_.p, v_.p, du_dx_.p, key_, st_.p);
@@ -490,8 +613,11 @@ class Context {
             if (kind == 0) {
                 record_step(lambda, dl_out, true);
             } else if (kind == 2) {
+                // steps after the first take the coordinates the previous
+                // step's integrator kernel staged
                 for (int k = 0; k < steps; k++) {
-                    record_step(lambda, nullptr, true);
+                    record_step(lambda, nullptr, true, TMNB_MD_FUSE != 0, TMNB_MD_FUSE && k > 0,
+                                TMNB_MD_FUSE && k + 1 < steps);
                 }
             } else {
                 record_barostat(lambda);

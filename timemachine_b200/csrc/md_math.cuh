@@ -40,8 +40,10 @@ __device__ __forceinline__ double2 normal2(unsigned a, unsigned b, unsigned c, u
 }
 
 // One component's update with its noise; the force accumulator is zeroed for
-// the next step.
-__device__ __forceinline__ void langevin_dim(
+// the next step. `extra` is added to the accumulator first (fixed point: the
+// forces a fused potential left in its own slot-ordered accumulators).
+// Returns the new coordinate.
+__device__ __forceinline__ double langevin_dim(
     int k,
     double noise,
     double ca,
@@ -50,13 +52,16 @@ __device__ __forceinline__ void langevin_dim(
     double dt,
     double *__restrict__ x,
     double *__restrict__ v,
-    unsigned long long *__restrict__ du_dx) {
-    const double force = static_cast<double>(static_cast<long long>(du_dx[k])) / FX_EXPONENT;
+    unsigned long long *__restrict__ du_dx,
+    unsigned long long extra = 0) {
+    const double force = static_cast<double>(static_cast<long long>(du_dx[k] + extra)) / FX_EXPONENT;
     const double v_mid = v[k] + cb * force;
     const double v_new = ca * v_mid + cc * noise;
     v[k] = v_new;
-    x[k] += 0.5 * dt * (v_mid + v_new);
+    const double x_new = x[k] + 0.5 * dt * (v_mid + v_new);
+    x[k] = x_new;
     du_dx[k] = 0; // the next step accumulates from zero
+    return x_new;
 }
 
 // One atom's update: v_mid = v + cb * F, v' = ca * v_mid + cc * noise,

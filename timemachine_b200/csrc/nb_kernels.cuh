@@ -256,7 +256,7 @@ static __global__ void k_check_prepare(
             const double dx = xn[0] - xo[0];
             const double dy = xn[1] - xo[1];
             const double dz = xn[2] - xo[2];
-            if (dx * dx + dy * dy + dz * dz > half_pad2) {
+            if (moved_beyond_half_padding(dx, dy, dz, half_pad2)) {
                 state->rebuild = 1; // benign race: every writer stores 1
             }
         }

@@ -341,4 +341,12 @@ __device__ __forceinline__ void lennard_jones(
     eps_grad = fmul(fmul(fmul(lj_scale, (Real)4), s6m1), s6);
 }
 
+// Neighbour-list validity: true when an atom moved more than half the padding
+// since the last rebuild (squared displacement against (padding / 2)^2).
+// Explicit rounding, so the pair kernel's own check and the MD integrator's
+// fused check take the same decision for the same coordinates.
+__device__ __forceinline__ bool moved_beyond_half_padding(double dx, double dy, double dz, double half_pad2) {
+    return __dadd_rn(__dadd_rn(__dmul_rn(dx, dx), __dmul_rn(dy, dy)), __dmul_rn(dz, dz)) > half_pad2;
+}
+
 } // namespace tmb

@@ -517,12 +517,14 @@ class NonbondedPotential : public PotentialBase {
         // k_check_prepare: one thread per (window, slot)
         const int pgrid = (int)std::max<size_t>(
             1, std::min<size_t>(((size_t)S_ * K + tpb - 1) / tpb, 8 * (size_t)num_sms()));
-        stage_begin(TMNB_STAGE_PREPARE, stream);
-        launch_dependent(
-            k_check_prepare, dim3(pgrid), dim3(tpb), 0, stream, pa, (const unsigned *)perm_.p,
-            (const double *)(has_nblist_ ? nb_x_.p : nullptr), (const double *)nb_box_.p, state_.p);
-        CK(cudaPeekAtLastError());
-        stage_end(TMNB_STAGE_PREPARE, stream);
+        if (!(fuse_ & FUSE_PRESTAGED)) {
+            stage_begin(TMNB_STAGE_PREPARE, stream);
+            launch_dependent(
+                k_check_prepare, dim3(pgrid), dim3(tpb), 0, stream, pa, (const unsigned *)perm_.p,
+                (const double *)(has_nblist_ ? nb_x_.p : nullptr), (const double *)nb_box_.p, state_.p);
+            CK(cudaPeekAtLastError());
+            stage_end(TMNB_STAGE_PREPARE, stream);
+        }
         if (has_nblist_) {
             stage_begin(TMNB_STAGE_REBUILD, stream);
             record_rebuild_chain(d_x, d_box, pa, sgrid, tpb, stream, K);
@@ -575,6 +577,9 @@ class NonbondedPotential : public PotentialBase {
             launch_dependent(k, dim3(pair_grid(k, smem)), dim3(128), smem, stream, a);
             CK(cudaPeekAtLastError());
             stage_end(TMNB_STAGE_PAIR, stream);
+            if (fuse_ & FUSE_KEEP_FORCES) {
+                return; // the integrator kernel reads and clears the accumulators
+            }
 
             FinalizeArgs fa;
             fa.N = N_;
@@ -613,6 +618,36 @@ class NonbondedPotential : public PotentialBase {
             CK(cudaMemsetAsync(acc_.p, 0, used * sizeof(unsigned long long), stream));
             stage_end(TMNB_STAGE_FINALIZE, stream);
         }
+    }
+
+    bool md_fusion(MDFusion &f) override {
+        // every atom in the set (slot_of a bijection), FP32 staging, a neighbour list
+        if (!has_nblist_ || fp64_ || kind_ == Kind::Group || S_ != N_ || set_atoms_.p != nullptr) {
+            return false;
+        }
+        ensure_windows(1);
+        f.slot_of = slot_of_.p;
+        f.posw = posw_.p;
+        f.nb_x = nb_x_.p;
+        f.half_pad2 = 0.25 * padding_ * padding_;
+        f.rebuild = &state_.p->rebuild;
+        f.next_item = &state_.p->next_item;
+        f.error = &state_.p->error;
+        f.acc = acc_.p;
+        f.S = S_;
+        return true;
+    }
+
+    void execute_md_fused(
+        int N, int P, const double *d_x, const double *d_p, const double *d_box, double lambda, bool prestaged,
+        cudaStream_t stream) override {
+        struct Reset {
+            int &v;
+            ~Reset() { v = 0; }
+        } reset{fuse_};
+        fuse_ = FUSE_KEEP_FORCES | (prestaged ? FUSE_PRESTAGED : 0);
+        // forces only; the du_dx argument selects the variant and is not written
+        execute_windows_device(N, P, d_x, d_p, d_box, 1, &lambda, acc_.p, nullptr, nullptr, nullptr, stream);
     }
 
     // Neighbour-list rebuild: spatial sort (keys, scan, scatter), block
@@ -882,6 +917,10 @@ class NonbondedPotential : public PotentialBase {
     DevBuf<double4> posw64_, prm64_, dprm64_;
     DevBuf<unsigned char> lamdep_;
     DevBuf<unsigned long long> acc_;
+    // MD integrator fusion of the call in progress (execute_md_fused)
+    static constexpr int FUSE_PRESTAGED = 1;   // coordinates staged by the integrator kernel
+    static constexpr int FUSE_KEEP_FORCES = 2; // forces left in acc_ (no k_finalize, no clear)
+    int fuse_ = 0;
     DevBuf<double> nb_x_, nb_box_;
     DevBuf<unsigned> keys_;
     DevBuf<int> bin_count_, bin_cursor_;
