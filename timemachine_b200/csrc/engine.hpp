@@ -143,6 +143,12 @@ class PotentialBase {
         }
     }
 
+    // Counts the changes to what launches recorded in a CUDA graph hold:
+    // reallocated device buffers (staging, accumulators, tile lists) and
+    // settings passed by value (padding, lambda schedules, sort order). A
+    // graph captured before a change must not be replayed after it.
+    virtual unsigned long long buffer_generation() const { return 0; }
+
     // MD integrator fusion: fills `f` and returns true when this potential can
     // leave its forces in slot-ordered accumulators for the integrator kernel
     // and take coordinates staged by it.

@@ -499,6 +499,15 @@ class Context {
         invalidate_graphs();
     }
 
+    std::vector<unsigned long long> buffer_generations() const {
+        std::vector<unsigned long long> g;
+        for (const auto &b : bps_) {
+            g.push_back(b->pot->buffer_generation());
+            g.push_back(b->trial ? b->trial->buffer_generation() : 0);
+        }
+        return g;
+    }
+
     void invalidate_graphs() {
         for (auto &kv : graphs_) {
             cudaGraphExecDestroy(kv.second);
@@ -599,6 +608,13 @@ class Context {
     // kind 0: one step (du_dl into dl_out if given); 1: the barostat move;
     // 2: `steps` steps.
     cudaGraphExec_t graph_for(int kind, double lambda, unsigned long long *dl_out, int steps = 1) {
+        // a potential that reallocated buffers since the graphs were captured
+        // (e.g. grown by a multi-window evaluation) invalidates all of them
+        const std::vector<unsigned long long> gens = buffer_generations();
+        if (gens != graph_generations_) {
+            invalidate_graphs();
+            graph_generations_ = gens;
+        }
         const auto key = std::make_tuple(kind, lambda, (const void *)dl_out, steps);
         auto it = graphs_.find(key);
         if (it != graphs_.end()) {
@@ -913,6 +929,7 @@ class Context {
     std::vector<std::unique_ptr<BoundPot>> bps_;
     cudaStream_t stream_ = nullptr;
     std::map<std::tuple<int, double, const void *, int>, cudaGraphExec_t> graphs_;
+    std::vector<unsigned long long> graph_generations_; // buffer_generations() when graphs_ were captured
     static constexpr int MAX_GRAPH_STEPS = 25; // steps captured in one graph at most
     std::vector<cudaStream_t> side_;
     std::vector<cudaEvent_t> join_ev_;

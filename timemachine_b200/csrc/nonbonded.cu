@@ -289,6 +289,7 @@ class NonbondedPotential : public PotentialBase {
 
     // Tile storage for row groups of rows_ slots (and the work-item capacity).
     void alloc_list() {
+        generation_++;
         n_row_blocks_ = ((kind_ == Kind::Group ? NR_ : S_) + rows_ - 1) / rows_;
         tile_cols_.alloc((size_t)tile_slots() * TILE);
         rb_ntiles_.alloc(n_row_blocks_);
@@ -372,8 +373,12 @@ class NonbondedPotential : public PotentialBase {
             throw Error(TMNB_ERR_INVALID_ARGUMENT, "padding must be non-negative");
         }
         padding_ = p;
+        generation_++; // captured launches hold the padding
     }
-    void disable_hilbert() { hilbert_ = false; }
+    void disable_hilbert() {
+        hilbert_ = false;
+        generation_++;
+    }
 
     // The four lambda schedules (timemachine/cpp/src/wrap_kernels.cpp:843-893);
     // nullptr keeps the identity "lambda". Parse errors throw.
@@ -389,6 +394,7 @@ class NonbondedPotential : public PotentialBase {
         }
         // (non-interpolated potentials, like the reference's, read only the w schedule)
         xf_ = t;
+        generation_++; // captured launches hold the schedules' values
     }
     const LambdaTransforms &transforms() const { return xf_; }
 
@@ -410,6 +416,10 @@ class NonbondedPotential : public PotentialBase {
     // Staging and accumulator capacity for K windows: K staged copies of the
     // slots and, for K > 1, the shared block plus one block per window.
     void ensure_windows(int K) {
+        if (posw_.n < (size_t)K * S_ || acc_.n < acc_block_elems() * (K > 1 ? 1 + K : 1) ||
+            (K > 1 && has_nblist_ && dep_tiles_.n == 0)) {
+            generation_++; // buffers below are reallocated
+        }
         if (posw_.n < (size_t)K * S_) {
             posw_.alloc((size_t)K * S_);
             prm_.alloc((size_t)K * S_);
@@ -619,6 +629,8 @@ class NonbondedPotential : public PotentialBase {
             stage_end(TMNB_STAGE_FINALIZE, stream);
         }
     }
+
+    unsigned long long buffer_generation() const override { return generation_; }
 
     bool md_fusion(MDFusion &f) override {
         // every atom in the set (slot_of a bijection), FP32 staging, a neighbour list
@@ -921,6 +933,7 @@ class NonbondedPotential : public PotentialBase {
     static constexpr int FUSE_PRESTAGED = 1;   // coordinates staged by the integrator kernel
     static constexpr int FUSE_KEEP_FORCES = 2; // forces left in acc_ (no k_finalize, no clear)
     int fuse_ = 0;
+    unsigned long long generation_ = 0; // buffer_generation()
     DevBuf<double> nb_x_, nb_box_;
     DevBuf<unsigned> keys_;
     DevBuf<int> bin_count_, bin_cursor_;
