@@ -21,16 +21,6 @@
 #include <map>
 #include <vector>
 
-// Captured multi-step MD graphs hand the nonbonded potential's per-step
-// staging and force scatter to the integrator kernel (k_langevin_fused).
-#ifndef TMNB_MD_FUSE
-#define TMNB_MD_FUSE 1
-#endif
-// 1: k_langevin_fused clears the accumulators it read; 0: a memset after it.
-#ifndef TMNB_MD_FUSED_ZERO
-#define TMNB_MD_FUSED_ZERO 0
-#endif
-
 namespace tmb {
 
 namespace {
@@ -95,8 +85,9 @@ __global__ void k_langevin(
 // The integrator step fused with a potential's per-step staging and force
 // scatter (MDFusion). Each atom's force adds the potential's slot-ordered
 // fixed-point accumulator (what k_finalize would have added; integer sums, so
-// the order does not matter), which is cleared for the next step here
-// (TMNB_MD_FUSED_ZERO) or by a memset after the kernel. With `stage_next` the
+// the order does not matter); a memset after the kernel clears the
+// accumulators for the next step (clearing each slot here, from the gathered
+// reads, measured slower). With `stage_next` the
 // new coordinates are staged into the potential's slots and the
 // neighbour-list test of k_check_prepare is taken, so the next step's forces
 // start at the rebuild chain and the pair kernel.
@@ -133,17 +124,10 @@ __global__ void k_langevin_fused(
         if (half == 0) {
             const unsigned long long ax = f.acc[s];
             const unsigned long long ay = f.acc[(size_t)f.S + s];
-            if (TMNB_MD_FUSED_ZERO) {
-                f.acc[s] = 0;
-                f.acc[(size_t)f.S + s] = 0;
-            }
             c0 = langevin_dim(3 * i + 0, n.x, ca, cbs[i], ccs[i], dt, x, v, du_dx, ok ? ax : 0ull);
             c1 = langevin_dim(3 * i + 1, n.y, ca, cbs[i], ccs[i], dt, x, v, du_dx, ok ? ay : 0ull);
         } else {
             const unsigned long long az = f.acc[2 * (size_t)f.S + s];
-            if (TMNB_MD_FUSED_ZERO) {
-                f.acc[2 * (size_t)f.S + s] = 0;
-            }
             c0 = langevin_dim(3 * i + 2, n.x, ca, cbs[i], ccs[i], dt, x, v, du_dx, ok ? az : 0ull);
         }
     }
@@ -573,9 +557,7 @@ class Context {
                 (const double *)cbs_.p, (const double *)ccs_.p, dt_, x_.p, v_.p, du_dx_.p, key_, st_.p, f,
                 stage_next ? 1 : 0);
             CK(cudaPeekAtLastError());
-            if (!TMNB_MD_FUSED_ZERO) {
-                CK(cudaMemsetAsync(f.acc, 0, 3 * (size_t)f.S * sizeof(unsigned long long), stream_));
-            }
+            CK(cudaMemsetAsync(f.acc, 0, 3 * (size_t)f.S * sizeof(unsigned long long), stream_));
             return;
         }
         launch_dependent(
@@ -632,8 +614,7 @@ class Context {
                 // steps after the first take the coordinates the previous
                 // step's integrator kernel staged
                 for (int k = 0; k < steps; k++) {
-                    record_step(lambda, nullptr, true, TMNB_MD_FUSE != 0, TMNB_MD_FUSE && k > 0,
-                                TMNB_MD_FUSE && k + 1 < steps);
+                    record_step(lambda, nullptr, true, true, k > 0, k + 1 < steps);
                 }
             } else {
                 record_barostat(lambda);
