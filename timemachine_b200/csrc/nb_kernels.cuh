@@ -59,7 +59,8 @@ struct DevState {
     int rebuild;          // 1: the neighbour list must be rebuilt in this evaluation
     int error;            // sticky error code (TMNB_ERR_* values), 0 = ok
     int n_items;          // tile work items produced by the last rebuild
-    int next_item;        // dynamic work counter of k_pair (reset by k_check_prepare)
+    int next_item;        // dynamic work counter of k_pair (reset by k_check_prepare, or in a
+                          // fused MD step by the integrator kernel that staged the coordinates)
     unsigned done_ctas;   // completion counter of k_build_tiles
     unsigned total_tiles; // tiles produced by the last rebuild
     int rebuilds;         // number of rebuilds performed (diagnostics)
