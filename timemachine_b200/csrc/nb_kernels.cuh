@@ -1975,8 +1975,10 @@ __global__ void __launch_bounds__(128, (pair_min_ctas<Real, U, DX, DL, DP, INTER
     const unsigned S = (unsigned)a.S;
     const int n_items = a.state->n_items;
     const int n_dep_units = MULTI ? a.state->n_dep * a.K : 0;
-    if (MULTI && blockIdx.x == 0 && threadIdx.x == 0) {
-        a.state->dep_dirty = 0; // k_dep_tiles (before this launch) has redone the list
+    if (MULTI && blockIdx.x == 0 && threadIdx.x == 0 && !a.state->error) {
+        // k_dep_tiles (before this launch) has redone the list; after an
+        // error it did not, so the list stays dirty for the next call
+        a.state->dep_dirty = 0;
     }
     const int n_tiles_units = n_items + n_dep_units;
     const int n_total = n_tiles_units + (a.M + TILE - 1) / TILE;
